@@ -1,0 +1,161 @@
+"""B200-native BAAS sparse hot path: Python binding over the C ABI (include/baas_b200.h).
+
+The compute runs in ``baas_b200/_lib/libbaas_b200.so`` (hand-written sm_100a kernels). This
+module only marshals arrays: host numpy arrays for the analysis, torch CUDA tensors for the
+device calls. There is no CPU fallback -- every compute call goes to the CUDA library and raises
+if it is missing or fails.
+
+Names follow the reference's runtime surface (test/Schedule.hpp:39-178): a :class:`Schedule`
+is built once from a matrix pattern (``Scheduler::preprocessing``) and then drives
+``ic0`` / ``ilu0`` (``runIC0``), ``forward`` / ``backward`` (``runForwardTRSVNoPerm`` /
+``runBackwardTRSVNoPerm``) and ``iccg`` (the ``pcg_opt`` loop).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, PREC_FP32_FACTORS, PREC_FP64,
+                      BaasError)
+from .gen import CSR
+
+__all__ = ["Schedule", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV", "KERNEL_ICCG", "KERNEL_IC0",
+           "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "version"]
+
+
+def version() -> str:
+    return _native.lib().baas_version().decode()
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array or a torch tensor."""
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+@dataclass
+class DeviceCSR:
+    """A CSR matrix resident on the GPU (torch tensors)."""
+    n: int
+    rowptr: "object"
+    colidx: "object"
+    values: "object"
+
+    @property
+    def nnz(self) -> int:
+        return int(self.colidx.numel())
+
+    @staticmethod
+    def from_host(m: CSR, device="cuda") -> "DeviceCSR":
+        import torch
+
+        return DeviceCSR(m.n, torch.from_numpy(m.rowptr).to(device), torch.from_numpy(m.colidx).to(device),
+                         torch.from_numpy(m.values).to(device))
+
+    def c(self) -> _native.BaasCsr:
+        return _native.BaasCsr(self.n, self.nnz, _ptr(self.rowptr), _ptr(self.colidx), _ptr(self.values))
+
+
+class Schedule:
+    """BAAS schedule + device plan for one sparsity pattern.
+
+    kind: KERNEL_SPTRSV (input is the lower triangle L), KERNEL_ICCG (full SPD A, as
+    ``Scheduler(A, true, false, P2P_RULE, nthread)``), KERNEL_IC0, KERNEL_ILU0.
+    """
+
+    def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
+                 ctas_per_sm: int = 0):
+        L = _native.lib()
+        self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
+        self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
+        c = _native.BaasCsr(A.n, int(self._rowptr[-1]), _ptr(self._rowptr), _ptr(self._colidx), None)
+        opt = _native.BaasOptions()
+        L.baas_options_default(C.byref(opt))
+        opt.nthread = nthread
+        opt.spin_limit = spin_limit
+        opt.ctas_per_sm = ctas_per_sm
+        h = C.c_void_p()
+        _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
+        self._h = h
+        self.n = A.n
+        self.nnz = int(self._rowptr[-1])
+        self.kind = kind
+        self.nthread = nthread
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _native.lib().baas_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ---- schedule export (host only) ----
+    def export(self, field: str) -> np.ndarray:
+        L = _native.lib()
+        fid = _native.FIELDS[field]
+        n = L.baas_schedule_export(self._h, fid, None)
+        if n < 0:
+            raise KeyError(field)
+        out = np.zeros(max(n, 1), dtype=np.int32)
+        L.baas_schedule_export(self._h, fid, out.ctypes.data)
+        return out[:n]
+
+    def arrays(self) -> dict:
+        return {k: self.export(k) for k in _native.FIELDS}
+
+    @property
+    def analysis_ms(self) -> float:
+        return _native.lib().baas_schedule_analysis_ms(self._h)
+
+    # ---- device compute (torch CUDA tensors) ----
+    def sptrsv(self, T: DeviceCSR, b, x, upper: bool, stream=None) -> None:
+        """x = T^-1 b for T lower (diagonal last) or upper (diagonal first); b, x are (n,) or
+        (nrhs, n) contiguous float64 CUDA tensors (rows of a 2-D tensor are right-hand sides)."""
+        nrhs = 1 if b.dim() == 1 else int(b.shape[0])
+        c = T.c()
+        st = _native.lib().baas_sptrsv(self._h, C.byref(c), int(upper), _ptr(b), _ptr(x), nrhs, self.n,
+                                       _stream_ptr(stream))
+        _native.check(st, "baas_sptrsv")
+
+    def forward(self, L: DeviceCSR, b, x, stream=None) -> None:
+        self.sptrsv(L, b, x, False, stream)
+
+    def backward(self, U: DeviceCSR, b, x, stream=None) -> None:
+        self.sptrsv(U, b, x, True, stream)
+
+    def ic0(self, A: DeviceCSR, lu, stream=None) -> None:
+        """IC0 in place on lu (pre-filled with A.values)."""
+        c = A.c()
+        _native.check(_native.lib().baas_ic0(self._h, C.byref(c), _ptr(lu), _stream_ptr(stream)), "baas_ic0")
+
+    def ilu0(self, A: DeviceCSR, lu, stream=None) -> None:
+        """ILU0 in place on lu (pre-filled with A.values)."""
+        c = A.c()
+        _native.check(_native.lib().baas_ilu0(self._h, C.byref(c), _ptr(lu), _stream_ptr(stream)), "baas_ilu0")
+
+    def iccg(self, A: DeviceCSR, b, x, tol: float = 1e-10, maxiter: int = 2000, precision: int = PREC_FP64,
+             stream=None, raise_on_nonconvergence: bool = True):
+        """IC0-PCG solve; x holds the initial guess. Returns (iterations, relative residual)."""
+        c = A.c()
+        it = C.c_int(0)
+        rr = C.c_double(0.0)
+        st = _native.lib().baas_iccg(self._h, C.byref(c), _ptr(b), _ptr(x), tol, maxiter, precision,
+                                     C.byref(it), C.byref(rr), _stream_ptr(stream))
+        if st == 5 and not raise_on_nonconvergence:
+            return it.value, rr.value
+        _native.check(st, "baas_iccg")
+        return it.value, rr.value

@@ -1,0 +1,102 @@
+"""ctypes binding of the in-tree C ABI (include/baas_b200.h).
+
+The library is ``baas_b200/_lib/libbaas_b200.so`` built by :mod:`baas_b200.build`. Importing
+this module never falls back to anything else: if the library is missing, :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libbaas_b200.so"
+_lib = None
+
+BAAS_OK = 0
+STATUS_NAMES = {
+    0: "BAAS_OK",
+    1: "BAAS_ERR_BAD_ARG",
+    2: "BAAS_ERR_CUDA",
+    3: "BAAS_ERR_TIMEOUT",
+    4: "BAAS_ERR_ZERO_PIVOT",
+    5: "BAAS_ERR_NOT_CONVERGED",
+    6: "BAAS_ERR_NO_DEVICE",
+    7: "BAAS_ERR_STATE",
+}
+
+KERNEL_SPTRSV, KERNEL_ICCG, KERNEL_IC0, KERNEL_ILU0 = 0, 1, 2, 3
+PREC_FP64, PREC_FP32_FACTORS = 0, 1
+
+FIELDS = {
+    "ngroups": 0, "nlevels": 1, "ntasks": 2, "group_ptr": 3, "group_set": 4, "level_ptr": 5,
+    "perm_to_orig": 6, "node_to_level": 7, "nthread_per_level": 8, "thread_boundaries": 9,
+    "task_boundaries": 10, "thread_cont_to_orig": 11, "orig_to_thread_cont": 12, "task_ptr": 13,
+    "task_set": 14, "btask_ptr": 15, "btask_set": 16, "cost": 17,
+}
+
+# every symbol include/baas_b200.h declares
+EXPORTS = [
+    "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
+    "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
+    "baas_version",
+]
+
+
+class BaasCsr(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz", C.c_int), ("rowptr", C.c_void_p), ("colidx", C.c_void_p),
+                ("values", C.c_void_p)]
+
+
+class BaasOptions(C.Structure):
+    _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("block_size", C.c_int),
+                ("ctas_per_sm", C.c_int)]
+
+
+class BaasError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str):
+        self.status = status
+        self.status_name = STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{where}: {self.status_name}: {detail}")
+
+
+def lib_path() -> Path:
+    return _LIB_PATH
+
+
+def lib():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise RuntimeError(f"{_LIB_PATH} is missing: run `python -m baas_b200.build` (no CPU fallback exists)")
+    L = C.CDLL(str(_LIB_PATH))
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.baas_options_default.argtypes = [C.POINTER(BaasOptions)]
+    L.baas_options_default.restype = None
+    L.baas_analyze.argtypes = [C.POINTER(BaasCsr), i, C.POINTER(BaasOptions), C.POINTER(vp)]
+    L.baas_analyze.restype = i
+    L.baas_schedule_export.argtypes = [vp, i, vp]
+    L.baas_schedule_export.restype = i
+    L.baas_schedule_analysis_ms.argtypes = [vp]
+    L.baas_schedule_analysis_ms.restype = d
+    L.baas_destroy.argtypes = [vp]
+    L.baas_destroy.restype = None
+    L.baas_sptrsv.argtypes = [vp, C.POINTER(BaasCsr), i, vp, vp, i, i, vp]
+    L.baas_sptrsv.restype = i
+    L.baas_ic0.argtypes = [vp, C.POINTER(BaasCsr), vp, vp]
+    L.baas_ic0.restype = i
+    L.baas_ilu0.argtypes = [vp, C.POINTER(BaasCsr), vp, vp]
+    L.baas_ilu0.restype = i
+    L.baas_iccg.argtypes = [vp, C.POINTER(BaasCsr), vp, vp, d, i, i, C.POINTER(C.c_int), C.POINTER(C.c_double), vp]
+    L.baas_iccg.restype = i
+    L.baas_last_error_string.argtypes = []
+    L.baas_last_error_string.restype = C.c_char_p
+    L.baas_version.argtypes = []
+    L.baas_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def check(status: int, where: str) -> None:
+    if status != BAAS_OK:
+        raise BaasError(status, where, lib().baas_last_error_string().decode())

@@ -1,0 +1,177 @@
+// Device helpers shared by the sparse kernels: memory-model-explicit loads and stores, the
+// "not yet written" sentinel used by the sweeps, bounded waits, a bounded grid barrier and a
+// deterministic block reduction.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace baas {
+
+// Status words written by kernels (mirrors baas_status).
+enum : int { kOk = 0, kTimeout = 3, kZeroPivot = 4 };
+
+struct DevStatus {
+    int code;        // first error (kOk if none)
+    int zero_pivots; // count of non-positive IC0 / zero ILU0 pivots
+    int where;       // row or barrier index where a wait gave up
+    int pad;
+};
+
+// --- relaxed / acquire / release accesses at GPU scope (PTX memory model) ---
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const void *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const void *p) {
+    unsigned int v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(void *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_u32(void *p, unsigned int v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_acquire_s32(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_s32(int *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned int atom_add_release_u32(unsigned int *p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// --- sentinels: signalling-NaN bit patterns. Arithmetic never produces a signalling NaN
+// (results of NaN inputs are quiet), so a solution slot holding the sentinel has not been
+// written yet. The value itself is the ready flag: one load both waits and fetches. ---
+constexpr unsigned long long kSent64 = 0xFFF0DEADBEEF0001ull;
+constexpr unsigned int kSent32 = 0xFF80DEADu;
+
+template <typename T> struct Sent;
+template <> struct Sent<double> {
+    static __device__ __forceinline__ bool is(double v) { return (unsigned long long)__double_as_longlong(v) == kSent64; }
+    static __device__ __forceinline__ double value() { return __longlong_as_double((long long)kSent64); }
+    static __device__ __forceinline__ double load(const double *p) { return __longlong_as_double((long long)ld_relaxed_u64(p)); }
+    static __device__ __forceinline__ void store(double *p, double v) { st_relaxed_u64(p, (unsigned long long)__double_as_longlong(v)); }
+};
+template <> struct Sent<float> {
+    static __device__ __forceinline__ bool is(float v) { return __float_as_uint(v) == kSent32; }
+    static __device__ __forceinline__ float value() { return __uint_as_float(kSent32); }
+    static __device__ __forceinline__ float load(const float *p) { return __uint_as_float(ld_relaxed_u32(p)); }
+    static __device__ __forceinline__ void store(float *p, float v) { st_relaxed_u32(p, __float_as_uint(v)); }
+};
+
+// Bounded wait bookkeeping. Every 128 polls the wait also looks at the shared status word so
+// that one failure ends every waiting thread promptly. Returns false when the caller must stop.
+struct Waiter {
+    unsigned int polls;
+    unsigned int limit;
+    DevStatus *st;
+    __device__ __forceinline__ Waiter(unsigned int lim, DevStatus *s) : polls(0), limit(lim), st(s) {}
+    __device__ __forceinline__ bool tick(int where) {
+        ++polls;
+        if ((polls & 127u) == 0u) {
+            if (ld_relaxed_u32(&st->code) != 0u) return false;
+            if (polls >= limit) {
+                if (atomicCAS(&st->code, kOk, kTimeout) == kOk) st->where = where;
+                return false;
+            }
+        }
+        return true;
+    }
+};
+
+// Wait until *p no longer holds the sentinel; returns false if the wait was abandoned.
+template <typename T>
+__device__ __forceinline__ bool wait_value(const T *p, T &out, Waiter &w, int where) {
+    T v = Sent<T>::load(p);
+    while (Sent<T>::is(v)) {
+        if (!w.tick(where)) return false;
+        v = Sent<T>::load(p);
+    }
+    out = v;
+    return true;
+}
+
+// Wait until an epoch-stamped ready flag reaches `epoch` (acquire).
+__device__ __forceinline__ bool wait_flag(const int *flag, int epoch, Waiter &w, int where) {
+    while (ld_acquire_s32(flag) != epoch) {
+        if (!w.tick(where)) return false;
+    }
+    return true;
+}
+
+// Grid barrier over all CTAs of a co-resident (cooperative) launch. `counter` starts at 0 for
+// the launch and only grows; barrier number k (0-based) completes when it reaches
+// (k+1)*gridDim.x. The wait is bounded. Returns false -- uniformly for the whole CTA -- when
+// the wait gave up or the status word carries an error, so every CTA leaves at the same
+// barrier or, at the latest, at the next one.
+__device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int &k, DevStatus *st, unsigned int limit) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int target = (k + 1) * gridDim.x;
+        __threadfence();
+        atom_add_release_u32(counter, 1u);
+        Waiter w(limit, st);
+        int ok = 1;
+        while (ld_acquire_u32(counter) < target) {
+            if (!w.tick(-1 - (int)k)) {
+                ok = 0;
+                break;
+            }
+        }
+        __threadfence();
+        if (ld_relaxed_u32(&st->code) != 0u) ok = 0;
+        s_ok = ok;
+    }
+    ++k;
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Deterministic sum over the block (fixed shuffle tree, fixed warp order). All threads
+// receive the result.
+template <int BLOCK>
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double s_part[BLOCK / 32];
+    __shared__ double s_total;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) s_part[wid] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < BLOCK / 32; i++) t += s_part[i];
+        s_total = t;
+    }
+    __syncthreads();
+    double r = s_total;
+    __syncthreads();
+    return r;
+}
+
+// Every CTA sums the per-CTA partials in CTA order and gets the bitwise-same value.
+template <int BLOCK>
+__device__ __forceinline__ double grid_total(const double *partials, int nparts) {
+    double v = 0.0;
+    // each thread sums a strided subset in a fixed order, then a fixed block tree
+    for (int i = threadIdx.x; i < nparts; i += BLOCK) v += Sent<double>::load(partials + i);
+    return block_sum<BLOCK>(v);
+}
+
+}  // namespace baas

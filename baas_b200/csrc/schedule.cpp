@@ -1,0 +1,618 @@
+// Host-side BAAS schedule (see schedule.hpp for the stage list and reference citations).
+//
+// Data structures are flat CSR-like vectors; the reference's std::list queues become FIFO
+// vectors with a read cursor (same visiting order). Where the reference's output depends on
+// the library's algorithm choice (std::nth_element tie order, merge/LevelTask.cpp:2482) the
+// same standard-library call is made on the same inputs.
+#include "schedule.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <numeric>
+
+namespace baas {
+namespace {
+
+// Tuning constants of the four-rule mapper, merge/include/MergeMarco.hpp:5-23.
+constexpr int kLevelWindow = 6;
+constexpr double kAmplify = 2.0;
+constexpr double kOverGamma = 6.0;
+constexpr double kAwardAlpha = 1.0;
+constexpr double kLoadBeta = 0.1;
+
+struct Csx {  // compressed sparse rows or columns
+    std::vector<int> ptr, idx;
+    int n() const { return (int)ptr.size() - 1; }
+    int len(int i) const { return ptr[i + 1] - ptr[i]; }
+};
+
+// Transpose of an n x n pattern. Entries are scattered in increasing source order, so every
+// output row comes out ascending -- what DAG::inverseDAG's per-row quicksort and dcsr2csc's
+// per-column quicksort produce for duplicate-free rows (spm/DAG.cpp:481-564, spm/CSR.cpp:914-950).
+Csx transpose(const Csx &a) {
+    const int n = a.n();
+    Csx t;
+    t.ptr.assign(n + 1, 0);
+    t.idx.resize(a.idx.size());
+    for (int v : a.idx) t.ptr[v + 1]++;
+    for (int i = 0; i < n; i++) t.ptr[i + 1] += t.ptr[i];
+    std::vector<int> cur(t.ptr.begin(), t.ptr.end() - 1);
+    for (int i = 0; i < n; i++)
+        for (int e = a.ptr[i]; e < a.ptr[i + 1]; e++) t.idx[cur[a.idx[e]]++] = i;
+    return t;
+}
+
+// Stage 2: drop edge i->j when a child k of i also has j as a child (one hop through the
+// unpruned DAG). Column i's own entry (first, the diagonal) is never dropped.
+Csx two_hop_reduce(const Csx &dag) {
+    const int n = dag.n();
+    std::vector<uint8_t> dead(dag.idx.size(), 0);
+    for (int i = 0; i < n; i++) {
+        const int cb = dag.ptr[i] + 1, ce = dag.ptr[i + 1];
+        if (ce - cb < 2) continue;  // a single child cannot be reached through a sibling
+        const int *kids = dag.idx.data() + cb;
+        const int nk = ce - cb;
+        for (int a = 0; a < nk; a++) {
+            const int k = kids[a];
+            for (int e = dag.ptr[k] + 1; e < dag.ptr[k + 1]; e++) {
+                const int j = dag.idx[e];
+                const int *hit = std::lower_bound(kids, kids + nk, j);
+                if (hit != kids + nk && *hit == j) dead[cb + (hit - kids)] = 1;
+            }
+        }
+    }
+    Csx out;
+    out.ptr.assign(n + 1, 0);
+    out.idx.reserve(dag.idx.size());
+    for (int i = 0; i < n; i++) {
+        for (int e = dag.ptr[i]; e < dag.ptr[i + 1]; e++)
+            if (!dead[e]) out.idx.push_back(dag.idx[e]);
+        out.ptr[i + 1] = (int)out.idx.size();
+    }
+    return out;
+}
+
+struct Grouping {
+    int ngroups = 0;
+    std::vector<int> ptr, set;
+};
+
+// Counting-sort relabel of BFS groups by a representative node (max for reverse trees, min for
+// forward trees); nodes keep their BFS order inside a group (merge/Coarsen.cpp:345-398, :176-224).
+void relabel_groups(int n, Grouping &g, bool by_max) {
+    std::vector<int> gid(n, 0), cnt(n + 1, 0);
+    for (int k = 0; k < g.ngroups; k++) {
+        int id = by_max ? 0 : n;
+        for (int e = g.ptr[k]; e < g.ptr[k + 1]; e++) {
+            const int v = g.set[e];
+            if (by_max ? (v > id) : (v < id)) id = v;
+        }
+        cnt[id + 1] = g.ptr[k + 1] - g.ptr[k];
+        for (int e = g.ptr[k]; e < g.ptr[k + 1]; e++) gid[g.set[e]] = id;
+    }
+    for (int i = 1; i < n; i++) cnt[i + 1] += cnt[i];
+    std::vector<int> ptr;
+    ptr.reserve(g.ngroups + 1);
+    ptr.push_back(0);
+    for (int i = 0; i < n; i++)
+        if (cnt[i + 1] != cnt[i]) ptr.push_back(cnt[i + 1]);
+    std::vector<int> set(n);
+    for (int i = 0; i < n; i++) set[cnt[gid[g.set[i]]]++] = g.set[i];
+    g.ptr.swap(ptr);
+    g.set.swap(set);
+}
+
+// Stages 3 and 5: BFS tree coarsening. `reverse` grows groups from sinks towards parents that
+// have exactly one child; otherwise from sources towards children that have exactly one parent.
+Grouping tree_coarsen(const Csx &dag, bool reverse) {
+    const int n = dag.n();
+    const Csx inv = transpose(dag);
+    const Csx &up = reverse ? inv : dag;    // where the next tree members come from
+    const Csx &down = reverse ? dag : inv;  // whose length decides "single edge" (self + 1)
+
+    std::vector<int> roots;
+    roots.reserve(n);
+    for (int i = 0; i < n; i++)
+        if ((reverse ? dag.len(i) : inv.len(i)) == 1) roots.push_back(i);
+    size_t rhead = 0;
+
+    Grouping g;
+    g.set.resize(n);
+    g.ptr.reserve(n + 1);
+    std::vector<uint8_t> visited(n, 0);
+    std::vector<int> fifo;
+    fifo.reserve(n);
+    std::vector<int> found;
+    int cnt = 0;
+    while (rhead < roots.size()) {
+        int head = roots[rhead++];
+        visited[head] = 1;
+        fifo.clear();
+        fifo.push_back(head);
+        size_t fhead = 0;
+        g.ptr.push_back(cnt);
+        g.ngroups++;
+        while (fhead < fifo.size()) {
+            head = fifo[fhead++];
+            g.set[cnt++] = head;
+            found.clear();
+            bool tree = true;
+            // parents of head = its inverse row without the trailing self entry; children of
+            // head = its CSC column without the leading self entry
+            const int b = reverse ? up.ptr[head] : up.ptr[head] + 1;
+            const int e = reverse ? up.ptr[head + 1] - 1 : up.ptr[head + 1];
+            for (int q = b; q < e; q++) {
+                const int v = up.idx[q];
+                if (visited[v]) continue;
+                visited[v] = 1;
+                found.push_back(v);
+                if (down.len(v) != 2) tree = false;
+            }
+            if (tree)
+                fifo.insert(fifo.end(), found.begin(), found.end());
+            else
+                roots.insert(roots.end(), found.begin(), found.end());
+        }
+    }
+    if (g.ptr.empty() || g.ptr.back() != cnt) g.ptr.push_back(cnt);
+    relabel_groups(n, g, /*by_max=*/reverse);
+    return g;
+}
+
+// Stage 4: DAG between groups: every child of every member, mapped to its group, sorted, unique.
+Csx group_dag(int n, const Grouping &g, const Csx &dag) {
+    std::vector<int> owner(n);
+    for (int k = 0; k < g.ngroups; k++)
+        for (int e = g.ptr[k]; e < g.ptr[k + 1]; e++) owner[g.set[e]] = k;
+    Csx out;
+    out.ptr.assign(g.ngroups + 1, 0);
+    std::vector<int> tmp;
+    for (int k = 0; k < g.ngroups; k++) {
+        tmp.clear();
+        for (int e = g.ptr[k]; e < g.ptr[k + 1]; e++) {
+            const int v = g.set[e];
+            for (int q = dag.ptr[v]; q < dag.ptr[v + 1]; q++) tmp.push_back(owner[dag.idx[q]]);
+        }
+        std::sort(tmp.begin(), tmp.end());
+        tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+        out.idx.insert(out.idx.end(), tmp.begin(), tmp.end());
+        out.ptr[k + 1] = (int)out.idx.size();
+    }
+    return out;
+}
+
+// Stage 7: Kahn BFS levels where a node is ready at in-degree 1 (its own diagonal entry).
+void level_sets(const Csx &dag, HostSchedule &s) {
+    const int n = dag.n();
+    std::vector<int> indeg(n, 0);
+    for (int v : dag.idx) indeg[v]++;
+    std::vector<int> q(n);
+    int rear = 0;
+    for (int i = 0; i < n; i++)
+        if (indeg[i] == 1) q[rear++] = i;
+    std::vector<int> lptr(n + 1, 0);
+    s.node_to_level.assign(n, 1);
+    int front = 0, lvl = 0;
+    while (front < rear) {
+        const int stop = rear;
+        lvl++;
+        while (front < stop) {
+            const int cur = q[front++];
+            s.node_to_level[cur] = lvl;
+            for (int e = dag.ptr[cur]; e < dag.ptr[cur + 1]; e++) {
+                const int c = dag.idx[e];
+                if (c == cur) continue;
+                if (--indeg[c] == 1) q[rear++] = c;
+            }
+        }
+        lptr[lvl] = front;
+    }
+    s.nlevels = lvl;
+    s.level_ptr.assign(lptr.begin(), lptr.begin() + lvl + 1);
+    for (int l = 0; l < lvl; l++) std::sort(q.begin() + s.level_ptr[l], q.begin() + s.level_ptr[l + 1]);
+    s.perm_to_orig.assign(q.begin(), q.begin() + n);
+    s.perm.assign(n, 0);
+    for (int i = 0; i < n; i++) s.perm[s.perm_to_orig[i]] = i;
+}
+
+// Stage 8: merge/LevelMerge.cpp:118-262.
+void threads_per_level(HostSchedule &s) {
+    const int nl = s.nlevels, nc = s.nthread;
+    s.nthread_per_level.assign(nl, 1);
+    if (nl == 1) {
+        s.nthread_per_level[0] = std::min(s.level_ptr[1] - s.level_ptr[0], nc);
+        return;
+    }
+    for (int l = 0; l < nl; l++) {
+        const int groups = s.level_ptr[l + 1] - s.level_ptr[l];
+        int rows = 0;
+        long long nnz = 0;
+        for (int p = s.level_ptr[l]; p < s.level_ptr[l + 1]; p++) {
+            const int g = s.perm_to_orig[p];
+            rows += s.group_ptr[g + 1] - s.group_ptr[g];
+            if (s.kind == SchedKind::SpTRSV || s.kind == SchedKind::ICCG)
+                for (int e = s.group_ptr[g]; e < s.group_ptr[g + 1]; e++) {
+                    const int r = s.group_set[e];
+                    nnz += s.a_rowptr[r + 1] - s.a_rowptr[r];
+                }
+        }
+        int t;
+        if (s.kind == SchedKind::SpTRSV || s.kind == SchedKind::ICCG) {
+            const int inz = (int)nnz;
+            if (rows < 16 || groups <= 4 || inz < 32) {
+                t = 1;
+            } else {
+                const int avg = (rows + 7) / 8;
+                t = std::min(std::min(std::max(inz / 32, avg), groups), nc);
+            }
+        } else {  // IC0 and ILU0 share one rule
+            if (rows < 4 || groups <= 2) {
+                t = 1;
+            } else {
+                const int avg = (rows + 1) / 2;
+                t = std::min(std::min(avg, groups), nc);
+            }
+        }
+        s.nthread_per_level[l] = t;
+    }
+}
+
+// Stage 9: four-rule mapping of groups to virtual threads, then the merge of consecutive
+// single-thread levels and the conversion to thread/task boundaries.
+//
+// The reference computes the per-thread vote sums inside an OpenMP region whose threads split
+// each level into ceil(width / nthread)-sized node ranges, then the master thread adds the
+// per-range partial sums in range order (merge/LevelTask.cpp:2386-2469). That order is
+// reproduced exactly; all-zero partials are skipped, which cannot change a sum of positive
+// votes.
+void four_rule_map(HostSchedule &s, const Csx &dag_csr) {
+    const int nl = s.nlevels, nt = s.nthread, nodes = s.ngroups;
+    const int *lp = s.level_ptr.data();
+    const int *p2o = s.perm_to_orig.data();
+
+    std::vector<int> by_level_thread(nodes);  // nodeByLevelThreadTask
+    std::vector<int> node_thread(nodes, -1);  // origNodeToThread
+    std::vector<std::pair<int, int>> task_rows((size_t)nl * nt);
+    std::vector<int> level_single(nl, -1);    // levelThreadOne
+
+    // level 0: cost-balanced contiguous split (merge/LevelTask.cpp:2325-2371)
+    {
+        const int et = s.nthread_per_level[0];
+        const int lb = lp[0], le = lp[1];
+        std::vector<double> pre(le - lb + 1);
+        double load = 0.0;
+        for (int i = lb; i < le; i++) {
+            pre[i - lb] = load;
+            load += s.cost[p2o[i]];
+        }
+        const double per = (load + et - 1) / et;
+        int prev_end = lb, r = lb;
+        if (et == 1) level_single[0] = 0;
+        for (int t = 0; t < et; t++) {
+            // lower_bound over [r, le); an empty or inverted range returns r
+            int nr = r;
+            if (r < le) nr = lb + (int)(std::lower_bound(pre.begin() + (r - lb), pre.begin() + (le - lb), (t + 1) * per) - pre.begin());
+            r = nr;
+            const int b = prev_end, e = std::min(r, le);
+            prev_end = e;
+            task_rows[(size_t)t * nl + 0] = {b, e};
+            for (int k = b; k < e; k++) {
+                by_level_thread[k] = p2o[k];
+                node_thread[p2o[k]] = t;
+            }
+            ++r;
+        }
+        for (int t = et; t < nt; t++) task_rows[(size_t)t * nl + 0] = {le, le};
+    }
+
+    std::vector<double> sel(nt), part(nt), penalty(nt), local_load(nt), score(nt);
+    std::vector<int> touched, idx(nt);
+    std::vector<uint8_t> chosen(nt), in_touched(nt);
+    std::vector<std::vector<int>> thread_nodes(nt);
+    // per-node affinity towards each parent thread: (thread, sum) in first-seen order
+    std::vector<int> aff_ptr;
+    std::vector<int> aff_thr;
+    std::vector<double> aff_val, aff_total;
+    const double pen0 = kLoadBeta * std::log(1.0 + (1.0 - 0.0));
+
+    for (int lvl = 1; lvl < nl; lvl++) {
+        const int lb = lp[lvl], le = lp[lvl + 1];
+        const int et = s.nthread_per_level[lvl];
+        const int width = le - lb;
+        std::fill(sel.begin(), sel.end(), 0.0);
+        std::fill(penalty.begin(), penalty.end(), pen0);
+        std::fill(local_load.begin(), local_load.end(), 0.0);
+        for (int t = 0; t < nt; t++) {
+            idx[t] = t;
+            thread_nodes[t].clear();
+        }
+
+        // votes, split into the reference's per-OpenMP-thread node ranges
+        const int chunk = (width + nt - 1) / nt;
+        aff_ptr.assign(width + 1, 0);
+        aff_thr.clear();
+        aff_val.clear();
+        aff_total.assign(width, 0.0);
+        double level_load = 0.0;
+        for (int tid = 0; tid < nt; tid++) {
+            const int rb = std::min(lb + chunk * tid, le);
+            const int re = std::min(lb + chunk * (tid + 1), le);
+            if (rb >= re) continue;
+            touched.clear();
+            for (int i = rb; i < re; i++) {
+                const int node = p2o[i];
+                const int nlev = s.node_to_level[node];
+                level_load += s.cost[node];
+                const int abeg = (int)aff_thr.size();
+                for (int q = dag_csr.ptr[node]; q < dag_csr.ptr[node + 1] - 1; q++) {
+                    const int par = dag_csr.idx[q];
+                    const int rt = node_thread[par];
+                    const int diff = nlev - s.node_to_level[par];
+                    if (diff > kLevelWindow) continue;
+                    const double vote = kAmplify * std::log2(1.0 * (s.group_ptr[par + 1] - s.group_ptr[par] + 1)) /
+                                        std::log2(diff + 1);
+                    if (!in_touched[rt]) {
+                        in_touched[rt] = 1;
+                        part[rt] = 0.0;
+                        touched.push_back(rt);
+                    }
+                    part[rt] += vote;
+                    aff_total[i - lb] += vote;
+                    int a = abeg;
+                    while (a < (int)aff_thr.size() && aff_thr[a] != rt) a++;
+                    if (a == (int)aff_thr.size()) {
+                        aff_thr.push_back(rt);
+                        aff_val.push_back(0.0);
+                    }
+                    aff_val[a] += vote;
+                }
+                aff_ptr[i - lb + 1] = (int)aff_thr.size();
+            }
+            for (int t : touched) {
+                sel[t] += part[t];
+                in_touched[t] = 0;
+            }
+        }
+        // level_load is a sum of integer-valued costs, exact in any order
+        const double avg = level_load / et;
+
+        std::nth_element(idx.begin(), idx.begin() + et, idx.end(),
+                         [&sel](int a, int b) { return sel[a] > sel[b]; });
+        if (et == 1) level_single[lvl] = idx[0];
+        std::fill(chosen.begin(), chosen.end(), 0);
+        for (int k = 0; k < et; k++) chosen[idx[k]] = 1;
+
+        for (int i = lb; i < le; i++) {
+            const int node = p2o[i];
+            const double total = aff_total[i - lb];
+            const int ab = aff_ptr[i - lb], ae = aff_ptr[i - lb + 1];
+            double best = std::numeric_limits<double>::lowest();
+            int target = -1;
+            for (int t = 0; t < nt; t++) {
+                if (!chosen[t]) continue;
+                double a = 0.0;
+                for (int q = ab; q < ae; q++)
+                    if (aff_thr[q] == t) {
+                        a = aff_val[q];
+                        break;
+                    }
+                score[t] = kAwardAlpha * (a / total) + penalty[t];
+                if (score[t] > best) {
+                    best = score[t];
+                    target = t;
+                }
+            }
+            thread_nodes[target].push_back(node);
+            local_load[target] += s.cost[node];
+            const double util = local_load[target] / avg;
+            double pen;
+            if (util < 1.0)
+                pen = kLoadBeta * std::log(1.0 + (1.0 - util));
+            else if (util > 1.05)
+                pen = std::numeric_limits<double>::lowest();
+            else
+                pen = -kOverGamma * (std::exp(10 * (util - 1)) - 1);
+            penalty[target] = pen;
+        }
+
+        int pos = lb;
+        for (int t = 0; t < nt; t++) {
+            auto &tr = task_rows[(size_t)t * nl + lvl];
+            if (chosen[t]) {
+                tr = {pos, pos + (int)thread_nodes[t].size()};
+                for (int v : thread_nodes[t]) {
+                    by_level_thread[pos++] = v;
+                    node_thread[v] = t;
+                }
+            } else {
+                tr = {pos, pos};
+            }
+        }
+    }
+
+    // merge runs of single-thread levels into the run's first task (merge/LevelTask.cpp:2646-2676)
+    {
+        std::vector<int> run_start(nl + 1, 0), ntpl(s.nthread_per_level);
+        int m = 0;
+        for (int lvl = 1; lvl < nl;) {
+            if (ntpl[lvl] == 1 && ntpl[m] == 1) {
+                auto &pre = task_rows[(size_t)level_single[m] * nl + run_start[m]];
+                auto &post = task_rows[(size_t)level_single[lvl] * nl + lvl];
+                pre.second = post.second;
+                post = {0, 0};
+                lvl++;
+            } else {
+                m++;
+                ntpl[m] = ntpl[lvl];
+                level_single[m] = level_single[lvl];
+                run_start[m] = lvl;
+                lvl++;
+            }
+        }
+    }
+
+    // taskMapToBoundaries, non-barrier form (merge/LevelTask.cpp:198-304)
+    std::vector<int> rows_before(nt + 1, 0);
+    s.thread_boundaries.assign(nt + 1, 0);
+    for (int t = 0; t < nt; t++) {
+        int sum = 0, cnt = 0;
+        for (int l = 0; l < nl; l++) {
+            const auto &tr = task_rows[(size_t)t * nl + l];
+            const int d = tr.second - tr.first;
+            sum += d;
+            if (d) ++cnt;
+        }
+        rows_before[t + 1] = sum;
+        s.thread_boundaries[t + 1] = cnt;
+    }
+    for (int t = 0; t < nt; t++) {
+        rows_before[t + 1] += rows_before[t];
+        s.thread_boundaries[t + 1] += s.thread_boundaries[t];
+    }
+    s.ntasks = s.thread_boundaries[nt];
+    s.task_boundaries.assign(s.ntasks + 1, 0);
+    s.orig_to_thread_cont.assign(nodes, 0);
+    s.thread_cont_to_orig.assign(nodes, 0);
+    for (int t = 0; t < nt; t++) {
+        int row = rows_before[t], task = s.thread_boundaries[t];
+        for (int l = 0; l < nl; l++) {
+            const auto &tr = task_rows[(size_t)t * nl + l];
+            if (tr.second > tr.first) {
+                s.task_boundaries[task++] = row;
+                for (int j = tr.first; j < tr.second; j++) {
+                    s.orig_to_thread_cont[by_level_thread[j]] = row;
+                    s.thread_cont_to_orig[row] = by_level_thread[j];
+                    row++;
+                }
+            }
+        }
+    }
+    s.task_boundaries[s.ntasks] = nodes;
+}
+
+// Stage 10: for every task, the sorted set of tasks on other threads that own a parent group.
+void task_dags(HostSchedule &s, const Csx &dag_csr) {
+    const int nt = s.nthread, ntask = s.ntasks;
+    std::vector<int> owner(s.ngroups);
+    for (int t = 0; t < ntask; t++)
+        for (int r = s.task_boundaries[t]; r < s.task_boundaries[t + 1]; r++) owner[s.thread_cont_to_orig[r]] = t;
+    s.task_ptr.assign(ntask + 1, 0);
+    s.task_set.clear();
+    std::vector<int> dep;
+    for (int th = 0; th < nt; th++) {
+        const int tb = s.thread_boundaries[th], te = s.thread_boundaries[th + 1];
+        for (int t = tb; t < te; t++) {
+            dep.clear();
+            for (int r = s.task_boundaries[t]; r < s.task_boundaries[t + 1]; r++) {
+                const int g = s.thread_cont_to_orig[r];
+                for (int q = dag_csr.ptr[g]; q < dag_csr.ptr[g + 1]; q++) {
+                    const int v = owner[dag_csr.idx[q]];
+                    if (v < tb || v >= te) dep.push_back(v);
+                }
+            }
+            std::sort(dep.begin(), dep.end());
+            dep.erase(std::unique(dep.begin(), dep.end()), dep.end());
+            s.task_set.insert(s.task_set.end(), dep.begin(), dep.end());
+            s.task_ptr[t + 1] = (int)s.task_set.size();
+        }
+    }
+    Csx td{s.task_ptr, s.task_set};
+    Csx bt = transpose(td);
+    s.btask_ptr = std::move(bt.ptr);
+    s.btask_set = std::move(bt.idx);
+}
+
+}  // namespace
+
+const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedKind kind) {
+    if (n <= 0) return "n must be positive";
+    if (!rowptr || !colidx) return "rowptr/colidx must not be NULL";
+    if (rowptr[0] != 0) return "rowptr[0] must be 0 (0-based CSR)";
+    for (int i = 0; i < n; i++) {
+        if (rowptr[i + 1] < rowptr[i]) return "rowptr must be non-decreasing";
+        bool diag = false;
+        for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
+            const int c = colidx[e];
+            if (c < 0 || c >= n) return "column index out of range";
+            if (e > rowptr[i] && colidx[e - 1] >= c) return "column indices must be strictly ascending in each row";
+            if (c == i) diag = true;
+            if (kind == SchedKind::SpTRSV && c > i) return "SpTRSV analysis takes the lower triangle only";
+        }
+        if (!diag) return "every row needs its diagonal entry";
+    }
+    return "";
+}
+
+void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread) {
+    auto t0 = std::chrono::steady_clock::now();
+    s = HostSchedule();
+    s.kind = kind;
+    s.n = n;
+    s.nthread = nthread;
+    const int nnz = rowptr[n];
+    s.a_rowptr.assign(rowptr, rowptr + n + 1);
+    s.a_colidx.assign(colidx, colidx + nnz);
+    s.a_diagptr.assign(n, 0);
+    for (int i = 0; i < n; i++) {
+        int e = rowptr[i];
+        while (e < rowptr[i + 1] && colidx[e] < i) e++;
+        s.a_diagptr[i] = e;
+    }
+
+    // Stage 1: lower triangle incl. diagonal (test/Schedule.hpp:134-154) and its CSC
+    s.l_rowptr.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) s.l_rowptr[i + 1] = s.l_rowptr[i] + s.a_diagptr[i] - rowptr[i] + 1;
+    s.l_colidx.resize(s.l_rowptr[n]);
+    s.l_src.resize(s.l_rowptr[n]);
+    for (int i = 0; i < n; i++)
+        for (int e = rowptr[i]; e <= s.a_diagptr[i]; e++) {
+            s.l_colidx[s.l_rowptr[i] + e - rowptr[i]] = colidx[e];
+            s.l_src[s.l_rowptr[i] + e - rowptr[i]] = e;
+        }
+    Csx lower{s.l_rowptr, s.l_colidx};
+    Csx dag0 = transpose(lower);  // column j: j itself, then the rows that depend on j
+
+    Csx dag = two_hop_reduce(dag0);                   // stage 2
+    Grouping rev = tree_coarsen(dag, true);           // stage 3
+    Csx gdag = group_dag(n, rev, dag);                // stage 4
+    Grouping fwd = tree_coarsen(gdag, false);         // stage 5
+    // remap forward groups (of reverse groups) onto rows (merge/Coarsen.cpp:896-928)
+    s.ngroups = fwd.ngroups;
+    s.group_ptr.assign(1, 0);
+    s.group_ptr.reserve(fwd.ngroups + 1);
+    s.group_set.clear();
+    s.group_set.reserve(n);
+    for (int f = 0; f < fwd.ngroups; f++) {
+        for (int q = fwd.ptr[f]; q < fwd.ptr[f + 1]; q++) {
+            const int g = fwd.set[q];
+            s.group_set.insert(s.group_set.end(), rev.set.begin() + rev.ptr[g], rev.set.begin() + rev.ptr[g + 1]);
+        }
+        s.group_ptr.push_back((int)s.group_set.size());
+    }
+    Csx fdag = group_dag(rev.ngroups, fwd, gdag);
+
+    // Stage 6: cost = rows' lower-triangle lengths summed over the group (merge/Coarsen.cpp:854-891)
+    s.cost.assign(s.ngroups, 0.0);
+    for (int g = 0; g < s.ngroups; g++)
+        for (int e = s.group_ptr[g]; e < s.group_ptr[g + 1]; e++) {
+            const int r = s.group_set[e];
+            s.cost[g] += 1 * (s.l_rowptr[r + 1] - s.l_rowptr[r]);
+        }
+
+    level_sets(fdag, s);       // stage 7
+    threads_per_level(s);      // stage 8
+    for (int g = 0; g < s.ngroups; g++)  // test/Schedule.hpp:72-79
+        std::sort(s.group_set.begin() + s.group_ptr[g], s.group_set.begin() + s.group_ptr[g + 1]);
+    Csx dag_csr = transpose(fdag);  // parents of each group, then the group itself
+    four_rule_map(s, dag_csr);      // stage 9
+    task_dags(s, dag_csr);          // stage 10
+    s.fdag_ptr = std::move(fdag.ptr);
+    s.fdag_set = std::move(fdag.idx);
+    auto t1 = std::chrono::steady_clock::now();
+    s.analysis_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+}  // namespace baas

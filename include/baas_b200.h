@@ -1,0 +1,172 @@
+/*
+ * baas_b200.h -- C ABI of the B200-native BAAS sparse hot path.
+ *
+ * The path is the one the reference drives from pcg_opt (test/iccg_level_merge.cpp:380-533):
+ * schedule construction (transitive reduction, bidirectional tree coarsening, level sets,
+ * per-level thread counts, four-rule affinity mapping, task DAG), then IC0 / ILU0 and the
+ * forward / backward triangular sweeps driven by that schedule, then the ICCG loop.
+ *
+ * Conventions
+ *  - Every function returns a baas_status; nothing aborts the process.
+ *  - Indices are int32, values FP64 (as in the reference's SPM::CSR, spm/include/CSR.hpp:16-31).
+ *  - baas_analyze works on HOST arrays and needs no GPU. Every other compute call takes CUDA
+ *    DEVICE pointers owned by the caller and a cudaStream_t passed as `void *stream`
+ *    (NULL = legacy default stream). Calls are stream-ordered; a call returns after its work
+ *    is enqueued unless it has to read a status or a scalar back (it then synchronises that
+ *    stream and says so below).
+ *  - A baas_schedule owns all of its host and device memory. It is not re-entrant: calls on
+ *    one schedule must not overlap in time (the reference's single taskFinsished array per
+ *    schedule has the same restriction, merge/include/LevelTask.hpp:177).
+ *  - Device waits are bounded: a wait that exceeds baas_options.spin_limit polls ends the
+ *    kernel with BAAS_ERR_TIMEOUT instead of hanging (the reference spins forever,
+ *    merge/include/SpTRSV.hpp:16-23).
+ */
+#ifndef BAAS_B200_H
+#define BAAS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum baas_status {
+    BAAS_OK = 0,
+    BAAS_ERR_BAD_ARG = 1,       /* NULL pointer, size mismatch, pattern the path cannot take */
+    BAAS_ERR_CUDA = 2,          /* a CUDA runtime call failed (see baas_last_error_string) */
+    BAAS_ERR_TIMEOUT = 3,       /* a bounded device wait ran out (schedule or input is inconsistent) */
+    BAAS_ERR_ZERO_PIVOT = 4,    /* IC0 met a pivot <= 0 (left unchanged, as merge/IC.cpp:371-378 does)
+                                   or ILU0 met a zero pivot; the factor is still written */
+    BAAS_ERR_NOT_CONVERGED = 5, /* ICCG hit maxiter before the tolerance */
+    BAAS_ERR_NO_DEVICE = 6,     /* the compute call needs a CUDA device and none is usable */
+    BAAS_ERR_STATE = 7          /* call order violated (e.g. a sweep before the factor exists) */
+} baas_status;
+
+/* Which reference driver's schedule to reproduce. */
+typedef enum baas_kernel {
+    /* SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule (test/SpTRSVRuntime.hpp:617-852): the input
+     * is the lower triangle L (diagonal last in each row); level thread counts from
+     * level_nthreads_group_TRSV over L (merge/LevelMerge.cpp:164-200). */
+    BAAS_KERNEL_SPTRSV = 0,
+    /* Schedule::Scheduler(A, isSymmetric=true, isTRSVPerm=false, P2P_RULE, nthread)
+     * (test/Schedule.hpp:117-296): the input is the full SPD matrix A; thread counts from
+     * level_nthreads_group_TRSV over the FULL A (test/Schedule.hpp:248); also builds the
+     * backward (inverse) task schedule. Used by ICCG. */
+    BAAS_KERNEL_ICCG = 1,
+    /* IC_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule (test/ICRuntime.hpp:353-583). */
+    BAAS_KERNEL_IC0 = 2,
+    /* ILU_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule (test/ILURuntime.hpp:207-436); the pattern
+     * must be structurally symmetric, as the reference assumes. */
+    BAAS_KERNEL_ILU0 = 3
+} baas_kernel;
+
+/* Schedule arrays exported for parity checks (names of the reference's members). */
+typedef enum baas_field {
+    BAAS_FIELD_NGROUPS = 0,            /* scalar: groups after both coarsenings */
+    BAAS_FIELD_NLEVELS = 1,            /* scalar: levels of the group DAG */
+    BAAS_FIELD_NTASKS = 2,             /* scalar */
+    BAAS_FIELD_GROUP_PTR = 3,          /* group_ptr[ngroups+1] */
+    BAAS_FIELD_GROUP_SET = 4,          /* group_set[n], rows ascending within a group */
+    BAAS_FIELD_LEVEL_PTR = 5,          /* LevelSet::level_ptr[nlevels+1] */
+    BAAS_FIELD_PERM_TO_ORIG = 6,       /* LevelSet::permToOrig[ngroups] */
+    BAAS_FIELD_NODE_TO_LEVEL = 7,      /* LevelSet::nodeToLevel[ngroups], 1-based */
+    BAAS_FIELD_NTHREAD_PER_LEVEL = 8,  /* nthread_per_level[nlevels] */
+    BAAS_FIELD_THREAD_BOUNDARIES = 9,  /* Task::threadBoundaries[nthread+1] */
+    BAAS_FIELD_TASK_BOUNDARIES = 10,   /* Task::taskBoundaries[ntasks+1] */
+    BAAS_FIELD_THREAD_CONT_TO_ORIG = 11, /* Task::threadContToOrigPerm[ngroups] */
+    BAAS_FIELD_ORIG_TO_THREAD_CONT = 12, /* Task::origToThreadContPerm[ngroups] */
+    BAAS_FIELD_TASK_PTR = 13,          /* task DAG (parents), CSR ptr[ntasks+1] */
+    BAAS_FIELD_TASK_SET = 14,          /* task DAG parents */
+    BAAS_FIELD_BTASK_PTR = 15,         /* backward (inverse) task DAG ptr[ntasks+1] */
+    BAAS_FIELD_BTASK_SET = 16,         /* backward parents */
+    BAAS_FIELD_COST = 17               /* Coarsen::costComputation cost[ngroups] (integer-valued) */
+} baas_field;
+
+typedef enum baas_precision {
+    BAAS_PREC_FP64 = 0,           /* factors and sweeps in FP64 */
+    BAAS_PREC_FP32_FACTORS = 1    /* factor computed in FP64, stored and applied in FP32 with FP32
+                                     accumulation; CG recurrence and dots stay FP64 */
+} baas_precision;
+
+/* CSR matrix, 0-based, column indices strictly ascending in each row. For baas_analyze the
+ * arrays are host memory; for the compute calls they are device memory. `values` may be NULL
+ * for baas_analyze. */
+typedef struct baas_csr {
+    int n;               /* rows == columns */
+    int nnz;             /* rowptr[n] */
+    const int *rowptr;   /* n + 1 */
+    const int *colidx;   /* nnz */
+    const double *values;/* nnz */
+} baas_csr;
+
+typedef struct baas_options {
+    int nthread;      /* the reference's num_thread: virtual threads of the schedule (>= 1) */
+    int spin_limit;   /* polls before a device wait gives up (0 = library default) */
+    int block_size;   /* threads per CTA of the persistent kernels (0 = library default) */
+    int ctas_per_sm;  /* persistent CTAs per SM (0 = as many as are co-resident) */
+} baas_options;
+
+typedef struct baas_schedule baas_schedule;
+
+/* Fills *opt with the defaults (nthread = 8, library-chosen GPU parameters). */
+void baas_options_default(baas_options *opt);
+
+/* Builds the reference-identical BAAS schedule for `kind` from A's pattern (host arrays),
+ * plus this library's device execution plan (uploaded on first GPU use). Replaces
+ * Scheduler::Scheduler + Scheduler::preprocessing (test/Schedule.hpp:117-155, 181-296) and the
+ * runtime classes' buildset() (test/SpTRSVRuntime.hpp:675-775, test/ICRuntime.hpp:408-520,
+ * test/ILURuntime.hpp:265-385). Needs no GPU. */
+baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options *opt, baas_schedule **out);
+
+/* Copies schedule array `field` into out (if out != NULL) and returns its length (-1 for an
+ * unknown field). Host only. */
+int baas_schedule_export(const baas_schedule *s, int field, int *out);
+
+/* Wall time of baas_analyze in milliseconds (the reference's Scheduling_Time,
+ * test/SpTRSV_level_merge.cpp:70). */
+double baas_schedule_analysis_ms(const baas_schedule *s);
+
+/* Frees the schedule and its device memory. */
+void baas_destroy(baas_schedule *s);
+
+/* Forward sweep x = L^-1 b (upper = 0; L is the analysed lower triangle, diagonal LAST in each
+ * row) or backward sweep x = U^-1 b (upper = 1; U has the transposed pattern, diagonal FIRST).
+ * Replaces Scheduler::runForwardTRSVNoPerm / runBackwardTRSVNoPerm (test/Schedule.hpp:332-347),
+ * i.e. sptrsv_p2p_csr_group_merge_no_perm_alloc (merge/SpTRSV.cpp:421-478) and
+ * sptrsv_backward_p2p_csr_group_merge_no_perm_alloc (:601-660); results are bit-identical to
+ * them. b and x hold nrhs column-major right-hand sides with leading dimension ldb >= n;
+ * x must not alias b. Synchronises `stream` to read the status. */
+baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const double *b, double *x,
+                        int nrhs, int ldb, void *stream);
+
+/* IC0 in place on lu (device, pre-filled with A.values), A the analysed full SPD matrix.
+ * Replaces Scheduler::runIC0 (test/Schedule.hpp:316-322) =
+ * spic0_csr_uL_p2p_group_merge_no_perm (merge/IC.cpp:296-393); bit-identical factor.
+ * Synchronises `stream` to read the status. */
+baas_status baas_ic0(baas_schedule *s, const baas_csr *A, double *lu, void *stream);
+
+/* ILU0 in place on lu (device, pre-filled with A.values). Replaces
+ * ilu0_p2p_csr_group_merge_no_perm_alloc (merge/ILU.cpp:638-720); bit-identical factor.
+ * Synchronises `stream` to read the status. */
+baas_status baas_ilu0(baas_schedule *s, const baas_csr *A, double *lu, void *stream);
+
+/* IC0-preconditioned CG on A x = b (device arrays; x holds the initial guess and receives the
+ * solution), stopping once ||r_k|| / ||r_0|| < tol or after maxiter iterations. One persistent
+ * kernel runs the factorisation and the whole iteration loop. Follows pcg_opt
+ * (test/iccg_level_merge.cpp:380-533) with a break at tol. Writes the iteration count and the
+ * final relative residual; synchronises `stream`. Requires a schedule of kind
+ * BAAS_KERNEL_ICCG. */
+baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, double *x, double tol,
+                      int maxiter, int precision, int *iters, double *relres, void *stream);
+
+/* Human-readable text for the last error on this thread (never NULL). */
+const char *baas_last_error_string(void);
+
+/* Library version string. */
+const char *baas_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BAAS_B200_H */

@@ -1,0 +1,222 @@
+"""ctypes access to the two checkers -- TEST INFRASTRUCTURE ONLY.
+
+* :class:`Ref` -- the reference itself, compiled from its own sources into
+  ``oracle/_ref/libbaas_ref.so`` by ``oracle/Makefile`` (present wherever that library was
+  built; the reference tree is not needed at run time).
+* :class:`Port` -- ``oracle/baas_oracle.c``, our plain-C restatement of the reference's serial
+  numeric routines and of the pcg loop, each function citing the reference line it follows.
+
+Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference arms
+import this module, and only to check or to time the CPU path -- never as the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_LIB = HERE / "_ref" / "libbaas_ref.so"
+PORT_LIB = HERE / "_lib" / "libbaas_oracle.so"
+
+FIELDS = {
+    "ngroups": 0, "nlevels": 1, "ntasks": 2, "group_ptr": 3, "group_set": 4, "level_ptr": 5,
+    "perm_to_orig": 6, "node_to_level": 7, "nthread_per_level": 8, "thread_boundaries": 9,
+    "task_boundaries": 10, "thread_cont_to_orig": 11, "orig_to_thread_cont": 12, "task_ptr": 13,
+    "task_set": 14, "btask_ptr": 15, "btask_set": 16, "cost": 17,
+}
+
+_vp, _i, _d = C.c_void_p, C.c_int, C.c_double
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+class Ref:
+    """The reference's own routines (schedule, p2p executors, serial routines, pcg)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not REF_LIB.exists():
+                raise RuntimeError(f"{REF_LIB} not built (make -C oracle ref)")
+            L = C.CDLL(str(REF_LIB))
+            L.ref_schedule_build.argtypes = [_i, _i, _vp, _vp, _i]
+            L.ref_schedule_build.restype = _vp
+            L.ref_schedule_get.argtypes = [_vp, _i, _vp]
+            L.ref_schedule_get.restype = _i
+            L.ref_schedule_free.argtypes = [_vp]
+            L.ref_schedule_analysis_ms.argtypes = [_vp]
+            L.ref_schedule_analysis_ms.restype = _d
+            for name in ("ref_sptrsv_forward", "ref_sptrsv_backward"):
+                getattr(L, name).argtypes = [_vp, _i, _vp, _vp, _vp, _vp, _vp]
+            for name in ("ref_ic0", "ref_ilu0"):
+                getattr(L, name).argtypes = [_vp, _i, _vp, _vp, _vp, _vp]
+            for name in ("ref_sptrsv_serial", "ref_upper_serial"):
+                getattr(L, name).argtypes = [_i, _vp, _vp, _vp, _vp, _vp]
+            for name in ("ref_ic0_serial", "ref_ilu0_serial"):
+                getattr(L, name).argtypes = [_i, _vp, _vp, _vp, _vp]
+            L.ref_spmv.argtypes = [_i, _vp, _vp, _vp, _vp, _vp, _d, _d]
+            L.ref_dot.argtypes = [_vp, _vp, _i]
+            L.ref_dot.restype = _d
+            L.ref_pcg.argtypes = [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _i, _d, _vp, _vp]
+            L.ref_pcg.restype = _i
+            cls._lib = L
+        return cls._lib
+
+    class Schedule:
+        def __init__(self, kind: int, A, nthread: int):
+            L = Ref.lib()
+            self.rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
+            self.colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
+            self.n = A.n
+            self.h = L.ref_schedule_build(kind, A.n, _p(self.rowptr), _p(self.colidx), nthread)
+
+        def __del__(self):
+            if getattr(self, "h", None):
+                Ref.lib().ref_schedule_free(self.h)
+                self.h = None
+
+        @property
+        def analysis_ms(self) -> float:
+            return Ref.lib().ref_schedule_analysis_ms(self.h)
+
+        def export(self, field: str) -> np.ndarray:
+            L = Ref.lib()
+            n = L.ref_schedule_get(self.h, FIELDS[field], None)
+            out = np.zeros(max(n, 1), dtype=np.int32)
+            L.ref_schedule_get(self.h, FIELDS[field], _p(out))
+            return out[:n]
+
+        def arrays(self) -> dict:
+            return {k: self.export(k) for k in FIELDS}
+
+        def forward(self, L, b: np.ndarray) -> np.ndarray:
+            x = np.zeros(L.n)
+            Ref.lib().ref_sptrsv_forward(self.h, L.n, _p(L.rowptr), _p(L.colidx), _p(L.values), _p(x),
+                                         _p(np.ascontiguousarray(b)))
+            return x
+
+        def backward(self, U, b: np.ndarray) -> np.ndarray:
+            x = np.zeros(U.n)
+            Ref.lib().ref_sptrsv_backward(self.h, U.n, _p(U.rowptr), _p(U.colidx), _p(U.values), _p(x),
+                                          _p(np.ascontiguousarray(b)))
+            return x
+
+        def ic0(self, A) -> np.ndarray:
+            lu = A.values.copy()
+            Ref.lib().ref_ic0(self.h, A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(lu))
+            return lu
+
+        def ilu0(self, A) -> np.ndarray:
+            lu = A.values.copy()
+            Ref.lib().ref_ilu0(self.h, A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(lu))
+            return lu
+
+    @staticmethod
+    def sptrsv_serial(L, b) -> np.ndarray:
+        x = np.zeros(L.n)
+        Ref.lib().ref_sptrsv_serial(L.n, _p(L.rowptr), _p(L.colidx), _p(L.values), _p(x), _p(np.ascontiguousarray(b)))
+        return x
+
+    @staticmethod
+    def upper_serial(U, b) -> np.ndarray:
+        x = np.zeros(U.n)
+        Ref.lib().ref_upper_serial(U.n, _p(U.rowptr), _p(U.colidx), _p(U.values), _p(x), _p(np.ascontiguousarray(b)))
+        return x
+
+    @staticmethod
+    def ic0_serial(A) -> np.ndarray:
+        lu = A.values.copy()
+        Ref.lib().ref_ic0_serial(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(lu))
+        return lu
+
+    @staticmethod
+    def ilu0_serial(A) -> np.ndarray:
+        lu = A.values.copy()
+        Ref.lib().ref_ilu0_serial(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(lu))
+        return lu
+
+    @staticmethod
+    def pcg(A, b, x0=None, maxiter=2000, tol=1e-10, mode=1, nthread=8):
+        """mode 0 = pcg_ref structure (serial), 1 = pcg_opt structure (BAAS p2p).
+        Returns (x, iterations, relres, times_ms[pre, ic, loop, total, trsv])."""
+        x = np.zeros(A.n) if x0 is None else np.array(x0, dtype=np.float64)
+        rel = C.c_double(0.0)
+        t = np.zeros(5)
+        it = Ref.lib().ref_pcg(mode, nthread, A.n, _p(A.rowptr), _p(A.colidx), _p(A.values),
+                               _p(np.ascontiguousarray(b)), _p(x), maxiter, tol, C.addressof(rel), _p(t))
+        return x, it, rel.value, t
+
+
+class Port:
+    """Plain-C restatement of the reference's serial numeric routines (oracle/baas_oracle.c)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not PORT_LIB.exists():
+                raise RuntimeError(f"{PORT_LIB} not built (make -C oracle oracle)")
+            L = C.CDLL(str(PORT_LIB))
+            L.orc_lower_solve.argtypes = [_i, _vp, _vp, _vp, _vp, _vp]
+            L.orc_upper_solve_desc.argtypes = [_i, _vp, _vp, _vp, _vp, _vp]
+            L.orc_upper_solve_asc.argtypes = [_i, _vp, _vp, _vp, _vp, _vp]
+            L.orc_ic0.argtypes = [_i, _vp, _vp, _vp, _vp]
+            L.orc_ic0.restype = _i
+            L.orc_ilu0.argtypes = [_i, _vp, _vp, _vp, _vp]
+            L.orc_ilu0.restype = _i
+            L.orc_spmv.argtypes = [_i, _vp, _vp, _vp, _vp, _vp, _d, _d]
+            L.orc_pcg.argtypes = [_i, _vp, _vp, _vp, _vp, _vp, _i, _d, _vp, _vp]
+            L.orc_pcg.restype = _i
+            cls._lib = L
+        return cls._lib
+
+    @staticmethod
+    def lower_solve(L, b):
+        x = np.zeros(L.n)
+        Port.lib().orc_lower_solve(L.n, _p(L.rowptr), _p(L.colidx), _p(L.values), _p(np.ascontiguousarray(b)), _p(x))
+        return x
+
+    @staticmethod
+    def upper_solve(U, b, descending=True):
+        x = np.zeros(U.n)
+        f = Port.lib().orc_upper_solve_desc if descending else Port.lib().orc_upper_solve_asc
+        f(U.n, _p(U.rowptr), _p(U.colidx), _p(U.values), _p(np.ascontiguousarray(b)), _p(x))
+        return x
+
+    @staticmethod
+    def ic0(A):
+        lu = A.values.copy()
+        bad = Port.lib().orc_ic0(A.n, _p(A.rowptr), _p(A.colidx), _p(A.diagptr()), _p(lu))
+        return lu, bad
+
+    @staticmethod
+    def ilu0(A):
+        lu = A.values.copy()
+        bad = Port.lib().orc_ilu0(A.n, _p(A.rowptr), _p(A.colidx), _p(A.diagptr()), _p(lu))
+        return lu, bad
+
+    @staticmethod
+    def spmv(A, x, y=None, alpha=1.0, beta=0.0):
+        y = np.zeros(A.n) if y is None else np.array(y, dtype=np.float64)
+        Port.lib().orc_spmv(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(np.ascontiguousarray(x)), _p(y), alpha, beta)
+        return y
+
+    @staticmethod
+    def pcg(A, b, x0=None, maxiter=2000, tol=1e-10):
+        """IC0-PCG with serial IC0 and serial sweeps; returns (x, iterations, relres)."""
+        x = np.zeros(A.n) if x0 is None else np.array(x0, dtype=np.float64)
+        rel = C.c_double(0.0)
+        it = Port.lib().orc_pcg(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(np.ascontiguousarray(b)), _p(x),
+                                maxiter, tol, C.addressof(rel), None)
+        return x, it, rel.value

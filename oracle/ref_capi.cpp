@@ -1,0 +1,522 @@
+/*
+ * oracle/ref_capi.cpp -- TEST INFRASTRUCTURE ONLY (the oracle), never shipped or measured
+ * as the product.
+ *
+ * A thin C ABI over the reference's own library code, compiled together with the
+ * reference sources spm/, merge/, blas/ by oracle/Makefile into oracle/_ref/libbaas_ref.so.
+ * Every schedule array and every numeric result this file returns is computed by the
+ * reference's functions; this file only sequences the calls the reference's drivers make:
+ *
+ *   kind SPTRSV : SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule::buildset
+ *                 (test/SpTRSVRuntime.hpp:675-775), fused_code :777-816
+ *   kind ICCG   : Schedule::Scheduler(A, true, false, P2P_RULE, nthread) + preprocessing()
+ *                 (test/Schedule.hpp:117-296), used by pcg_opt (test/iccg_level_merge.cpp:380-533)
+ *   kind IC0    : IC_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule::buildset (test/ICRuntime.hpp:408-520)
+ *   kind ILU0   : ILU_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule::buildset (test/ILURuntime.hpp:265-385)
+ *
+ * The test/*Runtime.hpp classes include mkl.h and cannot be compiled here (MKL is absent), so
+ * their buildset call sequences are repeated below against the library functions they call.
+ * Schedule.hpp has no MKL dependency and is included directly.
+ *
+ * pcg: the loop of pcg_opt / pcg_ref (test/iccg_level_merge.cpp:458-503, 741-777) with the
+ * reference's own BLAS-1 and SpMV (blas/blasone.cpp, blas/spmv.cpp) in place of MKL and a
+ * `break` once the relative residual drops below tol (the reference records the iteration
+ * and keeps going, :480-484).
+ */
+#include <omp.h>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include <chrono>
+
+#include "Schedule.hpp"
+#include "BlasDemo.hpp"
+
+#include "../include/baas_b200.h"
+
+void dcsrmv(const int m, const double *a, const int *ia, const int *ja, const double *x, double *y, const double alpha, const double beta);
+
+namespace refdrv
+{
+    using SPM::CSC;
+    using SPM::CSR;
+    using SPM::DAG;
+    using SPM::LevelSet;
+
+    // Scheduler exposes its schedule only to subclasses; the reference's destructor frees
+    // x_perm / csrA_perm even when they were never set (test/Schedule.hpp:127-131,165), so
+    // they are cleared here first.
+    struct OpenScheduler : public Schedule::Scheduler
+    {
+        OpenScheduler(const CSR *A, int nthread)
+            : Schedule::Scheduler(A, true, false, Schedule::ALG_SCHEDULE::P2P_RULE, nthread)
+        {
+            csrA_perm = nullptr;
+            x_perm = nullptr;
+        }
+        LevelSet *lvl() { return levelset_merge; }
+        int *ntpl() { return nthread_per_level; }
+        Merge::Task *tsk() { return task; }
+        Merge::TaskSchedule *sched() { return taskSchedule; }
+        DAG *tdag() { return taskDAG; }
+        std::vector<int> &gptr() { return group_ptr; }
+        std::vector<int> &gset() { return group_set; }
+        int ng() { return ngroups; }
+        std::vector<double> &cst() { return cost; }
+    };
+
+    struct Handle
+    {
+        int kind = 0;
+        int n = 0;
+        int nthread = 1;
+        std::vector<int> rowptr, colidx;
+        std::vector<double> values;
+        CSR *A = nullptr; // non-owning view of rowptr/colidx/values (diagptr owned)
+        CSC *csc = nullptr;
+        OpenScheduler *scheduler = nullptr;
+
+        // class-style schedules (kinds SPTRSV / IC0 / ILU0)
+        LevelSet *levelset = nullptr;
+        int *nthread_per_level = nullptr;
+        int ngroups = 0;
+        DAG *dag_group = nullptr;
+        DAG *taskDAG = nullptr;
+        Merge::Task *task = nullptr;
+        Merge::TaskSchedule *schedule = nullptr;
+        std::vector<int> group_set, group_ptr;
+        std::vector<double> cost;
+        double analysis_ms = 0.0;
+
+        LevelSet *L() { return scheduler ? scheduler->lvl() : levelset; }
+        int *NT() { return scheduler ? scheduler->ntpl() : nthread_per_level; }
+        Merge::Task *T() { return scheduler ? scheduler->tsk() : task; }
+        Merge::TaskSchedule *S() { return scheduler ? scheduler->sched() : schedule; }
+        DAG *TD() { return scheduler ? scheduler->tdag() : taskDAG; }
+        std::vector<int> &GP() { return scheduler ? scheduler->gptr() : group_ptr; }
+        std::vector<int> &GS() { return scheduler ? scheduler->gset() : group_set; }
+        int NG() { return scheduler ? scheduler->ng() : ngroups; }
+        std::vector<double> &C() { return scheduler ? scheduler->cst() : cost; }
+    };
+
+    static void orderingGroupSet(const int ngroups, const std::vector<int> &group_ptr, std::vector<int> &group_set)
+    {
+        for (int g = 0; g < ngroups; g++)
+            std::sort(group_set.begin() + group_ptr[g], group_set.begin() + group_ptr[g + 1]);
+    }
+
+    // Call sequence of the three runtime classes' buildset(); `lowerRowptr`/`lowerColidx`
+    // is the lower-triangle pattern (incl. diagonal) the DAG is built from, `csrForThreads`
+    // the matrix the thread-count heuristic reads.
+    static void class_buildset(Handle *h, const CSR *csrLower, const CSC *cscLower, const CSR *csrForThreads, int lowerNnz)
+    {
+        const int n = h->n;
+        h->dag_group = new DAG();
+        h->taskDAG = new DAG();
+        DAG *dag = new DAG(n, lowerNnz);
+        dag->DAG_ptr.clear();
+        dag->DAG_set.clear();
+        DAG::partialSparsification_CSC(n, lowerNnz, cscLower->colptr, cscLower->rowidx, dag->DAG_ptr, dag->DAG_set, false);
+
+        Coarsen::reverseTreeCoarseningBFS_all(n, dag->DAG_ptr, dag->DAG_set, h->ngroups, h->group_ptr, h->group_set);
+        Coarsen::buildGroupDAGParallel(n, h->ngroups, h->group_ptr.data(), h->group_set.data(),
+                                       dag->DAG_ptr.data(), dag->DAG_set.data(), h->dag_group->DAG_ptr, h->dag_group->DAG_set);
+        h->dag_group->setNodeNum(h->ngroups);
+        delete dag;
+
+        std::vector<int> group_ptr_f, group_set_f;
+        DAG *dag_group_f = new DAG();
+        int ngroups_f = 0;
+        Coarsen::forwardTreeCoarseningBFS_all(h->ngroups, h->dag_group->DAG_ptr, h->dag_group->DAG_set, ngroups_f, group_ptr_f, group_set_f, false);
+        Coarsen::groupRemapping(h->group_ptr, h->group_set, group_ptr_f, group_set_f, ngroups_f);
+        Coarsen::buildGroupDAGParallel(h->ngroups, ngroups_f, group_ptr_f.data(), group_set_f.data(),
+                                       h->dag_group->DAG_ptr.data(), h->dag_group->DAG_set.data(), dag_group_f->DAG_ptr, dag_group_f->DAG_set);
+        h->ngroups = ngroups_f;
+        dag_group_f->setNodeNum(ngroups_f);
+        dag_group_f->updateEdges();
+        h->levelset = new LevelSet();
+        dag_group_f->findLevelsPostOrder(h->levelset);
+        delete h->dag_group;
+        h->dag_group = dag_group_f;
+
+        Coarsen::costComputation(h->ngroups, nullptr, nullptr, csrLower->rowptr, csrLower->colidx,
+                                 Coarsen::Kernel::SpTRSV_LL, h->group_ptr.data(), h->group_set.data(), true, h->cost);
+        if (h->kind == BAAS_KERNEL_SPTRSV)
+            Merge::level_nthreads_group_TRSV(h->levelset, csrForThreads, h->group_ptr.data(), h->group_set.data(), h->nthread, h->nthread_per_level);
+        else if (h->kind == BAAS_KERNEL_IC0)
+            Merge::level_nthreads_group_IC0(h->levelset, csrForThreads, h->group_ptr.data(), h->group_set.data(), h->nthread, h->nthread_per_level);
+        else
+            Merge::level_nthreads_group_ILU0(h->levelset, csrForThreads, h->group_ptr.data(), h->group_set.data(), h->nthread, h->nthread_per_level);
+
+        orderingGroupSet(h->ngroups, h->group_ptr, h->group_set);
+        h->task = new Merge::Task(h->ngroups, false);
+        DAG *inv = DAG::inverseDAG(*h->dag_group);
+        h->task->constructMappingByFourRuleParallel(h->dag_group, inv, h->levelset, h->cost.data(), h->nthread,
+                                                    h->nthread_per_level, h->group_ptr.data(), h->group_set.data());
+        if (h->kind == BAAS_KERNEL_SPTRSV)
+            h->task->constructTaskDAG(h->dag_group, inv, h->taskDAG, h->nthread, false);
+        else
+            h->task->constructTaskDAGParallel(h->dag_group, inv, h->taskDAG, h->nthread, false);
+        delete inv;
+        h->schedule = new Merge::TaskSchedule(h->taskDAG->getNodeNum(), h->taskDAG->DAG_ptr.back());
+        h->schedule->constructTaskSchedule(h->taskDAG);
+        // the backward sweep after ILU0 uses the inverse task DAG, as Scheduler does for
+        // symmetric patterns (test/Schedule.hpp:288-291)
+        h->schedule->constructInverseSchedule(h->taskDAG);
+    }
+
+    static int copy_out(const int *src, int len, int *out)
+    {
+        if (out && len > 0)
+            std::memcpy(out, src, sizeof(int) * (size_t)len);
+        return len;
+    }
+} // namespace refdrv
+
+using namespace refdrv;
+
+extern "C"
+{
+    /* kind: a baas_kernel value. The matrix is the lower triangle incl. diagonal (diagonal last
+     * in each row) for BAAS_KERNEL_SPTRSV and the full matrix for the other kinds. */
+    void *ref_schedule_build(int kind, int n, const int *rowptr, const int *colidx, int nthread)
+    {
+        omp_set_num_threads(nthread);
+        Handle *h = new Handle();
+        h->kind = kind;
+        h->n = n;
+        h->nthread = nthread;
+        int nnz = rowptr[n];
+        h->rowptr.assign(rowptr, rowptr + n + 1);
+        h->colidx.assign(colidx, colidx + nnz);
+        h->values.assign((size_t)nnz, 1.0);
+        h->A = new CSR(n, n, h->rowptr.data(), h->colidx.data(), h->values.data());
+        h->A->constructDiagPtr();
+        auto t0 = std::chrono::steady_clock::now();
+        if (kind == BAAS_KERNEL_ICCG)
+        {
+            h->scheduler = new OpenScheduler(h->A, nthread);
+            h->scheduler->preprocessing();
+        }
+        else if (kind == BAAS_KERNEL_SPTRSV)
+        {
+            // test/SpTRSV_level_merge.cpp:59-60 builds the CSC this way
+            h->csc = new CSC();
+            CSR::transpositionToCSC(h->A, h->csc);
+            class_buildset(h, h->A, h->csc, h->A, nnz);
+        }
+        else
+        {
+            // test/ICRuntime.hpp:412-431 / test/ILURuntime.hpp:268-289: lower triangle of A
+            const int *rp = h->A->rowptr, *dp = h->A->diagptr, *ci = h->A->colidx;
+            int lowerNnz = 0;
+            for (int i = 0; i < n; i++)
+                lowerNnz += dp[i] - rp[i] + 1;
+            CSR *lower = new CSR(n, n, lowerNnz);
+            for (int i = 0; i < n; i++)
+            {
+                lower->rowptr[i + 1] = lower->rowptr[i] + dp[i] - rp[i] + 1;
+                std::copy(ci + rp[i], ci + dp[i] + 1, lower->colidx + lower->rowptr[i]);
+            }
+            CSC *cscLower = new CSC();
+            CSR::transpositionToCSC(lower, cscLower);
+            class_buildset(h, lower, cscLower, h->A, lowerNnz);
+            delete lower;
+            delete cscLower;
+        }
+        auto t1 = std::chrono::steady_clock::now();
+        h->analysis_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        return h;
+    }
+
+    double ref_schedule_analysis_ms(void *hv) { return ((Handle *)hv)->analysis_ms; }
+
+    /* Copies one schedule array (a baas_schedule_field) into out (if non-NULL); returns its length. */
+    int ref_schedule_get(void *hv, int field, int *out)
+    {
+        Handle *h = (Handle *)hv;
+        LevelSet *L = h->L();
+        Merge::Task *T = h->T();
+        Merge::TaskSchedule *S = h->S();
+        DAG *TD = h->TD();
+        int ng = h->NG();
+        int ntask = T->getTaskNum();
+        int scalar = 0;
+        switch (field)
+        {
+        case BAAS_FIELD_NGROUPS:
+            scalar = ng;
+            return copy_out(&scalar, 1, out);
+        case BAAS_FIELD_NLEVELS:
+            scalar = L->getLevels();
+            return copy_out(&scalar, 1, out);
+        case BAAS_FIELD_NTASKS:
+            scalar = ntask;
+            return copy_out(&scalar, 1, out);
+        case BAAS_FIELD_GROUP_PTR:
+            return copy_out(h->GP().data(), ng + 1, out);
+        case BAAS_FIELD_GROUP_SET:
+            return copy_out(h->GS().data(), h->n, out);
+        case BAAS_FIELD_LEVEL_PTR:
+            return copy_out(L->level_ptr, L->getLevels() + 1, out);
+        case BAAS_FIELD_PERM_TO_ORIG:
+            return copy_out(L->permToOrig, ng, out);
+        case BAAS_FIELD_NODE_TO_LEVEL:
+            return copy_out(L->nodeToLevel, ng, out);
+        case BAAS_FIELD_NTHREAD_PER_LEVEL:
+            return copy_out(h->NT(), L->getLevels(), out);
+        case BAAS_FIELD_THREAD_BOUNDARIES:
+            return copy_out(T->threadBoundaries.data(), (int)T->threadBoundaries.size(), out);
+        case BAAS_FIELD_TASK_BOUNDARIES:
+            return copy_out(T->taskBoundaries.data(), (int)T->taskBoundaries.size(), out);
+        case BAAS_FIELD_THREAD_CONT_TO_ORIG:
+            return copy_out(T->threadContToOrigPerm, ng, out);
+        case BAAS_FIELD_ORIG_TO_THREAD_CONT:
+            return copy_out(T->origToThreadContPerm, ng, out);
+        case BAAS_FIELD_TASK_PTR:
+            return copy_out(TD->DAG_ptr.data(), (int)TD->DAG_ptr.size(), out);
+        case BAAS_FIELD_TASK_SET:
+            return copy_out(TD->DAG_set.data(), TD->DAG_ptr.back(), out);
+        case BAAS_FIELD_BTASK_PTR:
+        {
+            std::vector<int> ptr(ntask + 1, 0);
+            for (int t = 0; t < ntask; t++)
+                ptr[t + 1] = ptr[t] + S->nparentsBackward[t];
+            return copy_out(ptr.data(), ntask + 1, out);
+        }
+        case BAAS_FIELD_BTASK_SET:
+        {
+            std::vector<int> set;
+            for (int t = 0; t < ntask; t++)
+                for (int j = 0; j < S->nparentsBackward[t]; j++)
+                    set.push_back(S->parentsBackward[t][j]);
+            return copy_out(set.data(), (int)set.size(), out);
+        }
+        case BAAS_FIELD_COST:
+        {
+            std::vector<int> c(ng);
+            for (int g = 0; g < ng; g++)
+                c[g] = (int)h->C()[g];
+            return copy_out(c.data(), ng, out);
+        }
+        default:
+            return -1;
+        }
+    }
+
+    void ref_schedule_free(void *hv)
+    {
+        Handle *h = (Handle *)hv;
+        delete h->scheduler;
+        delete h->levelset;
+        if (h->nthread_per_level)
+            free(h->nthread_per_level);
+        delete h->dag_group;
+        delete h->taskDAG;
+        delete h->task;
+        delete h->schedule;
+        delete h->csc;
+        delete h->A;
+        delete h;
+    }
+
+    /* Forward p2p sweep of the schedule on lower CSR L (diagonal last): x = L^-1 b.
+     * merge/SpTRSV.cpp:421-478 (through Scheduler::runForwardTRSVNoPerm for kind ICCG). */
+    void ref_sptrsv_forward(void *hv, int n, const int *rowptr, const int *colidx, const double *values, double *x, const double *b)
+    {
+        Handle *h = (Handle *)hv;
+        omp_set_num_threads(h->nthread);
+        CSR Lm(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        if (h->scheduler)
+            h->scheduler->runForwardTRSVNoPerm(&Lm, x, b);
+        else
+            sptrsv_p2p_csr_group_merge_no_perm_alloc(&Lm, x, b, h->levelset, h->nthread_per_level, h->group_ptr.data(),
+                                                     h->group_set.data(), h->task, h->schedule);
+    }
+
+    /* Backward p2p sweep on upper CSR U (diagonal first): merge/SpTRSV.cpp:601-660. */
+    void ref_sptrsv_backward(void *hv, int n, const int *rowptr, const int *colidx, const double *values, double *x, const double *b)
+    {
+        Handle *h = (Handle *)hv;
+        omp_set_num_threads(h->nthread);
+        CSR Um(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        if (h->scheduler)
+            h->scheduler->runBackwardTRSVNoPerm(&Um, x, b);
+        else
+            sptrsv_backward_p2p_csr_group_merge_no_perm_alloc(&Um, x, b, h->levelset, h->nthread_per_level, h->group_ptr.data(),
+                                                              h->group_set.data(), h->task, h->schedule);
+    }
+
+    /* IC0 in place on lu (pre-filled with A.values): merge/IC.cpp:296-393. The class driver
+     * falls back to the serial routine when the schedule has no p2p edge
+     * (test/ICRuntime.hpp:539-549). */
+    void ref_ic0(void *hv, int n, const int *rowptr, const int *colidx, const double *values, double *lu)
+    {
+        Handle *h = (Handle *)hv;
+        omp_set_num_threads(h->nthread);
+        CSR Am(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        Am.constructDiagPtr();
+        if (h->scheduler)
+            h->scheduler->runIC0(&Am, lu);
+        else if (h->schedule->getP2PNum() == 0)
+            spic0_csr_uL_serial(&Am, lu);
+        else
+            spic0_csr_uL_p2p_group_merge_no_perm(&Am, lu, h->levelset, h->nthread_per_level, h->group_ptr.data(),
+                                                 h->group_set.data(), h->task, h->schedule);
+    }
+
+    /* ILU0 in place on lu: merge/ILU.cpp:638-720 (serial fallback as test/ILURuntime.hpp:391-401). */
+    void ref_ilu0(void *hv, int n, const int *rowptr, const int *colidx, const double *values, double *lu)
+    {
+        Handle *h = (Handle *)hv;
+        omp_set_num_threads(h->nthread);
+        CSR Am(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        Am.constructDiagPtr();
+        if (h->schedule->getP2PNum() == 0)
+            ilu0csr_uplooking_ref(&Am, lu);
+        else
+            ilu0_p2p_csr_group_merge_no_perm_alloc(&Am, lu, h->levelset, h->nthread_per_level, h->group_ptr.data(),
+                                                   h->group_set.data(), h->task, h->schedule);
+    }
+
+    /* ---- serial reference routines ---- */
+    void ref_sptrsv_serial(int n, const int *rowptr, const int *colidx, const double *values, double *x, const double *b)
+    {
+        CSR Lm(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        sptrsv_serial_csr(Lm, x, b);
+    }
+    void ref_upper_serial(int n, const int *rowptr, const int *colidx, const double *values, double *x, const double *b)
+    {
+        CSR Um(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        upper_csr_trsv_serial(Um, x, b);
+    }
+    void ref_ic0_serial(int n, const int *rowptr, const int *colidx, const double *values, double *lu)
+    {
+        CSR Am(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        Am.constructDiagPtr();
+        spic0_csr_uL_serial(&Am, lu);
+    }
+    void ref_ilu0_serial(int n, const int *rowptr, const int *colidx, const double *values, double *lu)
+    {
+        CSR Am(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        Am.constructDiagPtr();
+        ilu0csr_uplooking_ref(&Am, lu);
+    }
+    void ref_spmv(int n, const int *rowptr, const int *colidx, const double *values, const double *x, double *y, double alpha, double beta)
+    {
+        dcsrmv(n, values, rowptr, colidx, x, y, alpha, beta);
+    }
+    double ref_dot(const double *x, const double *y, int n) { return dot(x, y, n); }
+
+    /* PCG with the IC0 preconditioner.
+     *   mode 0: pcg_ref structure -- serial IC0 + serial sweeps (test/iccg_level_merge.cpp:698-807)
+     *   mode 1: pcg_opt structure -- Scheduler (P2P_RULE, nthread) IC0 + p2p sweeps (:380-533)
+     * Both use the reference's dcsrmv / dot / norm / waxpby and stop once ||r||/||r0|| < tol.
+     * times_ms[5] = {pre(analysis), ic, loop, total, trsv}. Returns the iteration count. */
+    int ref_pcg(int mode, int nthread, int n, const int *rowptr, const int *colidx, const double *values,
+                const double *b, double *x, int maxiter, double tol, double *relres_out, double *times_ms)
+    {
+        omp_set_num_threads(nthread);
+        using clk = std::chrono::steady_clock;
+        auto ms = [](clk::time_point a, clk::time_point b)
+        { return std::chrono::duration<double, std::milli>(b - a).count(); };
+        auto t_start = clk::now();
+        CSR A(n, n, (int *)rowptr, (int *)colidx, (double *)values);
+        A.constructDiagPtr();
+        OpenScheduler *sch = nullptr;
+        if (mode == 1)
+        {
+            sch = new OpenScheduler(&A, nthread);
+            sch->preprocessing();
+        }
+        auto t_pre = clk::now();
+
+        // IC0_preconditioner (test/iccg_level_merge.cpp:809-906)
+        int nnz = rowptr[n];
+        int nnzL = (nnz + n) / 2;
+        std::vector<int> Lrp(n + 1, 0), Urp(n + 1, 0), Lci(nnzL), Uci(nnzL);
+        std::vector<double> Lv(nnzL), Uv(nnzL), lu(values, values + nnz);
+        for (int i = 0; i < n; i++)
+        {
+            Lrp[i + 1] = Lrp[i] + A.diagptr[i] - rowptr[i] + 1;
+            Urp[i + 1] = Urp[i] + rowptr[i + 1] - A.diagptr[i];
+        }
+        for (int i = 0; i < n; i++)
+        {
+            std::copy(colidx + rowptr[i], colidx + A.diagptr[i] + 1, Lci.data() + Lrp[i]);
+            std::copy(colidx + A.diagptr[i], colidx + rowptr[i + 1], Uci.data() + Urp[i]);
+        }
+        if (mode == 1)
+            sch->runIC0(&A, lu.data());
+        else
+            spic0_csr_uL_serial(&A, lu.data());
+        std::vector<int> ualias(Urp);
+        for (int i = 0; i < n; i++)
+            for (int j = rowptr[i]; j <= A.diagptr[i]; j++)
+            {
+                Lv[Lrp[i] + j - rowptr[i]] = lu[j];
+                Uv[ualias[colidx[j]]++] = lu[j];
+            }
+        CSR Lm(n, n, Lrp.data(), Lci.data(), Lv.data());
+        CSR Um(n, n, Urp.data(), Uci.data(), Uv.data());
+        auto t_ic = clk::now();
+
+        double trsv_ms = 0.0;
+        auto precond = [&](std::vector<double> &yv, std::vector<double> &zv, const std::vector<double> &rv)
+        {
+            auto a = clk::now();
+            if (mode == 1)
+            {
+                sch->runForwardTRSVNoPerm(&Lm, yv.data(), rv.data());
+                sch->runBackwardTRSVNoPerm(&Um, zv.data(), yv.data());
+            }
+            else
+            {
+                lower_csr_trsv_serial(Lm, yv.data(), rv.data());
+                upper_csr_trsv_serial(Um, zv.data(), yv.data());
+            }
+            trsv_ms += ms(a, clk::now());
+        };
+
+        std::vector<double> r(b, b + n), z(n), y(n), p(n), Ap(n);
+        dcsrmv(n, values, rowptr, colidx, x, r.data(), -1, 1);
+        double norm0 = norm(r.data(), n);
+        double rel_err = 1.0;
+        precond(y, z, r);
+        std::copy(z.begin(), z.end(), p.begin());
+        double rz = dot(r.data(), z.data(), n);
+        int k = 1;
+        int iters = 0;
+        auto t_loop0 = clk::now();
+        while (k <= maxiter)
+        {
+            double old_rz = rz;
+            dcsrmv(n, values, rowptr, colidx, p.data(), Ap.data(), 1.0, 0.0);
+            double alpha = old_rz / dot(p.data(), Ap.data(), n);
+            waxpby(n, x, 1, x, alpha, p.data());
+            waxpby(n, r.data(), 1, r.data(), -alpha, Ap.data());
+            rel_err = norm(r.data(), n) / norm0;
+            iters = k;
+            if (rel_err < tol)
+                break;
+            precond(y, z, r);
+            rz = dot(r.data(), z.data(), n);
+            double beta = rz / old_rz;
+            waxpby(n, p.data(), 1, z.data(), beta, p.data());
+            ++k;
+        }
+        auto t_end = clk::now();
+        if (relres_out)
+            *relres_out = rel_err;
+        if (times_ms)
+        {
+            times_ms[0] = ms(t_start, t_pre);
+            times_ms[1] = ms(t_pre, t_ic);
+            times_ms[2] = ms(t_loop0, t_end);
+            times_ms[3] = ms(t_start, t_end);
+            times_ms[4] = trsv_ms;
+        }
+        delete sch;
+        return iters;
+    }
+}
