@@ -76,7 +76,7 @@ class Schedule:
     """
 
     def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
-                 ctas_per_sm: int = 0):
+                 parts: int = 0, partition: int = 0):
         L = _native.lib()
         self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
         self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
@@ -85,7 +85,8 @@ class Schedule:
         L.baas_options_default(C.byref(opt))
         opt.nthread = nthread
         opt.spin_limit = spin_limit
-        opt.ctas_per_sm = ctas_per_sm
+        opt.parts = parts
+        opt.partition = partition
         h = C.c_void_p()
         _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
         self._h = h
@@ -116,6 +117,10 @@ class Schedule:
 
     def arrays(self) -> dict:
         return {k: self.export(k) for k in _native.FIELDS}
+
+    def inject_unsatisfiable_wait(self, row: int) -> None:
+        """Test hook: the next forward sweep waits on a value nothing writes (BAAS_ERR_TIMEOUT)."""
+        _native.check(_native.lib().baas_test_inject_unsatisfiable_wait(self._h, row), "inject")
 
     @property
     def analysis_ms(self) -> float:

@@ -37,7 +37,7 @@ FIELDS = {
 EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
-    "baas_version",
+    "baas_version", "baas_test_inject_unsatisfiable_wait",
 ]
 
 
@@ -47,8 +47,8 @@ class BaasCsr(C.Structure):
 
 
 class BaasOptions(C.Structure):
-    _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("block_size", C.c_int),
-                ("ctas_per_sm", C.c_int)]
+    _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("parts", C.c_int),
+                ("partition", C.c_int)]
 
 
 class BaasError(RuntimeError):
@@ -93,6 +93,8 @@ def lib():
     L.baas_last_error_string.restype = C.c_char_p
     L.baas_version.argtypes = []
     L.baas_version.restype = C.c_char_p
+    L.baas_test_inject_unsatisfiable_wait.argtypes = [vp, i]
+    L.baas_test_inject_unsatisfiable_wait.restype = i
     _lib = L
     return L
 

@@ -1,21 +1,25 @@
 // C ABI of the B200 BAAS hot path (declarations and contracts: include/baas_b200.h).
 //
-// baas_analyze builds the reference-identical schedule on the host (schedule.cpp) and the
-// device execution plan from it: the schedule's groups listed level by level become the work
-// items of the persistent kernels (kernels.cuh), in forward order for the lower sweep and the
-// factorisations and in exactly reversed order for the upper sweep. The plan is uploaded on
-// the first GPU call; the device is the current device of that call.
+// baas_analyze builds the reference-identical schedule on the host (schedule.cpp). From it the
+// device plan is derived: the schedule's groups listed level by level (the BAAS LevelSet
+// order, rows ascending inside a group) give one global topological order of the rows; rows
+// are given to P CTAs (contiguous row ranges by default, or the four-rule thread mapping);
+// each CTA walks its rows in the global order (part_kernels.cuh). The backward sweep uses the
+// exact reverse order. The plan is uploaded on the first GPU call, to the current device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/baas_b200.h"
 #include "kernels.cuh"
+#include "part_kernels.cuh"
+#include "staged.cuh"
 #include "schedule.hpp"
 
 using baas::DevStatus;
@@ -29,21 +33,29 @@ baas_status fail(baas_status st, const std::string &msg) {
     return st;
 }
 
-#define BAAS_CUDA(call)                                                                         \
-    do {                                                                                        \
-        cudaError_t e_ = (call);                                                                \
-        if (e_ != cudaSuccess)                                                                  \
-            return fail(BAAS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+#define BAAS_CUDA(call)                                                                      \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(BAAS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define BAAS_TRY(expr)                       \
+    do {                                     \
+        baas_status s_ = (expr);             \
+        if (s_ != BAAS_OK) return s_;        \
     } while (0)
 
 constexpr unsigned int kDefaultSpin = 1u << 22;
+// shared memory one CTA may use for its rows' solution values (B200: 227 KB per CTA)
+constexpr size_t kSmemBudget = 220 * 1024;
 
 template <typename T>
 baas_status upload(T *&d, const std::vector<T> &h) {
     d = nullptr;
-    if (h.empty()) return BAAS_OK;
-    BAAS_CUDA(cudaMalloc((void **)&d, h.size() * sizeof(T)));
-    BAAS_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    const size_t cnt = std::max<size_t>(h.size(), 1);
+    BAAS_CUDA(cudaMalloc((void **)&d, cnt * sizeof(T)));
+    if (!h.empty()) BAAS_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
     return BAAS_OK;
 }
 
@@ -56,6 +68,92 @@ baas_status dalloc(T *&d, size_t count) {
     return BAAS_OK;
 }
 
+// One sweep direction of the partitioned plan (host side). Positions are CTA-major; inside a
+// CTA they run level segment by level segment, group (item) by group, row by row.
+struct PartHost {
+    std::vector<int> cta_seg, seg_item, item_pos, cta_pos, row, eptr, dep;
+    std::vector<int> srcT, dsrcT;  // positions in the caller's triangular CSR (L or U)
+    std::vector<int> srcA, dsrcA;  // positions in A's value array (IC0 factor on A's pattern)
+    int max_local = 0;
+};
+
+struct PartDev {
+    int *cta_seg = nullptr, *seg_item = nullptr, *item_pos = nullptr, *cta_pos = nullptr;
+    int *row = nullptr, *eptr = nullptr, *dep = nullptr;
+    int *srcT = nullptr, *dsrcT = nullptr, *srcA = nullptr, *dsrcA = nullptr;
+    baas::PartView view(int P) const { return baas::PartView{P, cta_seg, seg_item, item_pos, cta_pos, row, eptr, dep}; }
+    void release() {
+        int *ptrs[] = {cta_seg, seg_item, item_pos, cta_pos, row, eptr, dep, srcT, dsrcT, srcA, dsrcA};
+        for (int *p : ptrs)
+            if (p) cudaFree(p);
+        *this = PartDev();
+    }
+};
+
+baas_status upload_part(PartDev &d, const PartHost &h) {
+    BAAS_TRY(upload(d.cta_seg, h.cta_seg));
+    BAAS_TRY(upload(d.seg_item, h.seg_item));
+    BAAS_TRY(upload(d.item_pos, h.item_pos));
+    BAAS_TRY(upload(d.cta_pos, h.cta_pos));
+    BAAS_TRY(upload(d.row, h.row));
+    BAAS_TRY(upload(d.eptr, h.eptr));
+    BAAS_TRY(upload(d.dep, h.dep));
+    BAAS_TRY(upload(d.srcT, h.srcT));
+    BAAS_TRY(upload(d.dsrcT, h.dsrcT));
+    BAAS_TRY(upload(d.srcA, h.srcA));
+    BAAS_TRY(upload(d.dsrcA, h.dsrcA));
+    return BAAS_OK;
+}
+
+// Staged plan (staged.cuh), host side: per direction the packed per-CTA int and value-source
+// blocks.
+struct StagedHostDir {
+    std::vector<int> ioff, voff, ns, nl, ne, ints, vsrcT, vsrcA;
+};
+struct StagedHost {
+    StagedHostDir dir[2];
+    size_t smem64 = 0, smem32 = 0;  // dynamic shared memory per CTA (FP64 / FP32 values)
+};
+struct StagedDevDir {
+    int *ioff = nullptr, *voff = nullptr, *ns = nullptr, *nl = nullptr, *ne = nullptr, *ints = nullptr,
+        *vsrcT = nullptr, *vsrcA = nullptr;
+};
+struct StagedDev {
+    StagedDevDir dir[2];
+    baas::StagedPlan plan(int P) const {
+        baas::StagedPlan p;
+        p.P = P;
+        for (int d = 0; d < 2; d++)
+            p.dir[d] = baas::StagedDir{dir[d].ioff, dir[d].voff, dir[d].ns, dir[d].nl, dir[d].ne,
+                                      dir[d].ints, dir[d].vsrcT, dir[d].vsrcA};
+        return p;
+    }
+    void release() {
+        for (auto &D : dir) {
+            int *ptrs[] = {D.ioff, D.voff, D.ns, D.nl, D.ne, D.ints, D.vsrcT, D.vsrcA};
+            for (int *p : ptrs)
+                if (p) cudaFree(p);
+        }
+        *this = StagedDev();
+    }
+};
+
+baas_status upload_staged(StagedDev &d, const StagedHost &h) {
+    for (int k = 0; k < 2; k++) {
+        const StagedHostDir &H = h.dir[k];
+        StagedDevDir &D = d.dir[k];
+        BAAS_TRY(upload(D.ioff, H.ioff));
+        BAAS_TRY(upload(D.voff, H.voff));
+        BAAS_TRY(upload(D.ns, H.ns));
+        BAAS_TRY(upload(D.nl, H.nl));
+        BAAS_TRY(upload(D.ne, H.ne));
+        BAAS_TRY(upload(D.ints, H.ints));
+        BAAS_TRY(upload(D.vsrcT, H.vsrcT));
+        BAAS_TRY(upload(D.vsrcA, H.vsrcA));
+    }
+    return BAAS_OK;
+}
+
 }  // namespace
 
 struct baas_schedule {
@@ -63,19 +161,24 @@ struct baas_schedule {
     baas_options opt{};
     int nnz_a = 0, nnz_l = 0;
 
-    // host plan
-    std::vector<int> f_item_ptr, f_ord, b_item_ptr, b_ord;
-    std::vector<int> fp_ptr, fp_col, fp_src, fp_dsrc;  // packed L (A positions)
-    std::vector<int> bp_ptr, bp_col, bp_src, bp_dsrc;  // packed U = L^T (A positions)
+    // global topological order of rows (forward) and the transpose of L (for U = L^T)
+    std::vector<int> f_ord;
+    std::vector<int> cptr, crow, cpos;  // CSC of L: rows ascending per column (diagonal first)
 
-    // device plan
+    // partition (built at first GPU use, when the SM count is known)
+    int P = 0;
+    std::vector<int> group_cta, row_cta;
+    PartHost fwd, bwd;
+    StagedHost stg;
+    int fault_row = -1;  // test hook: forward row made to wait on its own output
+
+    // device
     int device = -1;
     bool uploaded = false;
     int num_sms = 0;
-    int *d_f_item_ptr = nullptr, *d_f_ord = nullptr, *d_b_item_ptr = nullptr, *d_b_ord = nullptr;
+    PartDev d_fwd, d_bwd;
+    StagedDev d_stg;
     int *d_a_diag = nullptr;
-    int *d_fp_ptr = nullptr, *d_fp_col = nullptr, *d_fp_src = nullptr, *d_fp_dsrc = nullptr;
-    int *d_bp_ptr = nullptr, *d_bp_col = nullptr, *d_bp_src = nullptr, *d_bp_dsrc = nullptr;
     DevStatus *d_status = nullptr;
     DevStatus *h_status = nullptr;  // pinned
     int *d_flags = nullptr;
@@ -86,84 +189,239 @@ struct baas_schedule {
     bool ws_ready = false;
     double *d_lu = nullptr, *d_r = nullptr, *d_y = nullptr, *d_z = nullptr, *d_p = nullptr, *d_Ap = nullptr;
     float *d_y32 = nullptr, *d_z32 = nullptr;
-    double *d_fp_val = nullptr, *d_fp_diag = nullptr, *d_bp_val = nullptr, *d_bp_diag = nullptr;
-    float *d_fp_val32 = nullptr, *d_fp_diag32 = nullptr, *d_bp_val32 = nullptr, *d_bp_diag32 = nullptr;
+    double *d_gv64[2] = {nullptr, nullptr};
+    float *d_gv32[2] = {nullptr, nullptr};
     double *d_part = nullptr;
     int *d_iters = nullptr;
     double *d_relres = nullptr;
-    int part_cap = 0;
+
+    unsigned long long *d_trace = nullptr;  // BAAS_TRACE=1: phase timestamps of the last launch
 
     unsigned int spin() const { return opt.spin_limit > 0 ? (unsigned int)opt.spin_limit : kDefaultSpin; }
-    int block() const { return baas::kBlock; }
 };
 
 namespace {
 
-void build_plan(baas_schedule *s) {
+void build_order(baas_schedule *s) {
     const baas::HostSchedule &h = s->hs;
     const int n = h.n;
-    const int ng = h.ngroups;
-    // forward items: groups level by level (LevelSet permToOrig), rows ascending
-    s->f_item_ptr.assign(ng + 1, 0);
     s->f_ord.clear();
     s->f_ord.reserve(n);
-    for (int q = 0; q < ng; q++) {
+    for (int q = 0; q < h.ngroups; q++) {
         const int g = h.perm_to_orig[q];
         for (int e = h.group_ptr[g]; e < h.group_ptr[g + 1]; e++) s->f_ord.push_back(h.group_set[e]);
-        s->f_item_ptr[q + 1] = (int)s->f_ord.size();
     }
-    // backward items: the exact reverse (items reversed, rows descending)
-    s->b_item_ptr.assign(ng + 1, 0);
-    s->b_ord.assign(s->f_ord.rbegin(), s->f_ord.rend());
-    for (int q = 0; q < ng; q++) {
-        const int fq = ng - 1 - q;
-        s->b_item_ptr[q + 1] = s->b_item_ptr[q] + (s->f_item_ptr[fq + 1] - s->f_item_ptr[fq]);
-    }
-    // packed L: off-diagonals ascending, in forward order
-    s->fp_ptr.assign(n + 1, 0);
-    s->fp_col.clear();
-    s->fp_src.clear();
-    s->fp_dsrc.assign(n, 0);
-    for (int p = 0; p < n; p++) {
-        const int row = s->f_ord[p];
-        const int lb = h.l_rowptr[row], le = h.l_rowptr[row + 1];
-        for (int e = lb; e < le - 1; e++) {
-            s->fp_col.push_back(h.l_colidx[e]);
-            s->fp_src.push_back(h.l_src[e]);
+    s->cptr.assign(n + 1, 0);
+    for (int c : h.l_colidx) s->cptr[c + 1]++;
+    for (int i = 0; i < n; i++) s->cptr[i + 1] += s->cptr[i];
+    s->crow.resize(h.l_colidx.size());
+    s->cpos.resize(h.l_colidx.size());
+    std::vector<int> cur(s->cptr.begin(), s->cptr.end() - 1);
+    for (int i = 0; i < n; i++)
+        for (int e = h.l_rowptr[i]; e < h.l_rowptr[i + 1]; e++) {
+            const int c = h.l_colidx[e];
+            s->crow[cur[c]] = i;
+            s->cpos[cur[c]] = e;
+            cur[c]++;
         }
-        s->fp_dsrc[p] = h.l_src[le - 1];
-        s->fp_ptr[p + 1] = (int)s->fp_col.size();
+}
+
+// Groups -> CTAs. RANGES: the CTA whose row range holds the group's first row (P contiguous,
+// row-balanced ranges). BAAS_THREADS: the four-rule mapping's thread of the group.
+void build_partition(baas_schedule *s, int P) {
+    const baas::HostSchedule &h = s->hs;
+    const int n = h.n;
+    s->P = P;
+    s->group_cta.assign(h.ngroups, 0);
+    if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) {
+        for (int t = 0; t < h.nthread; t++)
+            for (int task = h.thread_boundaries[t]; task < h.thread_boundaries[t + 1]; task++)
+                for (int q = h.task_boundaries[task]; q < h.task_boundaries[task + 1]; q++) s->group_cta[h.thread_cont_to_orig[q]] = t;
+    } else {
+        for (int g = 0; g < h.ngroups; g++) {
+            const int r0 = h.group_set[h.group_ptr[g]];
+            s->group_cta[g] = (int)(((long long)r0 * P) / n);
+        }
     }
-    // packed U = L^T: row j of U = column j of L; off-diagonals DESCENDING, in backward order
-    std::vector<int> cptr(n + 1, 0), crow, cpos;
-    for (int e = 0; e < (int)h.l_colidx.size(); e++) cptr[h.l_colidx[e] + 1]++;
-    for (int i = 0; i < n; i++) cptr[i + 1] += cptr[i];
-    crow.resize(h.l_colidx.size());
-    cpos.resize(h.l_colidx.size());
-    {
-        std::vector<int> cur(cptr.begin(), cptr.end() - 1);
-        for (int i = 0; i < n; i++)
-            for (int e = h.l_rowptr[i]; e < h.l_rowptr[i + 1]; e++) {
-                const int c = h.l_colidx[e];
-                crow[cur[c]] = i;
-                cpos[cur[c]] = e;
-                cur[c]++;
+    s->row_cta.assign(n, 0);
+    for (int g = 0; g < h.ngroups; g++)
+        for (int e = h.group_ptr[g]; e < h.group_ptr[g + 1]; e++) s->row_cta[h.group_set[e]] = s->group_cta[g];
+}
+
+// One direction of the plan. Forward: levels ascending, groups in LevelSet order, rows
+// ascending. Backward (U = L^T): the exact reverse.
+void build_dir(baas_schedule *s, bool upper, PartHost &out) {
+    const baas::HostSchedule &h = s->hs;
+    const int n = h.n, P = s->P, nl = h.nlevels;
+    out = PartHost();
+    // per CTA: list of (level, group) in processing order
+    std::vector<std::vector<std::pair<int, int>>> items(P);
+    for (int li = 0; li < nl; li++) {
+        const int l = upper ? nl - 1 - li : li;
+        const int qb = h.level_ptr[l], qe = h.level_ptr[l + 1];
+        for (int qi = 0; qi < qe - qb; qi++) {
+            const int q = upper ? qe - 1 - qi : qb + qi;
+            const int g = h.perm_to_orig[q];
+            items[s->group_cta[g]].push_back({l, g});
+        }
+    }
+    out.cta_seg.assign(1, 0);
+    out.seg_item.assign(1, 0);
+    out.item_pos.assign(1, 0);
+    out.cta_pos.assign(1, 0);
+    out.row.clear();
+    out.row.reserve(n);
+    for (int c = 0; c < P; c++) {
+        int last_level = -1;
+        for (auto &lg : items[c]) {
+            if (lg.first != last_level) {
+                if (last_level != -1) out.seg_item.push_back((int)out.item_pos.size() - 1);
+                last_level = lg.first;
             }
-    }
-    s->bp_ptr.assign(n + 1, 0);
-    s->bp_col.clear();
-    s->bp_src.clear();
-    s->bp_dsrc.assign(n, 0);
-    for (int p = 0; p < n; p++) {
-        const int j = s->b_ord[p];
-        // column j of L: rows ascending, first is the diagonal
-        for (int e = cptr[j + 1] - 1; e > cptr[j]; e--) {
-            s->bp_col.push_back(crow[e]);
-            s->bp_src.push_back(h.l_src[cpos[e]]);
+            const int g = lg.second;
+            const int rb = h.group_ptr[g], re = h.group_ptr[g + 1];
+            for (int k = 0; k < re - rb; k++) out.row.push_back(h.group_set[upper ? re - 1 - k : rb + k]);
+            out.item_pos.push_back((int)out.row.size());
         }
-        s->bp_dsrc[p] = h.l_src[cpos[cptr[j]]];
-        s->bp_ptr[p + 1] = (int)s->bp_col.size();
+        if (last_level != -1) out.seg_item.push_back((int)out.item_pos.size() - 1);
+        out.cta_seg.push_back((int)out.seg_item.size() - 1);
+        out.cta_pos.push_back((int)out.row.size());
+        out.max_local = std::max(out.max_local, out.cta_pos[c + 1] - out.cta_pos[c]);
     }
+    std::vector<int> slot(n, 0);
+    for (int c = 0; c < P; c++)
+        for (int pos = out.cta_pos[c]; pos < out.cta_pos[c + 1]; pos++) slot[out.row[pos]] = pos - out.cta_pos[c];
+    out.eptr.assign(n + 1, 0);
+    out.dsrcT.assign(n, 0);
+    out.dsrcA.assign(n, 0);
+    auto add = [&](int row, int col, int posT, int posA) {
+        out.dep.push_back(s->row_cta[col] == s->row_cta[row] ? -(slot[col] + 1) : col);
+        out.srcT.push_back(posT);
+        out.srcA.push_back(posA);
+    };
+    for (int pos = 0; pos < n; pos++) {
+        const int r = out.row[pos];
+        if (!upper) {
+            // L row r: off-diagonals ascending, diagonal last
+            const int lb = h.l_rowptr[r], le = h.l_rowptr[r + 1];
+            for (int e = lb; e < le - 1; e++) add(r, h.l_colidx[e], e, h.l_src[e]);
+            out.dsrcT[pos] = le - 1;
+            out.dsrcA[pos] = h.l_src[le - 1];
+        } else {
+            // U = L^T row r = column r of L: diagonal first, off-diagonals DESCENDING
+            const int cb = s->cptr[r], ce = s->cptr[r + 1];
+            for (int e = ce - 1; e > cb; e--) add(r, s->crow[e], e, h.l_src[s->cpos[e]]);
+            out.dsrcT[pos] = cb;
+            out.dsrcA[pos] = h.l_src[s->cpos[cb]];
+        }
+        out.eptr[pos + 1] = (int)out.dep.size();
+    }
+    if (!upper && s->fault_row >= 0) {
+        for (int pos = 0; pos < n; pos++)
+            if (out.row[pos] == s->fault_row && out.eptr[pos + 1] > out.eptr[pos]) out.dep[out.eptr[pos]] = s->fault_row;
+    }
+}
+
+// Staged plan from the two position plans: per CTA, each level segment becomes as many steps
+// as its largest group has rows; step j holds the j-th row of every group of the level.
+// Slots are the rows' local positions in the lower sweep's step order.
+void build_staged(baas_schedule *s) {
+    const int n = s->hs.n, P = s->P;
+    StagedHost &S = s->stg;
+    S = StagedHost();
+    std::vector<int> slot_of(n, 0);  // lower-sweep local position of each row
+    size_t smem64 = 0, smem32 = 0;
+    for (int d = 0; d < 2; d++) {
+        const PartHost &H = d == 0 ? s->fwd : s->bwd;
+        StagedHostDir &D = S.dir[d];
+        D.ioff.assign(P + 1, 0);
+        D.voff.assign(P + 1, 0);
+        std::vector<int> pos_of(n, 0);
+        for (int pos = 0; pos < n; pos++) pos_of[H.row[pos]] = pos;
+        for (int c = 0; c < P; c++) {
+            // rows of the CTA in step order
+            std::vector<int> step_row(1, 0), step_E, order;
+            for (int sg = H.cta_seg[c]; sg < H.cta_seg[c + 1]; sg++) {
+                int m = 0;
+                for (int it = H.seg_item[sg]; it < H.seg_item[sg + 1]; it++) m = std::max(m, H.item_pos[it + 1] - H.item_pos[it]);
+                for (int j = 0; j < m; j++) {
+                    int E = 0;
+                    for (int it = H.seg_item[sg]; it < H.seg_item[sg + 1]; it++)
+                        if (H.item_pos[it] + j < H.item_pos[it + 1]) {
+                            const int pos = H.item_pos[it] + j;
+                            order.push_back(pos);
+                            E = std::max(E, H.eptr[pos + 1] - H.eptr[pos]);
+                        }
+                    step_row.push_back((int)order.size());
+                    step_E.push_back(E);
+                }
+            }
+            const int nl = (int)order.size(), S_ = (int)step_E.size();
+            if (d == 0)
+                for (int k = 0; k < nl; k++) slot_of[H.row[order[k]]] = k;
+            std::vector<int> step_ent(S_, 0), ne(nl), rowid(nl), slot(nl), dep;
+            std::vector<int> dT(nl), dA(nl), vT, vA;
+            int ent = 0;
+            for (int st = 0; st < S_; st++) {
+                step_ent[st] = ent;
+                for (int k = step_row[st]; k < step_row[st + 1]; k++) {
+                    const int pos = order[k];
+                    const int r = H.row[pos];
+                    ne[k] = H.eptr[pos + 1] - H.eptr[pos];
+                    rowid[k] = r;
+                    slot[k] = slot_of[r];
+                    dT[k] = H.dsrcT[pos];
+                    dA[k] = H.dsrcA[pos];
+                    for (int j = 0; j < step_E[st]; j++) {
+                        if (j < ne[k]) {
+                            const int e = H.eptr[pos] + j;
+                            int dd = H.dep[e];
+                            if (dd < 0) dd = -(slot_of[H.row[H.cta_pos[c] + (-dd - 1)]] + 1);
+                            dep.push_back(dd);
+                            vT.push_back(H.srcT[e]);
+                            vA.push_back(H.srcA[e]);
+                        } else {
+                            dep.push_back(0);
+                            vT.push_back(-1);
+                            vA.push_back(-1);
+                        }
+                    }
+                }
+                ent += (step_row[st + 1] - step_row[st]) * step_E[st];
+            }
+            D.ns.push_back(S_);
+            D.nl.push_back(nl);
+            D.ne.push_back(ent);
+            D.ints.insert(D.ints.end(), step_row.begin(), step_row.end());
+            D.ints.insert(D.ints.end(), step_ent.begin(), step_ent.end());
+            D.ints.insert(D.ints.end(), step_E.begin(), step_E.end());
+            D.ints.insert(D.ints.end(), ne.begin(), ne.end());
+            D.ints.insert(D.ints.end(), rowid.begin(), rowid.end());
+            D.ints.insert(D.ints.end(), slot.begin(), slot.end());
+            D.ints.insert(D.ints.end(), dep.begin(), dep.end());
+            D.ints.resize(baas::pad4((int)D.ints.size()), 0);
+            D.ioff[c + 1] = (int)D.ints.size();
+            D.vsrcT.insert(D.vsrcT.end(), dT.begin(), dT.end());
+            D.vsrcT.insert(D.vsrcT.end(), vT.begin(), vT.end());
+            D.vsrcA.insert(D.vsrcA.end(), dA.begin(), dA.end());
+            D.vsrcA.insert(D.vsrcA.end(), vA.begin(), vA.end());
+            const int padded = baas::pad4((int)D.vsrcA.size());
+            D.vsrcT.resize(padded, -1);
+            D.vsrcA.resize(padded, -1);
+            D.voff[c + 1] = padded;
+            baas::StageLayout L64, L32;
+            L64.make<double>(S_, nl, ent);
+            L32.make<float>(S_, nl, ent);
+            smem64 = std::max(smem64, (size_t)L64.total);
+            smem32 = std::max(smem32, (size_t)L32.total);
+        }
+        // slack so the last block's 16-byte copies stay inside the arrays
+        D.ints.resize(D.ints.size() + 4, 0);
+        D.vsrcT.resize(D.vsrcT.size() + 4, -1);
+        D.vsrcA.resize(D.vsrcA.size() + 4, -1);
+    }
+    S.smem64 = smem64;
+    S.smem32 = smem32;
 }
 
 baas_status ensure_device(baas_schedule *s) {
@@ -179,40 +437,47 @@ baas_status ensure_device(baas_schedule *s) {
     if (!prop.cooperativeLaunch) return fail(BAAS_ERR_NO_DEVICE, "device lacks cooperative launch");
     s->num_sms = prop.multiProcessorCount;
     s->device = dev;
-    baas_status st;
-#define UP(d, h)                               \
-    if ((st = upload(d, h)) != BAAS_OK) return st;
-    UP(s->d_f_item_ptr, s->f_item_ptr);
-    UP(s->d_f_ord, s->f_ord);
-    UP(s->d_b_item_ptr, s->b_item_ptr);
-    UP(s->d_b_ord, s->b_ord);
-    UP(s->d_a_diag, s->hs.a_diagptr);
-    UP(s->d_fp_ptr, s->fp_ptr);
-    UP(s->d_fp_col, s->fp_col);
-    UP(s->d_fp_src, s->fp_src);
-    UP(s->d_fp_dsrc, s->fp_dsrc);
-    UP(s->d_bp_ptr, s->bp_ptr);
-    UP(s->d_bp_col, s->bp_col);
-    UP(s->d_bp_src, s->bp_src);
-    UP(s->d_bp_dsrc, s->bp_dsrc);
-#undef UP
-    if ((st = dalloc(s->d_status, 1)) != BAAS_OK) return st;
-    if ((st = dalloc(s->d_flags, (size_t)s->hs.n)) != BAAS_OK) return st;
-    if ((st = dalloc(s->d_bar, 1)) != BAAS_OK) return st;
-    BAAS_CUDA(cudaMallocHost((void **)&s->h_status, sizeof(DevStatus)));
-    s->uploaded = true;
-    return BAAS_OK;
-}
 
-// Persistent grid: co-resident CTAs (capped by the options and by the work available).
-template <typename K>
-baas_status grid_for(baas_schedule *s, K kernel, int work_items, int &grid) {
-    int per_sm = 0;
-    BAAS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, s->block(), 0));
-    if (per_sm <= 0) return fail(BAAS_ERR_CUDA, "kernel cannot be resident");
-    if (s->opt.ctas_per_sm > 0) per_sm = std::min(per_sm, s->opt.ctas_per_sm);
-    grid = per_sm * s->num_sms;
-    if (work_items > 0) grid = std::min(grid, std::max(1, (work_items + s->block() - 1) / s->block()));
+    // partition size: the fewest CTAs whose staged plan slice fits in shared memory
+    const int n = s->hs.n;
+    int P;
+    if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) {
+        P = s->hs.nthread;
+        if (s->opt.parts > 0 && s->opt.parts != P) return fail(BAAS_ERR_BAD_ARG, "BAAS_THREADS partition needs parts == nthread");
+    } else if (s->opt.parts > 0) {
+        P = std::min(s->opt.parts, n);
+    } else {
+        P = (int)std::max<long long>(1, ((long long)n * 48 + kSmemBudget - 1) / (long long)kSmemBudget);
+    }
+    for (;;) {
+        if (P > s->num_sms) return fail(BAAS_ERR_BAD_ARG, "the partition needs more CTAs than the device has SMs");
+        build_partition(s, P);
+        build_dir(s, false, s->fwd);
+        build_dir(s, true, s->bwd);
+        build_staged(s);
+        if (s->stg.smem64 <= kSmemBudget) break;
+        if (s->opt.parts > 0 || s->opt.partition == BAAS_PARTITION_BAAS_THREADS)
+            return fail(BAAS_ERR_BAD_ARG, "a CTA's plan slice does not fit in shared memory: raise `parts`");
+        P = std::min(s->num_sms, std::max(P + 1, (int)(P * 1.25)));
+    }
+
+    BAAS_TRY(upload_part(s->d_fwd, s->fwd));
+    BAAS_TRY(upload_part(s->d_bwd, s->bwd));
+    BAAS_TRY(upload_staged(s->d_stg, s->stg));
+    BAAS_TRY(upload(s->d_a_diag, s->hs.a_diagptr));
+    BAAS_TRY(dalloc(s->d_status, 1));
+    BAAS_TRY(dalloc(s->d_flags, (size_t)n));
+    BAAS_TRY(dalloc(s->d_bar, 1));
+    BAAS_CUDA(cudaMallocHost((void **)&s->h_status, sizeof(DevStatus)));
+    if (getenv("BAAS_TRACE") && atoi(getenv("BAAS_TRACE")) > 0) BAAS_TRY(dalloc(s->d_trace, 2 * baas::kTraceSlots));
+    // the partitioned kernels take up to kSmemBudget bytes of dynamic shared memory
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_factor_part<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_factor_part<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_sweep_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_sweep_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_iccg_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_iccg_staged<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+    s->uploaded = true;
     return BAAS_OK;
 }
 
@@ -237,9 +502,26 @@ baas_status read_status(baas_schedule *s, cudaStream_t stream) {
     return BAAS_OK;
 }
 
+// BAAS_TRACE=1: print the phase timestamps of the last launch (microseconds from its start).
+void dump_trace(baas_schedule *s, const char *what, cudaStream_t stream) {
+    if (!s->d_trace) return;
+    unsigned long long h[2 * baas::kTraceSlots];
+    if (cudaMemcpyAsync(h, s->d_trace, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess) return;
+    cudaStreamSynchronize(stream);
+    for (int c = 0; c < 2; c++) {
+        const unsigned long long *t = h + c * baas::kTraceSlots;
+        fprintf(stderr, "[baas trace] %s cta=%s:", what, c == 0 ? "first" : "last");
+        for (int k = 0; k < baas::kTraceSlots; k++)
+            if (t[k]) fprintf(stderr, " %d:%.1f", k, (double)(t[k] - t[0]) / 1000.0);
+        fprintf(stderr, "\n");
+    }
+    cudaMemsetAsync(s->d_trace, 0, sizeof(h), stream);
+}
+
 bool csr_ok(const baas_csr *m, int n, int nnz) {
     return m && m->n == n && m->nnz == nnz && m->rowptr && m->colidx && m->values;
 }
+
 
 }  // namespace
 
@@ -249,13 +531,13 @@ void baas_options_default(baas_options *opt) {
     if (!opt) return;
     opt->nthread = 8;
     opt->spin_limit = 0;
-    opt->block_size = 0;
-    opt->ctas_per_sm = 0;
+    opt->parts = 0;
+    opt->partition = BAAS_PARTITION_RANGES;
 }
 
 const char *baas_last_error_string(void) { return g_err.c_str(); }
 
-const char *baas_version(void) { return "baas_b200 0.1.0 (sm_100a)"; }
+const char *baas_version(void) { return "baas_b200 0.2.0 (sm_100a)"; }
 
 baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options *opt, baas_schedule **out) {
     if (!A || !out) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
@@ -265,6 +547,9 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     baas_options_default(&o);
     if (opt) o = *opt;
     if (o.nthread < 1) return fail(BAAS_ERR_BAD_ARG, "nthread must be >= 1");
+    if (o.partition != BAAS_PARTITION_RANGES && o.partition != BAAS_PARTITION_BAAS_THREADS)
+        return fail(BAAS_ERR_BAD_ARG, "unknown partition");
+    if (o.parts < 0) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 0");
     if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
     if (A->rowptr[A->n] != A->nnz) return fail(BAAS_ERR_BAD_ARG, "nnz != rowptr[n]");
     const baas::SchedKind sk = (baas::SchedKind)kind;
@@ -279,7 +564,7 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         delete s;
         return fail(BAAS_ERR_BAD_ARG, "the pattern must be structurally symmetric");
     }
-    build_plan(s);
+    build_order(s);
     *out = s;
     return BAAS_OK;
 }
@@ -324,20 +609,34 @@ int baas_schedule_export(const baas_schedule *s, int field, int *out) {
 
 double baas_schedule_analysis_ms(const baas_schedule *s) { return s ? s->hs.analysis_ms : 0.0; }
 
+baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row) {
+    if (!s || row < 0 || row >= s->hs.n) return fail(BAAS_ERR_BAD_ARG, "bad row");
+    const int lb = s->hs.l_rowptr[row], le = s->hs.l_rowptr[row + 1];
+    if (le - lb < 2) return fail(BAAS_ERR_BAD_ARG, "the row has no off-diagonal entry");
+    if (s->uploaded) return fail(BAAS_ERR_STATE, "inject before the first GPU call on the schedule");
+    s->fault_row = row;
+    return BAAS_OK;
+}
+
 void baas_destroy(baas_schedule *s) {
     if (!s) return;
     if (s->uploaded) {
         int cur = -1;
         cudaGetDevice(&cur);
         if (cur != s->device) cudaSetDevice(s->device);
-        void *ptrs[] = {s->d_f_item_ptr, s->d_f_ord, s->d_b_item_ptr, s->d_b_ord, s->d_a_diag, s->d_fp_ptr, s->d_fp_col,
-                        s->d_fp_src, s->d_fp_dsrc, s->d_bp_ptr, s->d_bp_col, s->d_bp_src, s->d_bp_dsrc, s->d_status,
-                        s->d_flags, s->d_bar, s->d_lu, s->d_r, s->d_y, s->d_z, s->d_p, s->d_Ap, s->d_y32, s->d_z32,
-                        s->d_fp_val, s->d_fp_diag, s->d_bp_val, s->d_bp_diag, s->d_fp_val32, s->d_fp_diag32,
-                        s->d_bp_val32, s->d_bp_diag32, s->d_part, s->d_iters, s->d_relres};
+        s->d_fwd.release();
+        s->d_bwd.release();
+        s->d_stg.release();
+        for (int d = 0; d < 2; d++) {
+            if (s->d_gv64[d]) cudaFree(s->d_gv64[d]);
+            if (s->d_gv32[d]) cudaFree(s->d_gv32[d]);
+        }
+        void *ptrs[] = {s->d_a_diag, s->d_status, s->d_flags, s->d_bar, s->d_lu, s->d_r, s->d_y, s->d_z, s->d_p,
+                        s->d_Ap, s->d_y32, s->d_z32, s->d_part, s->d_iters, s->d_relres};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         if (s->h_status) cudaFreeHost(s->h_status);
+        if (s->d_trace) cudaFree(s->d_trace);
         if (cur >= 0 && cur != s->device) cudaSetDevice(cur);
     }
     delete s;
@@ -350,30 +649,22 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
     if (!csr_ok(T, n, s->nnz_l)) return fail(BAAS_ERR_BAD_ARG, "triangular factor does not match the analysed pattern");
     if (nrhs < 1 || ldb < n) return fail(BAAS_ERR_BAD_ARG, "nrhs must be >= 1 and ldb >= n");
     if (x == b) return fail(BAAS_ERR_BAD_ARG, "x must not alias b");
-    baas_status st = ensure_device(s);
-    if (st != BAAS_OK) return st;
+    BAAS_TRY(ensure_device(s));
     cudaStream_t stream = (cudaStream_t)stream_;
     BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
     {
-        const int fill_blocks = std::min(4 * s->num_sms, (int)(((long long)n * nrhs + 255) / 256));
+        const int fill_blocks = (int)std::min<long long>(4LL * s->num_sms, ((long long)n * nrhs + 255) / 256);
         baas::k_fill_sentinel<double><<<std::max(fill_blocks, 1), 256, 0, stream>>>(x, n, nrhs, ldb);
         BAAS_CUDA(cudaGetLastError());
     }
-    const int nitems = s->hs.ngroups;
-    const int *item_ptr = upper ? s->d_b_item_ptr : s->d_f_item_ptr;
-    const int *ord = upper ? s->d_b_ord : s->d_f_ord;
+    baas::StagedPlan pl = s->d_stg.plan(s->P);
     unsigned int spin = s->spin();
-    int grid = 0;
-    void *args[] = {(void *)&nitems, (void *)&item_ptr, (void *)&ord, (void *)&T->rowptr, (void *)&T->colidx,
-                    (void *)&T->values, (void *)&b, (void *)&ldb, (void *)&x, (void *)&ldb, (void *)&nrhs,
-                    (void *)&s->d_status, (void *)&spin};
-    if (upper) {
-        if ((st = grid_for(s, baas::k_sweep_csr<true>, nitems, grid)) != BAAS_OK) return st;
-        BAAS_CUDA(cudaLaunchCooperativeKernel((void *)baas::k_sweep_csr<true>, grid, s->block(), args, 0, stream));
-    } else {
-        if ((st = grid_for(s, baas::k_sweep_csr<false>, nitems, grid)) != BAAS_OK) return st;
-        BAAS_CUDA(cudaLaunchCooperativeKernel((void *)baas::k_sweep_csr<false>, grid, s->block(), args, 0, stream));
-    }
+    void *args[] = {(void *)&pl, (void *)&T->values, (void *)&b, (void *)&ldb, (void *)&x, (void *)&ldb,
+                    (void *)&nrhs, (void *)&s->d_status, (void *)&spin, (void *)&s->d_trace};
+    void *kern = upper ? (void *)baas::k_sweep_staged<true> : (void *)baas::k_sweep_staged<false>;
+
+    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, s->P, baas::kStageBlock, args, s->stg.smem64, stream));
+    dump_trace(s, upper ? "sptrsv-upper" : "sptrsv-lower", stream);
     return read_status(s, stream);
 }
 
@@ -382,24 +673,16 @@ static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void 
     if (s->hs.kind == baas::SchedKind::SpTRSV) return fail(BAAS_ERR_STATE, "a SpTRSV schedule cannot drive a factorisation");
     if (!A || A->n != s->hs.n || A->nnz != s->nnz_a || !A->rowptr || !A->colidx)
         return fail(BAAS_ERR_BAD_ARG, "matrix does not match the analysed pattern");
-    baas_status st = ensure_device(s);
-    if (st != BAAS_OK) return st;
+    BAAS_TRY(ensure_device(s));
     cudaStream_t stream = (cudaStream_t)stream_;
-    if ((st = next_epoch(s, stream)) != BAAS_OK) return st;
+    BAAS_TRY(next_epoch(s, stream));
     BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-    const int nitems = s->hs.ngroups;
+    baas::PartView pv = s->d_fwd.view(s->P);
     unsigned int spin = s->spin();
-    int grid = 0;
-    void *args[] = {(void *)&nitems, (void *)&s->d_f_item_ptr, (void *)&s->d_f_ord, (void *)&A->rowptr,
-                    (void *)&A->colidx, (void *)&s->d_a_diag, (void *)&lu, (void *)&s->d_flags, (void *)&s->epoch,
-                    (void *)&s->d_status, (void *)&spin};
-    if (ilu) {
-        if ((st = grid_for(s, baas::k_factor<true>, nitems, grid)) != BAAS_OK) return st;
-        BAAS_CUDA(cudaLaunchCooperativeKernel((void *)baas::k_factor<true>, grid, s->block(), args, 0, stream));
-    } else {
-        if ((st = grid_for(s, baas::k_factor<false>, nitems, grid)) != BAAS_OK) return st;
-        BAAS_CUDA(cudaLaunchCooperativeKernel((void *)baas::k_factor<false>, grid, s->block(), args, 0, stream));
-    }
+    void *args[] = {(void *)&pv, (void *)&A->rowptr, (void *)&A->colidx, (void *)&s->d_a_diag, (void *)&lu,
+                    (void *)&s->d_flags, (void *)&s->epoch, (void *)&s->d_status, (void *)&spin};
+    void *kern = ilu ? (void *)baas::k_factor_part<true> : (void *)baas::k_factor_part<false>;
+    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, s->P, baas::kPartBlock, args, (size_t)s->fwd.max_local * 4, stream));
     return read_status(s, stream);
 }
 
@@ -414,33 +697,33 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
     if (!csr_ok(A, s->hs.n, s->nnz_a)) return fail(BAAS_ERR_BAD_ARG, "matrix does not match the analysed pattern");
     if (maxiter < 0 || !(tol >= 0.0)) return fail(BAAS_ERR_BAD_ARG, "maxiter must be >= 0 and tol >= 0");
     if (precision != BAAS_PREC_FP64 && precision != BAAS_PREC_FP32_FACTORS) return fail(BAAS_ERR_BAD_ARG, "unknown precision");
-    baas_status st = ensure_device(s);
-    if (st != BAAS_OK) return st;
+    BAAS_TRY(ensure_device(s));
     cudaStream_t stream = (cudaStream_t)stream_;
     const int n = s->hs.n;
-    int grid = 0;
-    if ((st = grid_for(s, baas::k_iccg, 0, grid)) != BAAS_OK) return st;
+    const int P = s->P;
     if (!s->ws_ready) {
-        const size_t nf = std::max<size_t>(s->fp_col.size(), 1), nbk = std::max<size_t>(s->bp_col.size(), 1);
-        if ((st = dalloc(s->d_lu, (size_t)s->nnz_a)) != BAAS_OK) return st;
-        if ((st = dalloc(s->d_r, n)) || (st = dalloc(s->d_y, n)) || (st = dalloc(s->d_z, n)) || (st = dalloc(s->d_p, n)) ||
-            (st = dalloc(s->d_Ap, n)) || (st = dalloc(s->d_y32, n)) || (st = dalloc(s->d_z32, n)))
-            return st;
-        if ((st = dalloc(s->d_fp_val, nf)) || (st = dalloc(s->d_bp_val, nbk)) || (st = dalloc(s->d_fp_val32, nf)) ||
-            (st = dalloc(s->d_bp_val32, nbk)) || (st = dalloc(s->d_fp_diag, n)) || (st = dalloc(s->d_bp_diag, n)) ||
-            (st = dalloc(s->d_fp_diag32, n)) || (st = dalloc(s->d_bp_diag32, n)))
-            return st;
-        s->part_cap = grid;
-        if ((st = dalloc(s->d_part, (size_t)3 * grid)) || (st = dalloc(s->d_iters, 1)) || (st = dalloc(s->d_relres, 1)))
-            return st;
+        BAAS_TRY(dalloc(s->d_lu, (size_t)s->nnz_a));
+        BAAS_TRY(dalloc(s->d_r, n));
+        BAAS_TRY(dalloc(s->d_y, n));
+        BAAS_TRY(dalloc(s->d_z, n));
+        BAAS_TRY(dalloc(s->d_p, n));
+        BAAS_TRY(dalloc(s->d_Ap, n));
+        BAAS_TRY(dalloc(s->d_y32, n));
+        BAAS_TRY(dalloc(s->d_z32, n));
+        for (int d = 0; d < 2; d++) {
+            BAAS_TRY(dalloc(s->d_gv64[d], s->stg.dir[d].vsrcA.size()));
+            BAAS_TRY(dalloc(s->d_gv32[d], s->stg.dir[d].vsrcA.size()));
+        }
+        BAAS_TRY(dalloc(s->d_part, (size_t)3 * P));
+        BAAS_TRY(dalloc(s->d_iters, 1));
+        BAAS_TRY(dalloc(s->d_relres, 1));
         s->ws_ready = true;
     }
-    if (grid > s->part_cap) return fail(BAAS_ERR_STATE, "grid grew after the workspace was sized");
-    if ((st = next_epoch(s, stream)) != BAAS_OK) return st;
+    BAAS_TRY(next_epoch(s, stream));
     BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
     BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
 
-    baas::IccgArgs a{};
+    baas::StagedIccgArgs a{};
     a.n = n;
     a.a_rowptr = A->rowptr;
     a.a_colidx = A->colidx;
@@ -448,31 +731,16 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
     a.a_val = A->values;
     a.b = b;
     a.x = x;
-    a.nitems = s->hs.ngroups;
-    a.f_item_ptr = s->d_f_item_ptr;
-    a.f_ord = s->d_f_ord;
-    a.b_item_ptr = s->d_b_item_ptr;
-    a.b_ord = s->d_b_ord;
-    a.fp_ptr = s->d_fp_ptr;
-    a.fp_col = s->d_fp_col;
-    a.fp_src = s->d_fp_src;
-    a.fp_dsrc = s->d_fp_dsrc;
-    a.bp_ptr = s->d_bp_ptr;
-    a.bp_col = s->d_bp_col;
-    a.bp_src = s->d_bp_src;
-    a.bp_dsrc = s->d_bp_dsrc;
-    a.fp_val = s->d_fp_val;
-    a.fp_diag = s->d_fp_diag;
-    a.bp_val = s->d_bp_val;
-    a.bp_diag = s->d_bp_diag;
-    a.fp_val32 = s->d_fp_val32;
-    a.fp_diag32 = s->d_fp_diag32;
-    a.bp_val32 = s->d_bp_val32;
-    a.bp_diag32 = s->d_bp_diag32;
-    a.nnzf = (int)s->fp_col.size();
-    a.nnzb = (int)s->bp_col.size();
+    a.fac = s->d_fwd.view(P);
+    a.pl = s->d_stg.plan(P);
+    a.nv[0] = (int)s->stg.dir[0].vsrcA.size();
+    a.nv[1] = (int)s->stg.dir[1].vsrcA.size();
+    for (int d = 0; d < 2; d++) {
+        a.gv64[d] = s->d_gv64[d];
+        a.gv32[d] = s->d_gv32[d];
+    }
     a.lu = s->d_lu;
-    a.flags = s->d_flags;
+    a.gflag = s->d_flags;
     a.epoch = s->epoch;
     a.r = s->d_r;
     a.y = s->d_y;
@@ -482,23 +750,26 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
     a.y32 = s->d_y32;
     a.z32 = s->d_z32;
     a.part_a = s->d_part;
-    a.part_b = s->d_part + grid;
-    a.part_c = s->d_part + 2 * grid;
+    a.part_b = s->d_part + P;
+    a.part_c = s->d_part + 2 * P;
     a.bar = s->d_bar;
     a.st = s->d_status;
     a.maxiter = maxiter;
     a.tol = tol;
-    a.mixed = precision == BAAS_PREC_FP32_FACTORS;
     a.out_iters = s->d_iters;
     a.out_relres = s->d_relres;
     a.spin_limit = s->spin();
+    a.trace = s->d_trace;
     void *args[] = {(void *)&a};
-    BAAS_CUDA(cudaLaunchCooperativeKernel((void *)baas::k_iccg, grid, s->block(), args, 0, stream));
+    const bool mixed = precision == BAAS_PREC_FP32_FACTORS;
+    void *kern = mixed ? (void *)baas::k_iccg_staged<float> : (void *)baas::k_iccg_staged<double>;
+    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, P, baas::kStageBlock, args, mixed ? s->stg.smem32 : s->stg.smem64, stream));
     int it = 0;
     double rr = 0.0;
     BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));
     BAAS_CUDA(cudaMemcpyAsync(&rr, s->d_relres, sizeof(double), cudaMemcpyDeviceToHost, stream));
-    st = read_status(s, stream);
+    dump_trace(s, "iccg", stream);
+    baas_status st = read_status(s, stream);
     if (iters) *iters = it;
     if (relres) *relres = rr;
     if (st != BAAS_OK) return st;

@@ -1,0 +1,197 @@
+// Partitioned, level-synchronous kernels: the production execution of the BAAS hot path.
+//
+// Rows are owned by P CTAs (contiguous row ranges by default; one 512-thread CTA per SM). The
+// schedule's coarsened groups are the work items, and each CTA walks the schedule's global
+// group levels in order: at level l it runs its own groups of level l (one group per thread,
+// the group's rows in ascending order, exactly as one reference thread runs a group,
+// merge/SpTRSV.cpp:458-471), then a CTA barrier. So
+//   - a dependency on a row of the same CTA needs no wait at all: the barrier (or program
+//     order, inside a group) already made it visible, and its value is read from shared memory;
+//   - a dependency on a row of another CTA is a point-to-point wait on that row's global slot
+//     (the value itself is the ready flag for the sweeps; a release/acquire row flag for the
+//     factorisations), the analogue of the reference's taskFinsished waits
+//     (merge/include/SpTRSV.hpp:16-35).
+// A group of level l depends only on groups of levels < l and every CTA walks the levels in
+// the same increasing order, so by induction on l every CTA finishes every level: no deadlock
+// while all CTAs are resident (cooperative launch). With contiguous row ranges every cross-CTA
+// dependency of the lower sweep points to a later CTA, so a downstream CTA settles at a fixed
+// lag behind its upstream neighbour: the L2 hop (~360 ns one way on B200) is paid once per
+// range boundary on the critical path, not once per level.
+//
+// Dependency encoding per factor entry: dep >= 0 is a global row index (remote), dep < 0 is
+// -(slot + 1) with slot the CTA-local index of a row computed earlier by this CTA.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace baas {
+
+constexpr int kPartBlock = 512;
+
+struct PartView {
+    int P;
+    const int *cta_seg;   // P + 1: level segments of each CTA
+    const int *seg_item;  // nseg + 1: items (groups) of each segment
+    const int *item_pos;  // nitem + 1: positions (rows) of each item
+    const int *cta_pos;   // P + 1: first position of each CTA (local slot = pos - cta_pos[c])
+    const int *row;       // position -> row
+    const int *eptr;      // position -> off-diagonal entries [eptr[pos], eptr[pos+1])
+    const int *dep;       // entry -> encoded dependency
+};
+
+// Walks this CTA's level segments; `row_fn(pos, slot)` computes one row (false = give up).
+// Every thread passes every barrier, also after a failed wait, so the CTA never splits.
+template <typename RowFn>
+__device__ __forceinline__ bool walk_levels(const PartView &pv, RowFn row_fn) {
+    const int c = blockIdx.x;
+    const int pos0 = __ldg(pv.cta_pos + c);
+    const int sb = __ldg(pv.cta_seg + c), se = __ldg(pv.cta_seg + c + 1);
+    bool alive = true;
+    for (int sg = sb; sg < se; sg++) {
+        const int ib = __ldg(pv.seg_item + sg), ie = __ldg(pv.seg_item + sg + 1);
+        for (int it = ib + (int)threadIdx.x; it < ie && alive; it += blockDim.x) {
+            const int pb = __ldg(pv.item_pos + it), pe = __ldg(pv.item_pos + it + 1);
+            for (int pos = pb; pos < pe; pos++)
+                if (!row_fn(pos, pos - pos0)) {
+                    alive = false;
+                    break;
+                }
+        }
+        __syncthreads();
+    }
+    return alive;
+}
+
+// ---------------------------------------------------------------------------------------
+// Level-synchronous IC0 / ILU0. A row of this CTA from an earlier level is final after the
+// barrier and is read through L1; a row of another CTA is waited for on its epoch-stamped
+// global flag (acquire) and read from L2. Every row publishes its flag with a release store.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double ld_l2(const double *p) { return Sent<double>::load(p); }
+
+template <bool LOCAL>
+__device__ __forceinline__ double ldv(const double *p) {
+    if constexpr (LOCAL)
+        return *p;
+    else
+        return ld_l2(p);
+}
+
+// IC0 row i (merge/IC.cpp:296-393; sparse_dot_product :6-29), correctly rounded FP64.
+template <bool LOCAL>
+__device__ __forceinline__ double ic0_dot(int l1, int u1, int l2, int u2, const int *__restrict__ colidx, const double *lu) {
+    double dp = 0.0;
+    while (l1 < u1 && l2 < u2) {
+        const int c1 = __ldg(colidx + l1), c2 = __ldg(colidx + l2);
+        if (c1 == c2) {
+            dp = __dadd_rn(dp, __dmul_rn(lu[l1], ldv<LOCAL>(lu + l2)));
+            l1++;
+            l2++;
+        } else if (c1 < c2) {
+            l1++;
+        } else {
+            l2++;
+        }
+    }
+    return dp;
+}
+
+__device__ __forceinline__ bool ic0_row_part(const PartView &pv, int pos, int i, const int *__restrict__ rowptr,
+                                             const int *__restrict__ colidx, const int *__restrict__ diagptr, double *lu,
+                                             const int *gflag, int epoch, Waiter &w, DevStatus *st) {
+    const int rb = __ldg(rowptr + i), di = __ldg(diagptr + i), e0 = __ldg(pv.eptr + pos);
+    for (int k = rb; k < di; k++) {
+        const int j = __ldg(colidx + k);
+        const int d = __ldg(pv.dep + e0 + (k - rb));
+        const int l2 = __ldg(rowptr + j), u2 = __ldg(diagptr + j);
+        double dp, ljj;
+        if (d < 0) {
+            dp = ic0_dot<true>(rb, di, l2, u2, colidx, lu);
+            ljj = ldv<true>(lu + u2);
+        } else {
+            if (!wait_flag(gflag + j, epoch, w, i)) return false;
+            dp = ic0_dot<false>(rb, di, l2, u2, colidx, lu);
+            ljj = ldv<false>(lu + u2);
+        }
+        lu[k] = __ddiv_rn(__dsub_rn(lu[k], dp), ljj);
+    }
+    double dv = 0.0;
+    for (int k = rb; k < di; k++) dv = __dadd_rn(dv, __dmul_rn(lu[k], lu[k]));
+    const double t = __dsub_rn(lu[di], dv);
+    if (t > 0.0)
+        lu[di] = __dsqrt_rn(t);
+    else
+        atomicAdd(&st->zero_pivots, 1);
+    return true;
+}
+
+// ILU0 row i (merge/ILU.cpp:638-720).
+template <bool LOCAL>
+__device__ __forceinline__ void ilu0_update(int j, int re, int dc, int ec, double tmp, const int *__restrict__ colidx,
+                                            double *lu) {
+    int k1 = j + 1, k2 = dc + 1;
+    while (k1 < re && k2 < ec) {
+        const int c1 = __ldg(colidx + k1), c2 = __ldg(colidx + k2);
+        if (c1 < c2) {
+            k1++;
+        } else if (c1 > c2) {
+            k2++;
+        } else {
+            lu[k1] = __dsub_rn(lu[k1], __dmul_rn(tmp, ldv<LOCAL>(lu + k2)));
+            k1++;
+            k2++;
+        }
+    }
+}
+
+__device__ __forceinline__ bool ilu0_row_part(const PartView &pv, int pos, int i, const int *__restrict__ rowptr,
+                                              const int *__restrict__ colidx, const int *__restrict__ diagptr, double *lu,
+                                              const int *gflag, int epoch, Waiter &w, DevStatus *st) {
+    const int rb = __ldg(rowptr + i), di = __ldg(diagptr + i), re = __ldg(rowptr + i + 1), e0 = __ldg(pv.eptr + pos);
+    for (int j = rb; j < di; j++) {
+        const int c = __ldg(colidx + j);
+        const int d = __ldg(pv.dep + e0 + (j - rb));
+        const int dc = __ldg(diagptr + c), ec = __ldg(rowptr + c + 1);
+        if (d >= 0 && !wait_flag(gflag + c, epoch, w, i)) return false;
+        const double pivot = d < 0 ? ldv<true>(lu + dc) : ldv<false>(lu + dc);
+        if (pivot == 0.0) atomicAdd(&st->zero_pivots, 1);
+        const double tmp = __ddiv_rn(lu[j], pivot);
+        lu[j] = tmp;
+        if (d < 0)
+            ilu0_update<true>(j, re, dc, ec, tmp, colidx, lu);
+        else
+            ilu0_update<false>(j, re, dc, ec, tmp, colidx, lu);
+    }
+    return true;
+}
+
+template <bool ILU>
+__device__ __forceinline__ bool factor_part(const PartView &pv, const int *rowptr, const int *colidx, const int *diagptr,
+                                            double *lu, int *gflag, int epoch, Waiter &w, DevStatus *st) {
+    return walk_levels(pv, [&](int pos, int) {
+        const int row = __ldg(pv.row + pos);
+        const bool ok = ILU ? ilu0_row_part(pv, pos, row, rowptr, colidx, diagptr, lu, gflag, epoch, w, st)
+                            : ic0_row_part(pv, pos, row, rowptr, colidx, diagptr, lu, gflag, epoch, w, st);
+        if (!ok) return false;
+        __threadfence();
+        st_release_s32(gflag + row, epoch);
+        return true;
+    });
+}
+
+template <bool ILU>
+__global__ void __launch_bounds__(kPartBlock, 1) k_factor_part(PartView pv, const int *__restrict__ rowptr,
+                                                              const int *__restrict__ colidx,
+                                                              const int *__restrict__ diagptr, double *lu, int *gflag,
+                                                              int epoch, DevStatus *st, unsigned int spin_limit) {
+    Waiter w(spin_limit, st);
+    factor_part<ILU>(pv, rowptr, colidx, diagptr, lu, gflag, epoch, w, st);
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void put_partial(double *part, double v) {
+    const double s = block_sum<BLOCK>(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+}  // namespace baas

@@ -102,9 +102,15 @@ typedef struct baas_csr {
 typedef struct baas_options {
     int nthread;      /* the reference's num_thread: virtual threads of the schedule (>= 1) */
     int spin_limit;   /* polls before a device wait gives up (0 = library default) */
-    int block_size;   /* threads per CTA of the persistent kernels (0 = library default) */
-    int ctas_per_sm;  /* persistent CTAs per SM (0 = as many as are co-resident) */
+    int parts;        /* CTAs that own rows in the partitioned kernels (0 = automatic: the fewest
+                         whose rows fit in shared memory, at most one per SM) */
+    int partition;    /* BAAS_PARTITION_RANGES (default) or BAAS_PARTITION_BAAS_THREADS */
 } baas_options;
+
+/* How rows are given to CTAs. RANGES: contiguous row-index ranges, so every cross-CTA
+ * dependency of the lower sweep points to a later CTA. BAAS_THREADS: CTA t runs the groups the
+ * four-rule mapping gives virtual thread t (requires parts == nthread or parts == 0). */
+enum { BAAS_PARTITION_RANGES = 0, BAAS_PARTITION_BAAS_THREADS = 1 };
 
 typedef struct baas_schedule baas_schedule;
 
@@ -128,6 +134,13 @@ double baas_schedule_analysis_ms(const baas_schedule *s);
 
 /* Frees the schedule and its device memory. */
 void baas_destroy(baas_schedule *s);
+
+/* Failure-detection test hook (no counterpart in the reference, whose waits never end):
+ * makes the forward sweep's row `row` wait on a value that nothing ever writes, so the next
+ * forward sweep on this schedule ends with BAAS_ERR_TIMEOUT after spin_limit polls while every
+ * memory access stays in bounds and the CUDA context stays usable. Must be called before the
+ * schedule's first GPU call; `row` needs an off-diagonal entry in L. */
+baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row);
 
 /* Forward sweep x = L^-1 b (upper = 0; L is the analysed lower triangle, diagonal LAST in each
  * row) or backward sweep x = U^-1 b (upper = 1; U has the transposed pattern, diagonal FIRST).

@@ -101,14 +101,16 @@ class Ref:
 
         def forward(self, L, b: np.ndarray) -> np.ndarray:
             x = np.zeros(L.n)
+            bc = np.ascontiguousarray(b, dtype=np.float64)
             Ref.lib().ref_sptrsv_forward(self.h, L.n, _p(L.rowptr), _p(L.colidx), _p(L.values), _p(x),
-                                         _p(np.ascontiguousarray(b)))
+                                         _p(bc))
             return x
 
         def backward(self, U, b: np.ndarray) -> np.ndarray:
             x = np.zeros(U.n)
+            bc = np.ascontiguousarray(b, dtype=np.float64)
             Ref.lib().ref_sptrsv_backward(self.h, U.n, _p(U.rowptr), _p(U.colidx), _p(U.values), _p(x),
-                                          _p(np.ascontiguousarray(b)))
+                                          _p(bc))
             return x
 
         def ic0(self, A) -> np.ndarray:
@@ -124,13 +126,15 @@ class Ref:
     @staticmethod
     def sptrsv_serial(L, b) -> np.ndarray:
         x = np.zeros(L.n)
-        Ref.lib().ref_sptrsv_serial(L.n, _p(L.rowptr), _p(L.colidx), _p(L.values), _p(x), _p(np.ascontiguousarray(b)))
+        bc = np.ascontiguousarray(b, dtype=np.float64)
+        Ref.lib().ref_sptrsv_serial(L.n, _p(L.rowptr), _p(L.colidx), _p(L.values), _p(x), _p(bc))
         return x
 
     @staticmethod
     def upper_serial(U, b) -> np.ndarray:
         x = np.zeros(U.n)
-        Ref.lib().ref_upper_serial(U.n, _p(U.rowptr), _p(U.colidx), _p(U.values), _p(x), _p(np.ascontiguousarray(b)))
+        bc = np.ascontiguousarray(b, dtype=np.float64)
+        Ref.lib().ref_upper_serial(U.n, _p(U.rowptr), _p(U.colidx), _p(U.values), _p(x), _p(bc))
         return x
 
     @staticmethod
@@ -152,8 +156,9 @@ class Ref:
         x = np.zeros(A.n) if x0 is None else np.array(x0, dtype=np.float64)
         rel = C.c_double(0.0)
         t = np.zeros(5)
+        bc = np.ascontiguousarray(b, dtype=np.float64)
         it = Ref.lib().ref_pcg(mode, nthread, A.n, _p(A.rowptr), _p(A.colidx), _p(A.values),
-                               _p(np.ascontiguousarray(b)), _p(x), maxiter, tol, C.addressof(rel), _p(t))
+                               _p(bc), _p(x), maxiter, tol, C.addressof(rel), _p(t))
         return x, it, rel.value, t
 
 
@@ -184,32 +189,37 @@ class Port:
     @staticmethod
     def lower_solve(L, b):
         x = np.zeros(L.n)
-        Port.lib().orc_lower_solve(L.n, _p(L.rowptr), _p(L.colidx), _p(L.values), _p(np.ascontiguousarray(b)), _p(x))
+        bc = np.ascontiguousarray(b, dtype=np.float64)
+        Port.lib().orc_lower_solve(L.n, _p(L.rowptr), _p(L.colidx), _p(L.values), _p(bc), _p(x))
         return x
 
     @staticmethod
     def upper_solve(U, b, descending=True):
         x = np.zeros(U.n)
+        bc = np.ascontiguousarray(b, dtype=np.float64)
         f = Port.lib().orc_upper_solve_desc if descending else Port.lib().orc_upper_solve_asc
-        f(U.n, _p(U.rowptr), _p(U.colidx), _p(U.values), _p(np.ascontiguousarray(b)), _p(x))
+        f(U.n, _p(U.rowptr), _p(U.colidx), _p(U.values), _p(bc), _p(x))
         return x
 
     @staticmethod
     def ic0(A):
         lu = A.values.copy()
-        bad = Port.lib().orc_ic0(A.n, _p(A.rowptr), _p(A.colidx), _p(A.diagptr()), _p(lu))
+        dp = A.diagptr()
+        bad = Port.lib().orc_ic0(A.n, _p(A.rowptr), _p(A.colidx), _p(dp), _p(lu))
         return lu, bad
 
     @staticmethod
     def ilu0(A):
         lu = A.values.copy()
-        bad = Port.lib().orc_ilu0(A.n, _p(A.rowptr), _p(A.colidx), _p(A.diagptr()), _p(lu))
+        dp = A.diagptr()
+        bad = Port.lib().orc_ilu0(A.n, _p(A.rowptr), _p(A.colidx), _p(dp), _p(lu))
         return lu, bad
 
     @staticmethod
     def spmv(A, x, y=None, alpha=1.0, beta=0.0):
         y = np.zeros(A.n) if y is None else np.array(y, dtype=np.float64)
-        Port.lib().orc_spmv(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(np.ascontiguousarray(x)), _p(y), alpha, beta)
+        xc = np.ascontiguousarray(x, dtype=np.float64)
+        Port.lib().orc_spmv(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(xc), _p(y), alpha, beta)
         return y
 
     @staticmethod
@@ -217,6 +227,7 @@ class Port:
         """IC0-PCG with serial IC0 and serial sweeps; returns (x, iterations, relres)."""
         x = np.zeros(A.n) if x0 is None else np.array(x0, dtype=np.float64)
         rel = C.c_double(0.0)
-        it = Port.lib().orc_pcg(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(np.ascontiguousarray(b)), _p(x),
+        bc = np.ascontiguousarray(b, dtype=np.float64)
+        it = Port.lib().orc_pcg(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(bc), _p(x),
                                 maxiter, tol, C.addressof(rel), None)
         return x, it, rel.value
