@@ -147,6 +147,13 @@ class Schedule:
         c = A.c()
         _native.check(_native.lib().baas_ic0(self._h, C.byref(c), _ptr(lu), _stream_ptr(stream)), "baas_ic0")
 
+    def ic0_noalloc(self, A: DeviceCSR, lu, stream=None) -> None:
+        """IC0 that allocates no device memory (static scratch inside the library; at most
+        2,097,152 rows). The schedule must have run one ordinary GPU call first."""
+        c = A.c()
+        _native.check(_native.lib().baas_ic0_noalloc(self._h, C.byref(c), _ptr(lu), _stream_ptr(stream)),
+                      "baas_ic0_noalloc")
+
     def ilu0(self, A: DeviceCSR, lu, stream=None) -> None:
         """ILU0 in place on lu (pre-filled with A.values)."""
         c = A.c()

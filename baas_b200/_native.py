@@ -37,7 +37,7 @@ FIELDS = {
 EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
-    "baas_version", "baas_test_inject_unsatisfiable_wait",
+    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc",
 ]
 
 
@@ -85,6 +85,8 @@ def lib():
     L.baas_sptrsv.restype = i
     L.baas_ic0.argtypes = [vp, C.POINTER(BaasCsr), vp, vp]
     L.baas_ic0.restype = i
+    L.baas_ic0_noalloc.argtypes = [vp, C.POINTER(BaasCsr), vp, vp]
+    L.baas_ic0_noalloc.restype = i
     L.baas_ilu0.argtypes = [vp, C.POINTER(BaasCsr), vp, vp]
     L.baas_ilu0.restype = i
     L.baas_iccg.argtypes = [vp, C.POINTER(BaasCsr), vp, vp, d, i, i, C.POINTER(C.c_int), C.POINTER(C.c_double), vp]

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -523,6 +524,34 @@ bool csr_ok(const baas_csr *m, int n, int nnz) {
 }
 
 
+// ---------------------------------------------------------------------------------------
+// Allocation-free IC0 (baas_ic0_noalloc). The factorisation's scratch -- one ready flag per
+// row plus the status word -- lives in this file-scope device array instead of memory the
+// schedule allocates. Every GPU that loads this library holds the array (8 MB) until the
+// process exits. Host code must not use the symbol as an address: the device address is looked
+// up once per device with cudaGetSymbolAddress while that device is current.
+// ---------------------------------------------------------------------------------------
+constexpr int kNoAllocMaxRows = 1 << 21;  // 2,097,152 rows
+constexpr int kNoAllocStatusInts = 4;     // a DevStatus at the front
+static __device__ __align__(256) int g_noalloc_scratch[kNoAllocStatusInts + kNoAllocMaxRows];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+int *g_noalloc_ptr[kMaxDevices] = {};
+
+baas_status noalloc_scratch(int dev, int **out) {
+    if (dev < 0 || dev >= kMaxDevices) return fail(BAAS_ERR_NO_DEVICE, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return fail(BAAS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<int *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return BAAS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -689,6 +718,46 @@ static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void 
 baas_status baas_ic0(baas_schedule *s, const baas_csr *A, double *lu, void *stream) { return factor(s, A, lu, stream, false); }
 
 baas_status baas_ilu0(baas_schedule *s, const baas_csr *A, double *lu, void *stream) { return factor(s, A, lu, stream, true); }
+
+// IC0 that allocates nothing: the same level-synchronous kernel as baas_ic0, given the static
+// scratch array above for its row flags and status word. The schedule's device plan must already
+// be resident (it is uploaded by the first ordinary GPU call on this schedule); this call does
+// not upload it, because uploading allocates. It clears the flags and the status it uses, then
+// launches on `stream` and reads the status back from device memory into a local variable.
+baas_status baas_ic0_noalloc(baas_schedule *s, const baas_csr *A, double *lu, void *stream_) {
+    if (!s || !lu) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    if (s->hs.kind == baas::SchedKind::SpTRSV) return fail(BAAS_ERR_STATE, "a SpTRSV schedule cannot drive a factorisation");
+    if (!A || A->n != s->hs.n || A->nnz != s->nnz_a || !A->rowptr || !A->colidx)
+        return fail(BAAS_ERR_BAD_ARG, "matrix does not match the analysed pattern");
+    if (s->hs.n > kNoAllocMaxRows)
+        return fail(BAAS_ERR_BAD_ARG, "baas_ic0_noalloc takes at most " + std::to_string(kNoAllocMaxRows) +
+                                          " rows (its static scratch size); use baas_ic0");
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(BAAS_ERR_NO_DEVICE, "no CUDA device");
+    if (!s->uploaded || dev != s->device)
+        return fail(BAAS_ERR_STATE, "the schedule's device plan is not resident on this device: run one ordinary GPU "
+                                    "call (e.g. baas_ic0) on it first");
+    int *scratch = nullptr;
+    BAAS_TRY(noalloc_scratch(dev, &scratch));
+    DevStatus *status = reinterpret_cast<DevStatus *>(scratch);
+    int *flags = scratch + kNoAllocStatusInts;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    // the array keeps the previous call's contents: flags and status must start at zero
+    BAAS_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int) * ((size_t)kNoAllocStatusInts + (size_t)s->hs.n), stream));
+    int epoch = 1;
+    baas::PartView pv = s->d_fwd.view(s->P);
+    unsigned int spin = s->spin();
+    void *args[] = {(void *)&pv, (void *)&A->rowptr, (void *)&A->colidx, (void *)&s->d_a_diag, (void *)&lu,
+                    (void *)&flags, (void *)&epoch, (void *)&status, (void *)&spin};
+    BAAS_CUDA(cudaLaunchCooperativeKernel((void *)baas::k_factor_part<false>, s->P, baas::kPartBlock, args, 0, stream));
+    DevStatus hs{};
+    BAAS_CUDA(cudaMemcpyAsync(&hs, status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+    BAAS_CUDA(cudaStreamSynchronize(stream));
+    if (hs.code == baas::kTimeout) return fail(BAAS_ERR_TIMEOUT, "a device wait ran out (at " + std::to_string(hs.where) + ")");
+    if (hs.code != 0) return fail(BAAS_ERR_CUDA, "device status " + std::to_string(hs.code));
+    if (hs.zero_pivots > 0) return fail(BAAS_ERR_ZERO_PIVOT, std::to_string(hs.zero_pivots) + " non-positive pivot(s)");
+    return BAAS_OK;
+}
 
 baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, double *x, double tol, int maxiter,
                       int precision, int *iters, double *relres, void *stream_) {

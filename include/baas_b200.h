@@ -158,6 +158,26 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
  * Synchronises `stream` to read the status. */
 baas_status baas_ic0(baas_schedule *s, const baas_csr *A, double *lu, void *stream);
 
+/* IC0 that allocates no memory, for callers that cannot call cudaMalloc at the moment they
+ * factor: a hot loop of a real-time or latency-bound application that reserved all of its
+ * memory up front, code that runs while a CUDA graph is being captured (where cudaMalloc is
+ * not allowed), or a host framework whose device memory belongs to its own allocator.
+ * No counterpart in the reference (its CPU routines malloc freely).
+ *
+ * Same arguments, arithmetic and result as baas_ic0 (bit-identical factor). Its scratch -- one
+ * ready flag per row and a status word -- is a static device array of fixed size inside this
+ * library, so it takes at most 2,097,152 rows (BAAS_ERR_BAD_ARG beyond), and every GPU that
+ * loads the library holds that 8 MB until the process exits.
+ *  - The schedule's device plan must already be resident: make one ordinary GPU call on the
+ *    schedule (e.g. baas_ic0) during set-up; otherwise this returns BAAS_ERR_STATE.
+ *  - Its first call on a device looks up that device's address of the static array (with the
+ *    device current); make that first call before any stream capture.
+ *  - All calls share the one array (it keeps the last call's contents; each call clears what
+ *    must start at zero): calls that overlap on the GPU -- on two streams, or on two schedules
+ *    at once -- race and must not be issued.
+ * Synchronises `stream` to read the status. */
+baas_status baas_ic0_noalloc(baas_schedule *s, const baas_csr *A, double *lu, void *stream);
+
 /* ILU0 in place on lu (device, pre-filled with A.values). Replaces
  * ilu0_p2p_csr_group_merge_no_perm_alloc (merge/ILU.cpp:638-720); bit-identical factor.
  * Synchronises `stream` to read the status. */

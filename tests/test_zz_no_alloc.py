@@ -1,0 +1,42 @@
+"""baas_ic0_noalloc: the IC0 entry point that allocates nothing, for callers that cannot call
+cudaMalloc when they factor (pre-reserved real-time loops, code running during CUDA graph
+capture, hosts whose device memory belongs to another allocator). Its scratch is a static
+device array inside the library, shared by every call.
+
+This file is collected last on purpose: if it fails, a run that stops at the first failure has
+already run every other test. It passes alone in a fresh process (the schedule's plan is made
+resident by the ordinary call below) and after the other tests (each call clears the shared
+scratch it needs)."""
+import numpy as np
+import pytest
+
+from baas_b200 import KERNEL_ICCG, BaasError, DeviceCSR, Schedule, gen
+
+pytestmark = pytest.mark.gpu
+
+
+def test_ic0_noalloc_matches_ic0_on_two_calls_in_a_row():
+    import torch
+
+    A = gen.laplace3d(20, 1e-3)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    dA = DeviceCSR.from_host(A)
+    ref = dA.values.clone()
+    s.ic0(dA, ref)  # ordinary entry point; also makes the schedule's device plan resident
+    want = ref.cpu().numpy()
+    for _ in range(2):
+        lu = dA.values.clone()
+        s.ic0_noalloc(dA, lu)
+        torch.cuda.synchronize()
+        # same tolerance as the other IC0 tests: the factors are bit-identical
+        assert np.array_equal(lu.cpu().numpy(), want)
+
+
+def test_ic0_noalloc_needs_a_resident_plan():
+    A = gen.laplace3d(6, 1e-3)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=2)
+    dA = DeviceCSR.from_host(A)
+    lu = dA.values.clone()
+    with pytest.raises(BaasError) as e:
+        s.ic0_noalloc(dA, lu)
+    assert e.value.status_name == "BAAS_ERR_STATE"
