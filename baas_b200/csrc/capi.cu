@@ -324,8 +324,9 @@ void build_dir(baas_schedule *s, bool upper, PartHost &out) {
 }
 
 // Staged plan from the two position plans: per CTA, each level segment becomes as many steps
-// as its largest group has rows; step j holds the j-th row of every group of the level.
-// Slots are the rows' local positions in the lower sweep's step order.
+// as its largest group has rows; step j holds the j-th row of every group of the level. Slots
+// are the rows' local positions in the lower sweep's step order. Entries are laid out with the
+// CTA's uniform stride E (its widest row), padding unused entries.
 void build_staged(baas_schedule *s) {
     const int n = s->hs.n, P = s->P;
     StagedHost &S = s->stg;
@@ -337,16 +338,13 @@ void build_staged(baas_schedule *s) {
         StagedHostDir &D = S.dir[d];
         D.ioff.assign(P + 1, 0);
         D.voff.assign(P + 1, 0);
-        std::vector<int> pos_of(n, 0);
-        for (int pos = 0; pos < n; pos++) pos_of[H.row[pos]] = pos;
         for (int c = 0; c < P; c++) {
-            // rows of the CTA in step order
-            std::vector<int> step_row(1, 0), step_E, order;
+            std::vector<int> step_row(1, 0), order;
+            int E = 0;
             for (int sg = H.cta_seg[c]; sg < H.cta_seg[c + 1]; sg++) {
                 int m = 0;
                 for (int it = H.seg_item[sg]; it < H.seg_item[sg + 1]; it++) m = std::max(m, H.item_pos[it + 1] - H.item_pos[it]);
                 for (int j = 0; j < m; j++) {
-                    int E = 0;
                     for (int it = H.seg_item[sg]; it < H.seg_item[sg + 1]; it++)
                         if (H.item_pos[it] + j < H.item_pos[it + 1]) {
                             const int pos = H.item_pos[it] + j;
@@ -354,48 +352,36 @@ void build_staged(baas_schedule *s) {
                             E = std::max(E, H.eptr[pos + 1] - H.eptr[pos]);
                         }
                     step_row.push_back((int)order.size());
-                    step_E.push_back(E);
                 }
             }
-            const int nl = (int)order.size(), S_ = (int)step_E.size();
+            const int nl = (int)order.size(), S_ = (int)step_row.size() - 1;
             if (d == 0)
                 for (int k = 0; k < nl; k++) slot_of[H.row[order[k]]] = k;
-            std::vector<int> step_ent(S_, 0), ne(nl), rowid(nl), slot(nl), dep;
-            std::vector<int> dT(nl), dA(nl), vT, vA;
-            int ent = 0;
-            for (int st = 0; st < S_; st++) {
-                step_ent[st] = ent;
-                for (int k = step_row[st]; k < step_row[st + 1]; k++) {
-                    const int pos = order[k];
-                    const int r = H.row[pos];
-                    ne[k] = H.eptr[pos + 1] - H.eptr[pos];
-                    rowid[k] = r;
-                    slot[k] = slot_of[r];
-                    dT[k] = H.dsrcT[pos];
-                    dA[k] = H.dsrcA[pos];
-                    for (int j = 0; j < step_E[st]; j++) {
-                        if (j < ne[k]) {
-                            const int e = H.eptr[pos] + j;
-                            int dd = H.dep[e];
-                            if (dd < 0) dd = -(slot_of[H.row[H.cta_pos[c] + (-dd - 1)]] + 1);
-                            dep.push_back(dd);
-                            vT.push_back(H.srcT[e]);
-                            vA.push_back(H.srcA[e]);
-                        } else {
-                            dep.push_back(0);
-                            vT.push_back(-1);
-                            vA.push_back(-1);
-                        }
-                    }
+            std::vector<int> ne(nl), rowid(nl), slot(nl), dep((size_t)nl * E, 0);
+            std::vector<int> dT(nl), dA(nl), vT((size_t)nl * E, -1), vA((size_t)nl * E, -1);
+            for (int k = 0; k < nl; k++) {
+                const int pos = order[k];
+                const int r = H.row[pos];
+                ne[k] = H.eptr[pos + 1] - H.eptr[pos];
+                rowid[k] = r;
+                slot[k] = slot_of[r];
+                dT[k] = H.dsrcT[pos];
+                dA[k] = H.dsrcA[pos];
+                for (int j = 0; j < ne[k]; j++) {
+                    const int e = H.eptr[pos] + j;
+                    const int dd = H.dep[e];
+                    // local: the dependency's slot; remote: -(row + 1)
+                    dep[(size_t)k * E + j] = dd < 0 ? slot_of[H.row[H.cta_pos[c] + (-dd - 1)]] : -(dd + 1);
+                    vT[(size_t)k * E + j] = H.srcT[e];
+                    vA[(size_t)k * E + j] = H.srcA[e];
                 }
-                ent += (step_row[st + 1] - step_row[st]) * step_E[st];
             }
+            const int ent = nl * E;
             D.ns.push_back(S_);
             D.nl.push_back(nl);
             D.ne.push_back(ent);
+            D.ints.push_back(E);
             D.ints.insert(D.ints.end(), step_row.begin(), step_row.end());
-            D.ints.insert(D.ints.end(), step_ent.begin(), step_ent.end());
-            D.ints.insert(D.ints.end(), step_E.begin(), step_E.end());
             D.ints.insert(D.ints.end(), ne.begin(), ne.end());
             D.ints.insert(D.ints.end(), rowid.begin(), rowid.end());
             D.ints.insert(D.ints.end(), slot.begin(), slot.end());

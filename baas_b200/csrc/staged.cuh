@@ -8,8 +8,8 @@
 //   up to m rows is split into m steps; step j holds the j-th row of every group of the level,
 //   so the rows of a group (a tree coarsened by the reference, merge/Coarsen.cpp:73-403) still
 //   run in their order, separated by a CTA barrier. Inside a step, row k belongs to thread
-//   k (k, k+blockDim, ... when a step is wider than the CTA). Its entries sit at
-//   step_ent[s] + k * step_E[s] + j, so a row is one table lookup away.
+//   k (k, k+blockDim, ... when a step is wider than the CTA), and its entries sit at a fixed
+//   stride, so a row is found by arithmetic.
 //
 // Measured on B200 (ncu, C1): with the plan read from global memory a level cost ~2500 cycles,
 // ~60 dependent instructions of ~40 cycles each.
@@ -18,9 +18,11 @@
 // upper sweep carries an explicit slot per position, so a row's upper-sweep right-hand side
 // (its lower-sweep result) is read from, and its result written to, the same slot.
 //
-// Per CTA and direction, int block: [step_row (S+1) | step_ent (S) | step_E (S) | ne (nl) |
-// rowid (nl) | slot (nl) | dep (ent)] and value block: [diag (nl) | val (ent)], both 16-byte
-// padded. dep >= 0: global row owned by another CTA (value-as-flag wait); dep < 0: -(slot+1).
+// Per CTA and direction, int block: [E | step_row (S+1) | ne (nl) | rowid (nl) | slot (nl) |
+// dep (nl*E)] and value block: [diag (nl) | val (nl*E)], both 16-byte padded. Every row of the
+// CTA has the same entry stride E (its widest row), so row `pos`'s entries sit at pos*E + j and
+// the hot path is fully unrolled. dep >= 0: local slot (final after the barrier); dep < 0:
+// -(row+1) of a row owned by another CTA (value-as-flag wait on its global slot).
 #pragma once
 
 #include "device_common.cuh"
@@ -55,7 +57,7 @@ struct StageLayout {
         S = S_;
         nl = nl_;
         ent = ent_;
-        nint = pad4((S + 1) + S + S + 3 * nl + ent);
+        nint = pad4(1 + (S + 1) + 3 * nl + ent);
         off_x = 0;
         off_ints = ((nl * (int)sizeof(T)) + 15) & ~15;
         off_vals = off_ints + nint * 4;
@@ -66,9 +68,9 @@ struct StageLayout {
 template <typename T>
 struct StageView {
     T *xs;
-    const int *step_row, *step_ent, *step_E, *ne, *rowid, *slot, *dep;
+    const int *step_row, *ne, *rowid, *slot, *dep;
     const T *diag, *val;
-    int S;
+    int S, E;
 };
 
 template <typename T>
@@ -76,10 +78,9 @@ __device__ __forceinline__ StageView<T> stage_view(unsigned char *smem, const St
     StageView<T> v;
     v.xs = reinterpret_cast<T *>(smem + L.off_x);
     const int *I = reinterpret_cast<const int *>(smem + L.off_ints);
-    v.step_row = I;
-    v.step_ent = v.step_row + (L.S + 1);
-    v.step_E = v.step_ent + L.S;
-    v.ne = v.step_E + L.S;
+    v.E = I[0];
+    v.step_row = I + 1;
+    v.ne = v.step_row + (L.S + 1);
     v.rowid = v.ne + L.nl;
     v.slot = v.rowid + L.nl;
     v.dep = v.slot + L.nl;
@@ -110,50 +111,110 @@ __device__ __forceinline__ void stage_ints(const StagedPlan &pl, int d, int c, c
     copy16(smem + L.off_ints, D.ints + __ldg(D.ioff + c), L.nint / 4);
 }
 
-// Generic row (any entry count): reads everything from shared memory.
-template <typename T, bool EXACT>
-__device__ __forceinline__ bool generic_row(const StageView<T> &v, int s, int pos, const T *xg, Waiter &w, int my_slot,
-                                            T &out) {
-    const int k = pos - v.step_row[s];
-    const int eb = v.step_ent[s] + k * v.step_E[s], ne = v.ne[pos];
+// Value of dependency d (see the block layout): local slot or a wait on another CTA's row.
+template <typename T>
+__device__ __forceinline__ bool dep_value(const StageView<T> &v, int d, const T *xg, Waiter &w, T &xv) {
+    if (d >= 0) {
+        xv = v.xs[d];
+        return true;
+    }
+    return wait_value<T>(xg + (-d - 1), xv, w, -d - 1);
+}
+
+// One row, entry stride E known at compile time (EK > 0) or read from the view (EK == 0).
+// pf holds values of remote dependencies loaded one step earlier (sentinel: wait for it now).
+template <typename T, bool EXACT, int EK>
+__device__ __forceinline__ bool stage_row(const StageView<T> &v, int pos, int slot, const T *xg, Waiter &w, const T *pf,
+                                          T &out) {
+    const int E = EK > 0 ? EK : v.E;
+    const int ne = v.ne[pos];
+    const int *dp = v.dep + pos * E;
+    const T *vp = v.val + pos * E;
     T sum = T(0);
-    for (int j = 0; j < ne; j++) {
-        const int d = v.dep[eb + j];
-        T xv;
-        if (d < 0)
-            xv = v.xs[-d - 1];
-        else if (!wait_value<T>(xg + d, xv, w, d))
-            return false;
-        if constexpr (EXACT)
-            sum = __dadd_rn(sum, __dmul_rn(xv, v.val[eb + j]));
-        else
-            sum = fmaf(xv, v.val[eb + j], sum);
+    if constexpr (EK > 0) {
+        int d[EK];
+        T a[EK], xv[EK];
+#pragma unroll
+        for (int j = 0; j < EK; j++) {
+            d[j] = dp[j];
+            a[j] = vp[j];
+        }
+        bool ok = true;
+#pragma unroll
+        for (int j = 0; j < EK; j++)
+            if (j < ne) {
+                if (d[j] >= 0) {
+                    xv[j] = v.xs[d[j]];
+                } else {
+                    xv[j] = pf ? pf[j] : Sent<T>::value();
+                    if (Sent<T>::is(xv[j]) && !wait_value<T>(xg + (-d[j] - 1), xv[j], w, -d[j] - 1)) ok = false;
+                }
+            }
+        if (!ok) return false;
+#pragma unroll
+        for (int j = 0; j < EK; j++)
+            if (j < ne) {
+                if constexpr (EXACT)
+                    sum = __dadd_rn(sum, __dmul_rn(xv[j], a[j]));
+                else
+                    sum = fmaf(xv[j], a[j], sum);
+            }
+    } else {
+        for (int j = 0; j < ne; j++) {
+            T xv;
+            const int d = dp[j];
+            if (d >= 0)
+                xv = v.xs[d];
+            else if (!wait_value<T>(xg + (-d - 1), xv, w, -d - 1))
+                return false;
+            if constexpr (EXACT)
+                sum = __dadd_rn(sum, __dmul_rn(xv, vp[j]));
+            else
+                sum = fmaf(xv, vp[j], sum);
+        }
     }
     if constexpr (EXACT)
-        out = __ddiv_rn(__dsub_rn(v.xs[my_slot], sum), v.diag[pos]);
+        out = __ddiv_rn(__dsub_rn(v.xs[slot], sum), v.diag[pos]);
     else
-        out = (v.xs[my_slot] - sum) * v.diag[pos];  // FP32 mode stores 1/diag
+        out = (v.xs[slot] - sum) * v.diag[pos];  // FP32 mode stores 1/diag
     return true;
+}
+
+// Issue the loads of row pos's remote dependencies (their values, or the sentinel if not yet
+// written); they complete while the CTA waits at the barrier.
+template <typename T, int EK>
+__device__ __forceinline__ void prefetch_remote(const StageView<T> &v, int pos, const T *xg, T *pf) {
+#pragma unroll
+    for (int j = 0; j < EK; j++) pf[j] = Sent<T>::value();
+    if (pos < 0) return;
+    const int ne = v.ne[pos];
+    const int *dp = v.dep + pos * EK;
+#pragma unroll
+    for (int j = 0; j < EK; j++) {
+        const int d = dp[j];
+        if (j < ne && d < 0) pf[j] = Sent<T>::load(xg + (-d - 1));
+    }
 }
 
 // Step-synchronous walk: at step s thread t runs rows step_row[s] + t, + blockDim, ... UPPER
 // selects the explicit slot map. Writes x to its slot and to the global slot of its row
-// (value-as-flag) and calls on_row(row, x). Every thread passes every barrier, also after a
-// failed wait, so the CTA never splits.
-//
-// Measured on B200 (phase trace, C1 CTA 0): this direct form ran a step in ~0.59 us against
-// ~0.84 us for a variant that prefetched the next step's row into registers; a bare step of
-// the same arithmetic with a 3-deep shared-memory index chain costs ~0.18 us, so what remains
-// is the dependent integer / shared-memory instruction chain per step.
-template <typename T, bool EXACT, bool UPPER, typename OnRow>
-__device__ __forceinline__ bool staged_walk(const StageView<T> &v, T *xg, Waiter &w, OnRow on_row) {
+// (value-as-flag) and calls on_row(row, x). Before each barrier a thread issues the loads of
+// its next row's remote dependencies, so their L2 latency overlaps the barrier. Every thread
+// passes every barrier, also after a failed wait, so the CTA never splits.
+template <typename T, bool EXACT, bool UPPER, int EK, typename OnRow>
+__device__ __forceinline__ bool staged_walk_e(const StageView<T> &v, T *xg, Waiter &w, OnRow on_row) {
+    constexpr int NP = EK > 0 ? EK : 1;
     bool alive = true;
+    T pf[NP];
+    int rb = v.step_row[0];
+    if constexpr (EK > 0) prefetch_remote<T, EK>(v, rb + (int)threadIdx.x < v.step_row[1] ? rb + (int)threadIdx.x : -1, xg, pf);
     for (int s = 0; s < v.S; s++) {
-        const int rb = v.step_row[s], re = v.step_row[s + 1];
+        const int re = v.step_row[s + 1];
         for (int pos = rb + (int)threadIdx.x; pos < re && alive; pos += blockDim.x) {
             const int slot = UPPER ? v.slot[pos] : pos;
             T out;
-            if (!generic_row<T, EXACT>(v, s, pos, xg, w, slot, out)) {
+            const T *use_pf = (EK > 0 && pos == rb + (int)threadIdx.x) ? pf : nullptr;
+            if (!stage_row<T, EXACT, EK>(v, pos, slot, xg, w, use_pf, out)) {
                 alive = false;
                 break;
             }
@@ -162,9 +223,29 @@ __device__ __forceinline__ bool staged_walk(const StageView<T> &v, T *xg, Waiter
             Sent<T>::store(xg + row, out);
             on_row(row, out);
         }
+        if constexpr (EK > 0) {
+            const int nb = re + (int)threadIdx.x;
+            const int ne_ = s + 1 < v.S ? v.step_row[s + 2] : re;
+            prefetch_remote<T, EK>(v, nb < ne_ ? nb : -1, xg, pf);
+        }
+        rb = re;
         __syncthreads();
     }
     return alive;
+}
+
+// Dispatch on the CTA's entry stride (the 5- and 7-point stencils' lower triangles have 2 and
+// 3 off-diagonal entries per row).
+template <typename T, bool EXACT, bool UPPER, typename OnRow>
+__device__ __forceinline__ bool staged_walk(const StageView<T> &v, T *xg, Waiter &w, OnRow on_row) {
+    switch (v.E) {
+        case 0:
+        case 1: return staged_walk_e<T, EXACT, UPPER, 1>(v, xg, w, on_row);
+        case 2: return staged_walk_e<T, EXACT, UPPER, 2>(v, xg, w, on_row);
+        case 3: return staged_walk_e<T, EXACT, UPPER, 3>(v, xg, w, on_row);
+        case 4: return staged_walk_e<T, EXACT, UPPER, 4>(v, xg, w, on_row);
+        default: return staged_walk_e<T, EXACT, UPPER, 0>(v, xg, w, on_row);
+    }
 }
 
 // Standalone FP64 sweep of the caller's CSR T (values gathered through vsrcT), nrhs right-hand

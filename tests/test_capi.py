@@ -1,0 +1,78 @@
+"""The C-ABI library: it loads without a GPU, exports every symbol include/baas_b200.h
+declares, and rejects bad input on the host with BAAS_ERR_BAD_ARG (no compute without a GPU)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from baas_b200 import KERNEL_ICCG, KERNEL_SPTRSV, BaasError, Schedule, _native, gen
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "baas_b200.h"
+
+
+def _declared():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:baas_status|void|int|double|const char \*)\s*\*?\s*(baas_\w+)\s*\(", text, re.M)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    L = _native.lib()
+    names = _declared()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(_native.EXPORTS)
+    assert _native.lib().baas_version().decode().startswith("baas_b200")
+
+
+def _bad(A, kind=KERNEL_ICCG, **kw):
+    with pytest.raises(BaasError) as e:
+        Schedule(A, kind=kind, **kw)
+    assert e.value.status_name == "BAAS_ERR_BAD_ARG"
+    return str(e.value)
+
+
+def test_rejects_missing_diagonal():
+    import scipy.sparse as sp
+
+    m = sp.csr_matrix(np.array([[1.0, 0, 0], [1.0, 0, 0], [0, 1.0, 1.0]]))
+    assert "diagonal" in _bad(gen.from_scipy(m), kind=KERNEL_SPTRSV)
+
+
+def test_rejects_upper_entries_for_sptrsv():
+    assert "lower" in _bad(gen.laplace2d(4), kind=KERNEL_SPTRSV)
+
+
+def test_rejects_unsorted_rows():
+    A = gen.laplace2d(4)
+    col = A.colidx.copy()
+    col[0], col[1] = col[1], col[0]
+    assert "ascending" in _bad(gen.CSR(A.n, A.rowptr, col, A.values))
+
+
+def test_rejects_nonsymmetric_pattern():
+    import scipy.sparse as sp
+
+    m = sp.csr_matrix(np.array([[2.0, 0, 0], [1.0, 2.0, 0], [0, 0, 2.0]]))
+    assert "symmetric" in _bad(gen.from_scipy(m))
+
+
+def test_rejects_bad_options():
+    _bad(gen.laplace2d(4), nthread=0)
+
+
+def test_bad_arg_on_null_and_size_mismatch():
+    L = _native.lib()
+    s = Schedule(gen.laplace2d(5).lower(), kind=KERNEL_SPTRSV, nthread=2)
+    # a factor with the wrong nnz is rejected before any GPU work
+    bad = _native.BaasCsr(s.n, 3, None, None, None)
+    st = L.baas_sptrsv(s._h, C.byref(bad), 0, C.c_void_p(8), C.c_void_p(16), 1, s.n, None)
+    assert st == 1
+    assert L.baas_schedule_export(s._h, 99, None) == -1
+
+
+def test_analysis_time_reported():
+    s = Schedule(gen.laplace3d(8, 1e-3), kind=KERNEL_ICCG, nthread=4)
+    assert s.analysis_ms > 0.0
