@@ -18,8 +18,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native
-from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, PREC_FP32_FACTORS, PREC_FP64,
-                      BaasError)
+from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, PARTITION_BAAS_THREADS, PARTITION_RANGES,
+                      PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
 
 __all__ = ["Schedule", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV", "KERNEL_ICCG", "KERNEL_IC0",
@@ -76,7 +76,7 @@ class Schedule:
     """
 
     def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
-                 parts: int = 0, partition: int = 0):
+                 parts: int = 0, partition: int = 0, smem_budget: int = 0):
         L = _native.lib()
         self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
         self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
@@ -87,6 +87,7 @@ class Schedule:
         opt.spin_limit = spin_limit
         opt.parts = parts
         opt.partition = partition
+        opt.smem_budget = smem_budget
         h = C.c_void_p()
         _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
         self._h = h
@@ -121,6 +122,16 @@ class Schedule:
     def inject_unsatisfiable_wait(self, row: int) -> None:
         """Test hook: the next forward sweep waits on a value nothing writes (BAAS_ERR_TIMEOUT)."""
         _native.check(_native.lib().baas_test_inject_unsatisfiable_wait(self._h, row), "inject")
+
+    def emulate_sweep(self, T: CSR, b: np.ndarray, upper: bool = False, parts: int = 0,
+                      smem_budget: int = 0) -> np.ndarray:
+        """Test hook: run the chunked sweep plan on the host (no GPU) and return x."""
+        tv = np.ascontiguousarray(T.values, dtype=np.float64)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        _native.check(_native.lib().baas_test_emulate_sweep(self._h, parts, smem_budget, int(upper), _ptr(tv),
+                                                             _ptr(bb), _ptr(x)), "emulate_sweep")
+        return x
 
     @property
     def analysis_ms(self) -> float:
@@ -170,4 +181,20 @@ class Schedule:
         if st == 5 and not raise_on_nonconvergence:
             return it.value, rr.value
         _native.check(st, "baas_iccg")
+        return it.value, rr.value
+
+    def iccg_adjoint(self, A: DeviceCSR, g, lam, x=None, grad_a=None, tol: float = 1e-10, maxiter: int = 2000,
+                     precision: int = PREC_FP64, stream=None, raise_on_nonconvergence: bool = True):
+        """Adjoint solve A^T lam = g with the factors of the previous `iccg` call; if x and grad_a
+        are given, grad_a[e] = -lam_i x_j on A's pattern. Returns (iterations, relative residual)."""
+        c = A.c()
+        it = C.c_int(0)
+        rr = C.c_double(0.0)
+        st = _native.lib().baas_iccg_adjoint(self._h, C.byref(c), _ptr(g), _ptr(lam),
+                                             _ptr(x) if x is not None else None,
+                                             _ptr(grad_a) if grad_a is not None else None, tol, maxiter, precision,
+                                             C.byref(it), C.byref(rr), _stream_ptr(stream))
+        if st == 5 and not raise_on_nonconvergence:
+            return it.value, rr.value
+        _native.check(st, "baas_iccg_adjoint")
         return it.value, rr.value

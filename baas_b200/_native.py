@@ -25,6 +25,7 @@ STATUS_NAMES = {
 
 KERNEL_SPTRSV, KERNEL_ICCG, KERNEL_IC0, KERNEL_ILU0 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32_FACTORS = 0, 1
+PARTITION_RANGES, PARTITION_BAAS_THREADS = 0, 1
 
 FIELDS = {
     "ngroups": 0, "nlevels": 1, "ntasks": 2, "group_ptr": 3, "group_set": 4, "level_ptr": 5,
@@ -37,7 +38,7 @@ FIELDS = {
 EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
-    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc",
+    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint",
 ]
 
 
@@ -48,7 +49,7 @@ class BaasCsr(C.Structure):
 
 class BaasOptions(C.Structure):
     _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("parts", C.c_int),
-                ("partition", C.c_int)]
+                ("partition", C.c_int), ("smem_budget", C.c_int)]
 
 
 class BaasError(RuntimeError):
@@ -97,6 +98,11 @@ def lib():
     L.baas_version.restype = C.c_char_p
     L.baas_test_inject_unsatisfiable_wait.argtypes = [vp, i]
     L.baas_test_inject_unsatisfiable_wait.restype = i
+    L.baas_iccg_adjoint.argtypes = [vp, C.POINTER(BaasCsr), vp, vp, vp, vp, d, i, i, C.POINTER(C.c_int),
+                                    C.POINTER(C.c_double), vp]
+    L.baas_iccg_adjoint.restype = i
+    L.baas_test_emulate_sweep.argtypes = [vp, i, i, i, vp, vp, vp]
+    L.baas_test_emulate_sweep.restype = i
     _lib = L
     return L
 

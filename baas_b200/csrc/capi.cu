@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <map>
 #include <mutex>
 #include <cstdio>
 #include <cstdlib>
@@ -106,52 +107,62 @@ baas_status upload_part(PartDev &d, const PartHost &h) {
     return BAAS_OK;
 }
 
-// Staged plan (staged.cuh), host side: per direction the packed per-CTA int and value-source
-// blocks.
-struct StagedHostDir {
-    std::vector<int> ioff, voff, ns, nl, ne, ints, vsrcT, vsrcA;
+// Chunk plan (staged.cuh), host side: per direction the chunk int blocks and value-slot
+// sources, CTA by CTA; the slot order rows of every CTA.
+struct ChunkHostDir {
+    std::vector<int> ints, vsrcT, vsrcA;
+    std::vector<int> cval;                    // P + 1: value slots of each CTA
+    std::vector<int> cchunk;                  // P + 1: chunks of each CTA
+    std::vector<int> chunk_ioff, chunk_voff;  // nchunk + 1
 };
-struct StagedHost {
-    StagedHostDir dir[2];
-    size_t smem64 = 0, smem32 = 0;  // dynamic shared memory per CTA (FP64 / FP32 values)
+struct ChunkHost {
+    ChunkHostDir dir[2];
+    std::vector<int> soff, srow;
+    int nl_max = 0;
 };
-struct StagedDevDir {
-    int *ioff = nullptr, *voff = nullptr, *ns = nullptr, *nl = nullptr, *ne = nullptr, *ints = nullptr,
-        *vsrcT = nullptr, *vsrcA = nullptr;
+struct ChunkDevDir {
+    int *ints = nullptr, *vsrcT = nullptr, *vsrcA = nullptr, *cval = nullptr;
 };
-struct StagedDev {
-    StagedDevDir dir[2];
-    baas::StagedPlan plan(int P) const {
-        baas::StagedPlan p;
-        p.P = P;
-        for (int d = 0; d < 2; d++)
-            p.dir[d] = baas::StagedDir{dir[d].ioff, dir[d].voff, dir[d].ns, dir[d].nl, dir[d].ne,
-                                      dir[d].ints, dir[d].vsrcT, dir[d].vsrcA};
-        return p;
-    }
+struct ChunkDev {
+    ChunkDevDir dir[2];
+    int *soff = nullptr, *srow = nullptr;
     void release() {
         for (auto &D : dir) {
-            int *ptrs[] = {D.ioff, D.voff, D.ns, D.nl, D.ne, D.ints, D.vsrcT, D.vsrcA};
+            int *ptrs[] = {D.ints, D.vsrcT, D.vsrcA, D.cval};
             for (int *p : ptrs)
                 if (p) cudaFree(p);
         }
-        *this = StagedDev();
+        if (soff) cudaFree(soff);
+        if (srow) cudaFree(srow);
+        *this = ChunkDev();
+    }
+};
+// Windows of one launch configuration (value width, right-hand sides walked together).
+struct WinCfg {
+    int4 *rec[2] = {nullptr, nullptr};
+    int *swptr[2] = {nullptr, nullptr};
+    int xs_bytes = 0, cap = 0;
+    size_t smem = 0;
+    int nrec = 0;  // most windows of one CTA, both directions
+    void release() {
+        for (int d = 0; d < 2; d++) {
+            if (rec[d]) cudaFree(rec[d]);
+            if (swptr[d]) cudaFree(swptr[d]);
+        }
     }
 };
 
-baas_status upload_staged(StagedDev &d, const StagedHost &h) {
+baas_status upload_chunks(ChunkDev &d, const ChunkHost &h) {
     for (int k = 0; k < 2; k++) {
-        const StagedHostDir &H = h.dir[k];
-        StagedDevDir &D = d.dir[k];
-        BAAS_TRY(upload(D.ioff, H.ioff));
-        BAAS_TRY(upload(D.voff, H.voff));
-        BAAS_TRY(upload(D.ns, H.ns));
-        BAAS_TRY(upload(D.nl, H.nl));
-        BAAS_TRY(upload(D.ne, H.ne));
+        const ChunkHostDir &H = h.dir[k];
+        ChunkDevDir &D = d.dir[k];
         BAAS_TRY(upload(D.ints, H.ints));
         BAAS_TRY(upload(D.vsrcT, H.vsrcT));
         BAAS_TRY(upload(D.vsrcA, H.vsrcA));
+        BAAS_TRY(upload(D.cval, H.cval));
     }
+    BAAS_TRY(upload(d.soff, h.soff));
+    BAAS_TRY(upload(d.srow, h.srow));
     return BAAS_OK;
 }
 
@@ -170,7 +181,7 @@ struct baas_schedule {
     int P = 0;
     std::vector<int> group_cta, row_cta;
     PartHost fwd, bwd;
-    StagedHost stg;
+    ChunkHost chk;
     int fault_row = -1;  // test hook: forward row made to wait on its own output
 
     // device
@@ -178,7 +189,12 @@ struct baas_schedule {
     bool uploaded = false;
     int num_sms = 0;
     PartDev d_fwd, d_bwd;
-    StagedDev d_stg;
+    ChunkDev d_chk;
+    std::map<int, WinCfg> wins;  // key: value bytes * 16 + right-hand sides
+    int smem_budget = 0;
+    int rmax64 = 1;  // most FP64 right-hand sides one sweep walks together
+    int factor_prec = -1;  // precision of the IC0 factors the last baas_iccg left in the value slots
+    double *d_gvT[2] = {nullptr, nullptr};  // packed values of the caller's factor (sweeps)
     int *d_a_diag = nullptr;
     DevStatus *d_status = nullptr;
     DevStatus *h_status = nullptr;  // pinned
@@ -323,93 +339,206 @@ void build_dir(baas_schedule *s, bool upper, PartHost &out) {
     }
 }
 
-// Staged plan from the two position plans: per CTA, each level segment becomes as many steps
-// as its largest group has rows; step j holds the j-th row of every group of the level. Slots
-// are the rows' local positions in the lower sweep's step order. Entries are laid out with the
-// CTA's uniform stride E (its widest row), padding unused entries.
-void build_staged(baas_schedule *s) {
+// Chunk plan from the two position plans: per CTA, each level segment becomes as many steps as
+// its largest group has rows; step j holds the j-th row of every group of the level. A step is
+// one chunk, cut into several when its block would exceed kChunkBytes (FP64 values). All chunks
+// of a CTA and direction share one entry stride, the CTA's widest row. Slots are the rows'
+// positions in the CTA's lower-sweep order.
+constexpr int kChunkBytes = 16 * 1024;
+
+int chunk_bytes64(int nl, int E) { return baas::chunk_nint(nl, E) * 4 + baas::chunk_nval(nl, E) * 8; }
+
+void build_chunks(baas_schedule *s) {
     const int n = s->hs.n, P = s->P;
-    StagedHost &S = s->stg;
-    S = StagedHost();
-    std::vector<int> slot_of(n, 0);  // lower-sweep local position of each row
-    size_t smem64 = 0, smem32 = 0;
+    ChunkHost &C = s->chk;
+    C = ChunkHost();
+    std::vector<int> slot_of(n, 0);
+    C.soff.assign(P + 1, 0);
+    C.srow.reserve(n);
     for (int d = 0; d < 2; d++) {
         const PartHost &H = d == 0 ? s->fwd : s->bwd;
-        StagedHostDir &D = S.dir[d];
-        D.ioff.assign(P + 1, 0);
-        D.voff.assign(P + 1, 0);
+        ChunkHostDir &D = C.dir[d];
+        D.cval.assign(P + 1, 0);
+        D.cchunk.assign(P + 1, 0);
+        D.chunk_ioff.assign(1, 0);
+        D.chunk_voff.assign(1, 0);
         for (int c = 0; c < P; c++) {
-            std::vector<int> step_row(1, 0), order;
-            int E = 0;
+            // steps of this CTA: positions in order
+            std::vector<int> order, step_end;
             for (int sg = H.cta_seg[c]; sg < H.cta_seg[c + 1]; sg++) {
                 int m = 0;
                 for (int it = H.seg_item[sg]; it < H.seg_item[sg + 1]; it++) m = std::max(m, H.item_pos[it + 1] - H.item_pos[it]);
                 for (int j = 0; j < m; j++) {
                     for (int it = H.seg_item[sg]; it < H.seg_item[sg + 1]; it++)
-                        if (H.item_pos[it] + j < H.item_pos[it + 1]) {
-                            const int pos = H.item_pos[it] + j;
-                            order.push_back(pos);
-                            E = std::max(E, H.eptr[pos + 1] - H.eptr[pos]);
-                        }
-                    step_row.push_back((int)order.size());
+                        if (H.item_pos[it] + j < H.item_pos[it + 1]) order.push_back(H.item_pos[it] + j);
+                    step_end.push_back((int)order.size());
                 }
             }
-            const int nl = (int)order.size(), S_ = (int)step_row.size() - 1;
-            if (d == 0)
-                for (int k = 0; k < nl; k++) slot_of[H.row[order[k]]] = k;
-            std::vector<int> ne(nl), rowid(nl), slot(nl), dep((size_t)nl * E, 0);
-            std::vector<int> dT(nl), dA(nl), vT((size_t)nl * E, -1), vA((size_t)nl * E, -1);
-            for (int k = 0; k < nl; k++) {
-                const int pos = order[k];
-                const int r = H.row[pos];
-                ne[k] = H.eptr[pos + 1] - H.eptr[pos];
-                rowid[k] = r;
-                slot[k] = slot_of[r];
-                dT[k] = H.dsrcT[pos];
-                dA[k] = H.dsrcA[pos];
-                for (int j = 0; j < ne[k]; j++) {
-                    const int e = H.eptr[pos] + j;
-                    const int dd = H.dep[e];
-                    // local: the dependency's slot; remote: -(row + 1)
-                    dep[(size_t)k * E + j] = dd < 0 ? slot_of[H.row[H.cta_pos[c] + (-dd - 1)]] : -(dd + 1);
-                    vT[(size_t)k * E + j] = H.srcT[e];
-                    vA[(size_t)k * E + j] = H.srcA[e];
+            if (d == 0) {
+                for (size_t k = 0; k < order.size(); k++) {
+                    slot_of[H.row[order[k]]] = (int)k;
+                    C.srow.push_back(H.row[order[k]]);
                 }
+                C.soff[c + 1] = (int)C.srow.size();
             }
-            const int ent = nl * E;
-            D.ns.push_back(S_);
-            D.nl.push_back(nl);
-            D.ne.push_back(ent);
-            D.ints.push_back(E);
-            D.ints.insert(D.ints.end(), step_row.begin(), step_row.end());
-            D.ints.insert(D.ints.end(), ne.begin(), ne.end());
-            D.ints.insert(D.ints.end(), rowid.begin(), rowid.end());
-            D.ints.insert(D.ints.end(), slot.begin(), slot.end());
-            D.ints.insert(D.ints.end(), dep.begin(), dep.end());
-            D.ints.resize(baas::pad4((int)D.ints.size()), 0);
-            D.ioff[c + 1] = (int)D.ints.size();
-            D.vsrcT.insert(D.vsrcT.end(), dT.begin(), dT.end());
-            D.vsrcT.insert(D.vsrcT.end(), vT.begin(), vT.end());
-            D.vsrcA.insert(D.vsrcA.end(), dA.begin(), dA.end());
-            D.vsrcA.insert(D.vsrcA.end(), vA.begin(), vA.end());
-            const int padded = baas::pad4((int)D.vsrcA.size());
-            D.vsrcT.resize(padded, -1);
-            D.vsrcA.resize(padded, -1);
-            D.voff[c + 1] = padded;
-            baas::StageLayout L64, L32;
-            L64.make<double>(S_, nl, ent);
-            L32.make<float>(S_, nl, ent);
-            smem64 = std::max(smem64, (size_t)L64.total);
-            smem32 = std::max(smem32, (size_t)L32.total);
+            // one entry stride for all of the CTA's chunks: its widest row
+            int E = 0;
+            for (int pos : order) E = std::max(E, H.eptr[pos + 1] - H.eptr[pos]);
+            auto emit = [&](int kb, int ke) {
+                const int nl = ke - kb;
+                const size_t i0 = D.ints.size();
+                D.ints.resize(i0 + baas::chunk_nint(nl, E), 0);
+                int *I = D.ints.data() + i0;
+                I[0] = nl;
+                I[1] = E;
+                int *rowid = I + baas::kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
+                const size_t v0 = D.vsrcT.size();
+                D.vsrcT.resize(v0 + baas::chunk_nval(nl, E), -1);
+                D.vsrcA.resize(v0 + baas::chunk_nval(nl, E), -1);
+                int *vT = D.vsrcT.data() + v0, *vA = D.vsrcA.data() + v0;
+                for (int k = kb; k < ke; k++) {
+                    const int q = k - kb, pos = order[k], r = H.row[pos];
+                    rowid[q] = r;
+                    slot[q] = slot_of[r];
+                    ne[q] = H.eptr[pos + 1] - H.eptr[pos];
+                    vT[q] = baas::diag_code(H.dsrcT[pos]);
+                    vA[q] = baas::diag_code(H.dsrcA[pos]);
+                    for (int j = 0; j < ne[q]; j++) {
+                        const int e = H.eptr[pos] + j;
+                        const int dd = H.dep[e];
+                        // local: the dependency's slot; remote: -(row + 1)
+                        dep[q * E + j] = dd < 0 ? slot_of[H.row[H.cta_pos[c] + (-dd - 1)]] : -(dd + 1);
+                        vT[nl + q * E + j] = H.srcT[e];
+                        vA[nl + q * E + j] = H.srcA[e];
+                    }
+                }
+                D.chunk_ioff.push_back((int)D.ints.size());
+                D.chunk_voff.push_back((int)D.vsrcT.size());
+            };
+            int kb = 0;
+            for (int se : step_end) {
+                // cut the step [kb, se) into chunks of at most kChunkBytes
+                int cb = kb;
+                for (int k = kb; k < se; k++)
+                    if (k > cb && chunk_bytes64(k + 1 - cb, E) > kChunkBytes) {
+                        emit(cb, k);
+                        cb = k;
+                    }
+                if (se > cb) emit(cb, se);
+                kb = se;
+            }
+            D.cchunk[c + 1] = (int)D.chunk_ioff.size() - 1;
+            D.cval[c + 1] = (int)D.vsrcT.size();
         }
-        // slack so the last block's 16-byte copies stay inside the arrays
-        D.ints.resize(D.ints.size() + 4, 0);
-        D.vsrcT.resize(D.vsrcT.size() + 4, -1);
-        D.vsrcA.resize(D.vsrcA.size() + 4, -1);
     }
-    S.smem64 = smem64;
-    S.smem32 = smem32;
+    C.nl_max = 0;
+    for (int c = 0; c < P; c++) C.nl_max = std::max(C.nl_max, C.soff[c + 1] - C.soff[c]);
 }
+
+// Windows for values of `vbytes` bytes and R right-hand sides: each CTA's chunks grouped
+// greedily into blocks that fit one of the two buffers. False if a chunk does not fit.
+// Window buffers: at most kWindowTarget bytes each unless the budget was set explicitly (then
+// as large as it allows), and never larger than the largest window formed, so that shared
+// memory the plan does not need stays L1 cache for the SpMV and vector phases.
+constexpr int kWindowTarget = 32 * 1024;
+
+bool plan_windows(const ChunkHost &C, int P, int budget, bool explicit_budget, int vbytes, int R,
+                  std::vector<int4> rec[2], std::vector<int> swptr[2], int &xs_bytes, int &cap, int &nrec) {
+    xs_bytes = (int)(((long long)C.nl_max * R * vbytes + 127) / 128 * 128);
+    long long big = 0;  // every chunk must fit a buffer
+    for (int d = 0; d < 2; d++) {
+        const ChunkHostDir &D = C.dir[d];
+        for (size_t k = 0; k + 1 < D.chunk_ioff.size(); k++)
+            big = std::max(big, (long long)(D.chunk_ioff[k + 1] - D.chunk_ioff[k]) * 4 +
+                                    (long long)(D.chunk_voff[k + 1] - D.chunk_voff[k]) * vbytes);
+    }
+    // the control block holds one record per window of a CTA: reserve room for it, and grow
+    // the reserve if the windows outnumber it
+    for (int reserve = 1024;;) {
+        const int cap_max = ((budget - xs_bytes - reserve) / 2) & ~127;
+        if (cap_max < 1024 || big > cap_max) return false;
+        cap = explicit_budget ? cap_max : std::min(cap_max, kWindowTarget);
+        cap = std::max(cap, (int)((big + 127) / 128 * 128));
+        std::vector<int> count(P, 0);
+        for (int d = 0; d < 2; d++) {
+            const ChunkHostDir &D = C.dir[d];
+            rec[d].clear();
+            swptr[d].assign(P + 1, 0);
+            for (int c = 0; c < P; c++) {
+                const int kb = D.cchunk[c], ke = D.cchunk[c + 1];
+                int a = kb;
+                auto bytes = [&](int x, int y) {
+                    return (long long)(D.chunk_ioff[y] - D.chunk_ioff[x]) * 4 +
+                           (long long)(D.chunk_voff[y] - D.chunk_voff[x]) * vbytes;
+                };
+                auto close = [&](int x, int y) {
+                    rec[d].push_back(make_int4(D.chunk_ioff[x], D.chunk_ioff[y] - D.chunk_ioff[x], D.chunk_voff[x],
+                                               D.chunk_voff[y] - D.chunk_voff[x]));
+                };
+                for (int k = kb; k < ke; k++)
+                    if (k > a && bytes(a, k + 1) > cap) {
+                        close(a, k);
+                        a = k;
+                    }
+                if (ke > a) close(a, ke);
+                swptr[d][c + 1] = (int)rec[d].size();
+                count[c] += swptr[d][c + 1] - swptr[d][c];
+            }
+        }
+        nrec = 1;
+        for (int c = 0; c < P; c++) nrec = std::max(nrec, count[c]);
+        if (baas::win_ctl_bytes(nrec) <= reserve) break;
+        reserve = baas::win_ctl_bytes(nrec) + 512;
+        if (reserve > budget / 4) return false;
+    }
+    long long widest = 0;
+    for (int d = 0; d < 2; d++)
+        for (const int4 &r : rec[d]) widest = std::max(widest, (long long)r.y * 4 + (long long)r.w * vbytes);
+    cap = std::min(cap, (int)((widest + 127) / 128 * 128));
+    return true;
+}
+
+baas_status get_windows(baas_schedule *s, int vbytes, int R, WinCfg **out) {
+    const int key = vbytes * 16 + R;
+    auto it = s->wins.find(key);
+    if (it != s->wins.end()) {
+        *out = &it->second;
+        return BAAS_OK;
+    }
+    std::vector<int4> rec[2];
+    std::vector<int> swptr[2];
+    int xs_bytes = 0, cap = 0, mw = 0;
+    if (!plan_windows(s->chk, s->P, s->smem_budget, s->opt.smem_budget > 0, vbytes, R, rec, swptr, xs_bytes, cap, mw))
+        return fail(BAAS_ERR_BAD_ARG, "a CTA's rows do not fit its shared memory: raise `parts` or smem_budget");
+    WinCfg w;
+    for (int d = 0; d < 2; d++) {
+        BAAS_TRY(upload(w.rec[d], rec[d]));
+        BAAS_TRY(upload(w.swptr[d], swptr[d]));
+    }
+    w.xs_bytes = xs_bytes;
+    w.cap = cap;
+    w.smem = (size_t)baas::chunk_smem_bytes(xs_bytes, cap, mw);
+    w.nrec = mw;
+    *out = &(s->wins[key] = w);
+    return BAAS_OK;
+}
+
+baas::ChunkPlan chunk_plan(const baas_schedule *s, const WinCfg &w) {
+    baas::ChunkPlan p;
+    p.P = s->P;
+    for (int d = 0; d < 2; d++) {
+        const ChunkDevDir &D = s->d_chk.dir[d];
+        p.dir[d] = baas::ChunkDir{D.ints, D.vsrcT, D.vsrcA, D.cval, w.rec[d], w.swptr[d]};
+    }
+    p.soff = s->d_chk.soff;
+    p.srow = s->d_chk.srow;
+    p.xs_bytes = w.xs_bytes;
+    p.cap = w.cap;
+    p.nrec = w.nrec;
+    return p;
+}
+
+constexpr int kMaxSmemBudget = 224 * 1024;
 
 baas_status ensure_device(baas_schedule *s) {
     int dev = 0;
@@ -424,8 +553,10 @@ baas_status ensure_device(baas_schedule *s) {
     if (!prop.cooperativeLaunch) return fail(BAAS_ERR_NO_DEVICE, "device lacks cooperative launch");
     s->num_sms = prop.multiProcessorCount;
     s->device = dev;
+    s->smem_budget = s->opt.smem_budget > 0 ? std::min(s->opt.smem_budget, kMaxSmemBudget) : (int)kSmemBudget;
 
-    // partition size: the fewest CTAs whose staged plan slice fits in shared memory
+    // partition size: BAAS_THREADS: the schedule's threads; else `parts`, or about one CTA per
+    // 2,048 rows (at most 128, at most one per SM)
     const int n = s->hs.n;
     int P;
     if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) {
@@ -434,37 +565,44 @@ baas_status ensure_device(baas_schedule *s) {
     } else if (s->opt.parts > 0) {
         P = std::min(s->opt.parts, n);
     } else {
-        P = (int)std::max<long long>(1, ((long long)n * 48 + kSmemBudget - 1) / (long long)kSmemBudget);
+        P = std::max(1, std::min({(n + 2047) / 2048, 128, s->num_sms}));
     }
-    for (;;) {
-        if (P > s->num_sms) return fail(BAAS_ERR_BAD_ARG, "the partition needs more CTAs than the device has SMs");
-        build_partition(s, P);
-        build_dir(s, false, s->fwd);
-        build_dir(s, true, s->bwd);
-        build_staged(s);
-        if (s->stg.smem64 <= kSmemBudget) break;
-        if (s->opt.parts > 0 || s->opt.partition == BAAS_PARTITION_BAAS_THREADS)
-            return fail(BAAS_ERR_BAD_ARG, "a CTA's plan slice does not fit in shared memory: raise `parts`");
-        P = std::min(s->num_sms, std::max(P + 1, (int)(P * 1.25)));
-    }
+    if (P > s->num_sms) return fail(BAAS_ERR_BAD_ARG, "the partition needs more CTAs than the device has SMs");
+    build_partition(s, P);
+    build_dir(s, false, s->fwd);
+    build_dir(s, true, s->bwd);
+    build_chunks(s);
 
     BAAS_TRY(upload_part(s->d_fwd, s->fwd));
     BAAS_TRY(upload_part(s->d_bwd, s->bwd));
-    BAAS_TRY(upload_staged(s->d_stg, s->stg));
+    BAAS_TRY(upload_chunks(s->d_chk, s->chk));
     BAAS_TRY(upload(s->d_a_diag, s->hs.a_diagptr));
     BAAS_TRY(dalloc(s->d_status, 1));
     BAAS_TRY(dalloc(s->d_flags, (size_t)n));
     BAAS_TRY(dalloc(s->d_bar, 1));
     BAAS_CUDA(cudaMallocHost((void **)&s->h_status, sizeof(DevStatus)));
     if (getenv("BAAS_TRACE") && atoi(getenv("BAAS_TRACE")) > 0) BAAS_TRY(dalloc(s->d_trace, 2 * baas::kTraceSlots));
-    // the partitioned kernels take up to kSmemBudget bytes of dynamic shared memory
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_factor_part<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_factor_part<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_sweep_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_sweep_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_iccg_staged<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_iccg_staged<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_sweep_chunked<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_sweep_chunked<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_iccg_chunked<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
+    BAAS_CUDA(cudaFuncSetAttribute(baas::k_iccg_chunked<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
     s->uploaded = true;
+    // the single-right-hand-side FP64 windows must exist for every kind of call
+    WinCfg *w = nullptr;
+    BAAS_TRY(get_windows(s, 8, 1, &w));
+    // multi-right-hand-side sweeps: the widest batch that leaves both window buffers >= 8 KiB
+    s->rmax64 = 1;
+    for (int R = baas::kMaxRhs; R > 1; R--) {
+        const long long xs = ((long long)s->chk.nl_max * R * 8 + 127) / 128 * 128;
+        if ((s->smem_budget - xs - 32) / 2 < 8 * 1024) continue;
+        std::vector<int4> rec[2];
+        std::vector<int> swptr[2];
+        int xb = 0, cap = 0, mw = 0;
+        if (plan_windows(s->chk, s->P, s->smem_budget, s->opt.smem_budget > 0, 8, R, rec, swptr, xb, cap, mw)) {
+            s->rmax64 = R;
+            break;
+        }
+    }
     return BAAS_OK;
 }
 
@@ -548,6 +686,7 @@ void baas_options_default(baas_options *opt) {
     opt->spin_limit = 0;
     opt->parts = 0;
     opt->partition = BAAS_PARTITION_RANGES;
+    opt->smem_budget = 0;
 }
 
 const char *baas_last_error_string(void) { return g_err.c_str(); }
@@ -565,6 +704,7 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     if (o.partition != BAAS_PARTITION_RANGES && o.partition != BAAS_PARTITION_BAAS_THREADS)
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     if (o.parts < 0) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 0");
+    if (o.smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
     if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
     if (A->rowptr[A->n] != A->nnz) return fail(BAAS_ERR_BAD_ARG, "nnz != rowptr[n]");
     const baas::SchedKind sk = (baas::SchedKind)kind;
@@ -633,6 +773,137 @@ baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row) {
     return BAAS_OK;
 }
 
+baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget, int upper, const double *tval,
+                                    const double *b, double *x) {
+    if (!s || !tval || !b || !x) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    if (s->uploaded) return fail(BAAS_ERR_STATE, "the schedule's plan is resident on a GPU");
+    const int n = s->hs.n;
+    int P = parts > 0 ? std::min(parts, n) : std::max(1, std::min({(n + 2047) / 2048, 128, 148}));
+    if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) P = s->hs.nthread;
+    build_partition(s, P);
+    build_dir(s, false, s->fwd);
+    build_dir(s, true, s->bwd);
+    build_chunks(s);
+    const int budget = smem_budget > 0 ? std::min(smem_budget, kMaxSmemBudget) : (int)kSmemBudget;
+    std::vector<int4> rec[2];
+    std::vector<int> swptr[2];
+    int xs_bytes = 0, cap = 0, mw = 0;
+    if (!plan_windows(s->chk, P, budget, smem_budget > 0, 8, 1, rec, swptr, xs_bytes, cap, mw))
+        return fail(BAAS_ERR_BAD_ARG, "emulate: a chunk does not fit the window buffer");
+    if (baas::chunk_smem_bytes(xs_bytes, cap, mw) > budget) return fail(BAAS_ERR_BAD_ARG, "emulate: shared memory over budget");
+    const int d = upper ? 1 : 0;
+    const ChunkHostDir &D = s->chk.dir[d];
+    const ChunkHost &C = s->chk;
+    auto bad = [](const std::string &m) { return fail(BAAS_ERR_BAD_ARG, "emulate: " + m); };
+    // packing of the value slots, as the sweep kernel does
+    std::vector<double> gv(D.vsrcT.size());
+    for (size_t i = 0; i < gv.size(); i++) {
+        const int code = D.vsrcT[i];
+        const int src = code >= 0 ? code : (code <= -2 ? -2 - code : -1);
+        if (src >= s->nnz_l) return bad("value source out of range");
+        gv[i] = src >= 0 ? tval[src] : 0.0;
+    }
+    std::vector<char> ready(n, 0);
+    struct Cta {
+        int q = 0, qend = 0;
+        std::vector<int> ibuf;
+        std::vector<double> vbuf;
+        size_t ip = 0, vp = 0;
+        bool loaded = false, done = false;
+        std::vector<double> xs;
+        std::vector<char> xs_done;
+    };
+    std::vector<Cta> cta(P);
+    for (int c = 0; c < P; c++) {
+        Cta &K = cta[c];
+        const int s0 = C.soff[c], nl = C.soff[c + 1] - s0;
+        K.xs.resize(nl);
+        K.xs_done.assign(nl, 0);
+        for (int k = 0; k < nl; k++) K.xs[k] = b[C.srow[s0 + k]];
+        K.q = swptr[d][c];
+        K.qend = swptr[d][c + 1];
+        K.done = K.q == K.qend;
+    }
+    int remaining = P;
+    for (int c = 0; c < P; c++) remaining -= cta[c].done ? 1 : 0;
+    while (remaining > 0) {
+        bool progress = false;
+        for (int c = 0; c < P; c++) {
+            Cta &K = cta[c];
+            if (K.done) continue;
+            if (!K.loaded) {
+                const int4 r = rec[d][K.q];
+                if (r.x % 8 || r.y % 8 || r.z % 4 || r.w % 4) return bad("window block misaligned");
+                if ((long long)r.y * 4 + (long long)r.w * 8 > cap) return bad("window larger than its buffer");
+                if (r.x < 0 || r.x + r.y > (int)D.ints.size() || r.z < 0 || r.z + r.w > (int)gv.size())
+                    return bad("window outside the plan arrays");
+                K.ibuf.assign(D.ints.begin() + r.x, D.ints.begin() + r.x + r.y);
+                K.vbuf.assign(gv.begin() + r.z, gv.begin() + r.z + r.w);
+                K.ip = K.vp = 0;
+                K.loaded = true;
+            }
+            const int *I = K.ibuf.data() + K.ip;
+            const int nl = I[0], E = I[1];
+            if (nl < 1 || E < 0) return bad("bad chunk header");
+            if (K.ip + baas::chunk_nint(nl, E) > K.ibuf.size() || K.vp + baas::chunk_nval(nl, E) > K.vbuf.size())
+                return bad("chunk runs past its window");
+            const int *rowid = I + baas::kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
+            const double *V = K.vbuf.data() + K.vp;
+            const double *diag = V, *val = V + nl;
+            const int nlc = (int)K.xs.size();
+            bool wait = false;
+            for (int pos = 0; pos < nl && !wait; pos++) {
+                if (ne[pos] < 0 || ne[pos] > E) return bad("row entry count exceeds the chunk stride");
+                for (int j = 0; j < ne[pos]; j++) {
+                    const int dd = dep[pos * E + j];
+                    if (dd < 0) {
+                        const int r = -dd - 1;
+                        if (r >= n) return bad("remote dependency out of range");
+                        if (!ready[r]) wait = true;
+                    }
+                }
+            }
+            if (wait) continue;
+            for (int pos = 0; pos < nl; pos++) {
+                const int sl = slot[pos], row = rowid[pos];
+                if (sl < 0 || sl >= nlc) return bad("slot out of range");
+                if (row < 0 || row >= n || ready[row]) return bad("row out of range or computed twice");
+                double sum = 0.0;
+                for (int j = 0; j < ne[pos]; j++) {
+                    const int dd = dep[pos * E + j];
+                    double xv;
+                    if (dd >= 0) {
+                        if (dd >= nlc || !K.xs_done[dd]) return bad("local dependency not yet computed");
+                        xv = K.xs[dd];
+                    } else {
+                        xv = x[-dd - 1];
+                    }
+                    sum = sum + xv * val[pos * E + j];
+                }
+                const double out = (K.xs[sl] - sum) / diag[pos];
+                K.xs[sl] = out;
+                K.xs_done[sl] = 1;
+                x[row] = out;
+                ready[row] = 1;
+            }
+            K.ip += baas::chunk_nint(nl, E);
+            K.vp += baas::chunk_nval(nl, E);
+            if (K.ip == K.ibuf.size()) {
+                K.loaded = false;
+                if (++K.q == K.qend) {
+                    K.done = true;
+                    remaining--;
+                }
+            }
+            progress = true;
+        }
+        if (!progress) return bad("no CTA can make progress (the plan would deadlock)");
+    }
+    for (int i = 0; i < n; i++)
+        if (!ready[i]) return bad("a row was never computed");
+    return BAAS_OK;
+}
+
 void baas_destroy(baas_schedule *s) {
     if (!s) return;
     if (s->uploaded) {
@@ -641,10 +912,12 @@ void baas_destroy(baas_schedule *s) {
         if (cur != s->device) cudaSetDevice(s->device);
         s->d_fwd.release();
         s->d_bwd.release();
-        s->d_stg.release();
+        s->d_chk.release();
+        for (auto &kv : s->wins) kv.second.release();
         for (int d = 0; d < 2; d++) {
             if (s->d_gv64[d]) cudaFree(s->d_gv64[d]);
             if (s->d_gv32[d]) cudaFree(s->d_gv32[d]);
+            if (s->d_gvT[d]) cudaFree(s->d_gvT[d]);
         }
         void *ptrs[] = {s->d_a_diag, s->d_status, s->d_flags, s->d_bar, s->d_lu, s->d_r, s->d_y, s->d_z, s->d_p,
                         s->d_Ap, s->d_y32, s->d_z32, s->d_part, s->d_iters, s->d_relres};
@@ -666,19 +939,25 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
     if (x == b) return fail(BAAS_ERR_BAD_ARG, "x must not alias b");
     BAAS_TRY(ensure_device(s));
     cudaStream_t stream = (cudaStream_t)stream_;
+    const int d = upper ? 1 : 0;
+    // right-hand sides walked together: as many as the solution slots leave room for
+    const int R = std::min(nrhs, s->rmax64);
+    WinCfg *w = nullptr;
+    BAAS_TRY(get_windows(s, 8, R, &w));
+    if (!s->d_gvT[d]) BAAS_TRY(dalloc(s->d_gvT[d], s->chk.dir[d].vsrcT.size()));
     BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
     {
         const int fill_blocks = (int)std::min<long long>(4LL * s->num_sms, ((long long)n * nrhs + 255) / 256);
         baas::k_fill_sentinel<double><<<std::max(fill_blocks, 1), 256, 0, stream>>>(x, n, nrhs, ldb);
         BAAS_CUDA(cudaGetLastError());
     }
-    baas::StagedPlan pl = s->d_stg.plan(s->P);
+    baas::ChunkPlan pl = chunk_plan(s, *w);
     unsigned int spin = s->spin();
-    void *args[] = {(void *)&pl, (void *)&T->values, (void *)&b, (void *)&ldb, (void *)&x, (void *)&ldb,
-                    (void *)&nrhs, (void *)&s->d_status, (void *)&spin, (void *)&s->d_trace};
-    void *kern = upper ? (void *)baas::k_sweep_staged<true> : (void *)baas::k_sweep_staged<false>;
-
-    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, s->P, baas::kStageBlock, args, s->stg.smem64, stream));
+    double *gv = s->d_gvT[d];
+    void *args[] = {(void *)&pl, (void *)&d, (void *)&T->values, (void *)&gv, (void *)&b, (void *)&ldb, (void *)&x,
+                    (void *)&ldb, (void *)&nrhs, (void *)&R, (void *)&s->d_status, (void *)&spin, (void *)&s->d_trace};
+    void *kern = R > 1 ? (void *)baas::k_sweep_chunked<true> : (void *)baas::k_sweep_chunked<false>;
+    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, s->P, baas::kStageBlock, args, w->smem, stream));
     dump_trace(s, upper ? "sptrsv-upper" : "sptrsv-lower", stream);
     return read_status(s, stream);
 }
@@ -697,7 +976,7 @@ static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void 
     void *args[] = {(void *)&pv, (void *)&A->rowptr, (void *)&A->colidx, (void *)&s->d_a_diag, (void *)&lu,
                     (void *)&s->d_flags, (void *)&s->epoch, (void *)&s->d_status, (void *)&spin};
     void *kern = ilu ? (void *)baas::k_factor_part<true> : (void *)baas::k_factor_part<false>;
-    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, s->P, baas::kPartBlock, args, (size_t)s->fwd.max_local * 4, stream));
+    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, s->P, baas::kPartBlock, args, 0, stream));
     return read_status(s, stream);
 }
 
@@ -745,8 +1024,9 @@ baas_status baas_ic0_noalloc(baas_schedule *s, const baas_csr *A, double *lu, vo
     return BAAS_OK;
 }
 
-baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, double *x, double tol, int maxiter,
-                      int precision, int *iters, double *relres, void *stream_) {
+static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double *b, double *x, double tol, int maxiter,
+                               int precision, int *iters, double *relres, void *stream_, bool reuse, const double *xf,
+                               double *grad_a) {
     if (!s || !b || !x) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     if (s->hs.kind != baas::SchedKind::ICCG) return fail(BAAS_ERR_STATE, "ICCG needs a schedule of kind BAAS_KERNEL_ICCG");
     if (!csr_ok(A, s->hs.n, s->nnz_a)) return fail(BAAS_ERR_BAD_ARG, "matrix does not match the analysed pattern");
@@ -766,8 +1046,8 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
         BAAS_TRY(dalloc(s->d_y32, n));
         BAAS_TRY(dalloc(s->d_z32, n));
         for (int d = 0; d < 2; d++) {
-            BAAS_TRY(dalloc(s->d_gv64[d], s->stg.dir[d].vsrcA.size()));
-            BAAS_TRY(dalloc(s->d_gv32[d], s->stg.dir[d].vsrcA.size()));
+            BAAS_TRY(dalloc(s->d_gv64[d], s->chk.dir[d].vsrcA.size()));
+            BAAS_TRY(dalloc(s->d_gv32[d], s->chk.dir[d].vsrcA.size()));
         }
         BAAS_TRY(dalloc(s->d_part, (size_t)3 * P));
         BAAS_TRY(dalloc(s->d_iters, 1));
@@ -778,7 +1058,10 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
     BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
     BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
 
-    baas::StagedIccgArgs a{};
+    const bool mixed = precision == BAAS_PREC_FP32_FACTORS;
+    WinCfg *w = nullptr;
+    BAAS_TRY(get_windows(s, mixed ? 4 : 8, 1, &w));
+    baas::IccgArgs a{};
     a.n = n;
     a.a_rowptr = A->rowptr;
     a.a_colidx = A->colidx;
@@ -787,9 +1070,7 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
     a.b = b;
     a.x = x;
     a.fac = s->d_fwd.view(P);
-    a.pl = s->d_stg.plan(P);
-    a.nv[0] = (int)s->stg.dir[0].vsrcA.size();
-    a.nv[1] = (int)s->stg.dir[1].vsrcA.size();
+    a.pl = chunk_plan(s, *w);
     for (int d = 0; d < 2; d++) {
         a.gv64[d] = s->d_gv64[d];
         a.gv32[d] = s->d_gv32[d];
@@ -815,10 +1096,12 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
     a.out_relres = s->d_relres;
     a.spin_limit = s->spin();
     a.trace = s->d_trace;
+    a.reuse = reuse ? 1 : 0;
+    a.xf = xf;
+    a.grad_a = grad_a;
     void *args[] = {(void *)&a};
-    const bool mixed = precision == BAAS_PREC_FP32_FACTORS;
-    void *kern = mixed ? (void *)baas::k_iccg_staged<float> : (void *)baas::k_iccg_staged<double>;
-    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, P, baas::kStageBlock, args, mixed ? s->stg.smem32 : s->stg.smem64, stream));
+    void *kern = mixed ? (void *)baas::k_iccg_chunked<float> : (void *)baas::k_iccg_chunked<double>;
+    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, P, baas::kStageBlock, args, w->smem, stream));
     int it = 0;
     double rr = 0.0;
     BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -827,9 +1110,30 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
     baas_status st = read_status(s, stream);
     if (iters) *iters = it;
     if (relres) *relres = rr;
+    if (!reuse) s->factor_prec = st == BAAS_OK || st == BAAS_ERR_NOT_CONVERGED ? precision : -1;
     if (st != BAAS_OK) return st;
     if (!(rr < tol)) return fail(BAAS_ERR_NOT_CONVERGED, "maxiter reached before tol");
     return BAAS_OK;
+}
+
+baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, double *x, double tol, int maxiter,
+                      int precision, int *iters, double *relres, void *stream) {
+    return iccg_launch(s, A, b, x, tol, maxiter, precision, iters, relres, stream, false, nullptr, nullptr);
+}
+
+// Adjoint solve: A^T lambda = g with the IC0 factors of the previous baas_iccg (A is symmetric,
+// so the transposed sweeps L^-T, L^-1 of the preconditioner are the forward ones), from
+// lambda = 0; with x and grad_a, the pattern gradient grad_a[e] = -lambda_i x_j in the same launch.
+baas_status baas_iccg_adjoint(baas_schedule *s, const baas_csr *A, const double *g, double *lambda, const double *x,
+                              double *grad_a, double tol, int maxiter, int precision, int *iters, double *relres,
+                              void *stream_) {
+    if (!s || !g || !lambda) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    if ((x == nullptr) != (grad_a == nullptr)) return fail(BAAS_ERR_BAD_ARG, "x and grad_a go together");
+    if (s->factor_prec != precision)
+        return fail(BAAS_ERR_STATE, "no IC0 factors of this precision: run baas_iccg on this schedule first");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    BAAS_CUDA(cudaMemsetAsync(lambda, 0, sizeof(double) * (size_t)s->hs.n, stream));
+    return iccg_launch(s, A, g, lambda, tol, maxiter, precision, iters, relres, stream_, true, x, grad_a);
 }
 
 }  // extern "C"

@@ -170,6 +170,52 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int
     return s_ok != 0;
 }
 
+// --- shared-memory mbarriers and untiled bulk copies (the TMA engine's cp.async.bulk form):
+// global -> shared copies of contiguous, 16-byte aligned blocks whose size is a multiple of
+// 16 bytes, completion counted in bytes on an mbarrier. ---
+__device__ __forceinline__ unsigned int smem_u32(const void *p) { return (unsigned int)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// makes mbarrier initialisation visible to the async proxy (the bulk-copy engine)
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// orders this thread's earlier shared-memory accesses before its later async-proxy ones
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// orders this thread's generic-proxy global writes before later async-proxy reads of them
+__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned int bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned int bytes, unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned int parity) {
+    unsigned int ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+// Bounded wait for the completion of phase `parity` of `bar` (each try_wait may suspend the
+// thread for a while, so `limit` tries last far longer than `limit` polls).
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned int parity, unsigned int limit) {
+    for (unsigned int i = 0; i < limit; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 // Phase tracing (BAAS_TRACE=1): thread 0 of the first and last CTA record %globaltimer (ns)
 // at phase boundaries into trace[cta_sel * kTraceSlots + k]; a NULL trace disables it.
 constexpr int kTraceSlots = 64;

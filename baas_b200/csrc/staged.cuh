@@ -1,28 +1,28 @@
-// Shared-memory-staged, step-synchronous sweeps: the production triangular sweeps.
+// Chunked, shared-memory-staged, step-synchronous sweeps: the production triangular sweeps.
 //
 // Each CTA owns a set of rows (part_kernels.cuh explains the partition and why it is
-// deadlock-free). Its slice of the plan is copied into shared memory once per sweep, laid out
-// so that a thread finds its next row by arithmetic instead of a chain of dependent loads:
+// deadlock-free). The CTA walks the schedule's group levels in the global order. A level whose
+// groups hold up to m rows is split into m steps; step j holds the j-th row of every group of
+// the level, so the rows of a group (a tree coarsened by the reference, merge/Coarsen.cpp:
+// 73-403) still run in their order, separated by a CTA barrier. Inside a step, row k belongs to
+// thread k (k, k + blockDim, ... when a step is wider than the CTA).
 //
-//   The CTA walks the schedule's group levels in the global order. A level whose groups hold
-//   up to m rows is split into m steps; step j holds the j-th row of every group of the level,
-//   so the rows of a group (a tree coarsened by the reference, merge/Coarsen.cpp:73-403) still
-//   run in their order, separated by a CTA barrier. Inside a step, row k belongs to thread
-//   k (k, k+blockDim, ... when a step is wider than the CTA), and its entries sit at a fixed
-//   stride, so a row is found by arithmetic.
+// The plan of a step is a self-contained CHUNK (a wide step is cut into several):
+//   int block   [nl, E, 0, 0 | rowid (nl) | slot (nl) | ne (nl) | dep (nl*E)], padded to 8 ints
+//   value block [diag (nl) | val (nl*E)], padded to 4 values
+// with E the widest row of the CTA (one stride for all of a CTA's chunks, so the walk is
+// specialised on it once per window), and row `pos` finds its entries at pos*E + j.
+// dep >= 0 is a CTA-local slot (final after the barrier that ended the producing step); dep < 0
+// is -(row+1) of a row owned by another CTA (a value-as-flag wait on its global slot). The
+// slot of a row is its position in the CTA's lower-sweep order; the lower and the upper sweep
+// use the same slots, so the upper sweep finds its right-hand side (the lower result) in place.
 //
-// Measured on B200 (ncu, C1): with the plan read from global memory a level cost ~2500 cycles,
-// ~60 dependent instructions of ~40 cycles each.
-//
-// Slots (shared-memory solution cells) are the rows' positions in the lower sweep's order; the
-// upper sweep carries an explicit slot per position, so a row's upper-sweep right-hand side
-// (its lower-sweep result) is read from, and its result written to, the same slot.
-//
-// Per CTA and direction, int block: [E | step_row (S+1) | ne (nl) | rowid (nl) | slot (nl) |
-// dep (nl*E)] and value block: [diag (nl) | val (nl*E)], both 16-byte padded. Every row of the
-// CTA has the same entry stride E (its widest row), so row `pos`'s entries sit at pos*E + j and
-// the hot path is fully unrolled. dep >= 0: local slot (final after the barrier); dep < 0:
-// -(row+1) of a row owned by another CTA (value-as-flag wait on its global slot).
+// A CTA's chunks are contiguous in global memory. Consecutive chunks are grouped into WINDOWS
+// that fit one of two shared-memory buffers; a window arrives through two bulk copies (ints,
+// values) issued by one thread and completes on an mbarrier, so the copy of window k+1 (or of the
+// next sweep's first windows) overlaps the walk of window k. When all of a CTA's windows fit the
+// two buffers they are copied once and stay resident. Solution slots (one value per row and
+// right-hand side) sit in front of the buffers.
 #pragma once
 
 #include "device_common.cuh"
@@ -31,105 +31,162 @@
 namespace baas {
 
 constexpr int kStageBlock = 512;
-
-struct StagedDir {
-    const int *ioff, *voff;   // P + 1 element offsets of each CTA's int / value block
-    const int *ns, *nl, *ne;  // P: steps, rows, padded entries of each CTA
-    const int *ints;          // packed int blocks
-    const int *vsrcT;         // laid out like the value blocks: position in the caller's CSR
-    const int *vsrcA;         // same, position in A's value array (the IC0 factor)
-};
-
-struct StagedPlan {
-    int P;
-    StagedDir dir[2];
-};
+constexpr int kChunkHdr = 4;
+constexpr int kIssuer = kStageBlock - 32;  // lane 0 of the last warp issues the bulk copies
+constexpr int kMaxRhs = 8;                 // right-hand sides walked together
 
 __host__ __device__ constexpr int pad4(int x) { return (x + 3) & ~3; }
+__host__ __device__ constexpr int pad8(int x) { return (x + 7) & ~7; }
+__host__ __device__ constexpr int chunk_nint(int nl, int E) { return pad8(kChunkHdr + 3 * nl + nl * E); }
+__host__ __device__ constexpr int chunk_nval(int nl, int E) { return pad4(nl + nl * E); }
+// value-source code of a diagonal entry at position p (off-diagonals: p >= 0; padding: -1)
+__host__ __device__ constexpr int diag_code(int p) { return -2 - p; }
 
-// Shared-memory carve-up, identical on host and device.
-struct StageLayout {
-    int S, nl, ent;
-    int nint;                              // ints of the block (padded)
-    int off_x, off_ints, off_vals, total;  // byte offsets
-    template <typename T>
-    __host__ __device__ void make(int S_, int nl_, int ent_) {
-        S = S_;
-        nl = nl_;
-        ent = ent_;
-        nint = pad4(1 + (S + 1) + 3 * nl + ent);
-        off_x = 0;
-        off_ints = ((nl * (int)sizeof(T)) + 15) & ~15;
-        off_vals = off_ints + nint * 4;
-        total = off_vals + ((((nl + ent) * (int)sizeof(T)) + 15) & ~15);
+struct ChunkDir {
+    const int *ints;           // chunk int blocks, CTA by CTA
+    const int *vsrcT, *vsrcA;  // per value slot: source position in the caller's CSR / in A
+    const int *cval;           // P + 1: value slots of each CTA
+    const int4 *swrec;         // windows: {int offset, ints, value offset, values}
+    const int *swptr;          // P + 1: windows of each CTA
+};
+
+struct ChunkPlan {
+    int P;
+    ChunkDir dir[2];
+    const int *soff;  // P + 1: slots of each CTA
+    const int *srow;  // row of each slot, CTA by CTA
+    int xs_bytes;     // shared-memory bytes of the solution slots
+    int cap;          // bytes of each window buffer
+    int nrec;         // most windows of one CTA, both directions together
+};
+
+// shared memory: [slots | buffer 0 | buffer 1 | stream control block with the CTA's window
+// records]; nrec = the most windows one CTA has (both directions)
+struct WinCtl {
+    unsigned long long mbar[2];
+    int nint[2];              // int count of the window in each buffer
+    const int *ints0, *ints1; // chunk int blocks of the first / second direction
+    const void *vals0, *vals1;
+    int n0, n1;               // windows of this CTA in each direction
+    unsigned int limit;       // no copy is issued for sequence numbers >= limit
+    int resident;             // all windows fit the two buffers: copied once
+    int4 rec[1];              // n0 + n1 window records {int offset, ints, value offset, values}
+};
+__host__ __device__ constexpr int win_ctl_bytes(int nrec) { return 128 + 16 * nrec; }
+__host__ __device__ constexpr int chunk_smem_bytes(int xs_bytes, int cap, int nrec) {
+    return xs_bytes + 2 * cap + win_ctl_bytes(nrec);
+}
+
+// Value of source code s in array v (the packing of a window's value slots).
+template <typename V>
+__device__ __forceinline__ double src_value(const V *v, int s) {
+    return s >= 0 ? (double)v[s] : (s <= -2 ? (double)v[-2 - s] : 0.0);
+}
+
+// The stream of windows one CTA walks: the windows of direction `first`, then (two_dirs)
+// those of direction 1, pass after pass. Its configuration sits in shared memory; every thread
+// holds the same two counters; one thread issues the copies.
+template <typename T>
+struct WinStream {
+    WinCtl *ctl;
+    unsigned char *buf;
+    int cap;
+    unsigned int issued, consumed;  // sequence numbers
+    bool loaded;
+
+    __device__ void init(const ChunkPlan &pl, int first, bool two_dirs, const T *v0, const T *v1, unsigned char *smem,
+                         unsigned int lim) {
+        const int c = blockIdx.x;
+        cap = pl.cap;
+        buf = smem + pl.xs_bytes;
+        ctl = reinterpret_cast<WinCtl *>(smem + pl.xs_bytes + 2 * pl.cap);
+        issued = consumed = 0;
+        loaded = false;
+        const ChunkDir &A = first ? pl.dir[1] : pl.dir[0];
+        const int q0 = __ldg(A.swptr + c), n0 = __ldg(A.swptr + c + 1) - q0;
+        const int q1 = two_dirs ? __ldg(pl.dir[1].swptr + c) : 0;
+        const int n1 = two_dirs ? __ldg(pl.dir[1].swptr + c + 1) - q1 : 0;
+        if (threadIdx.x == 0) {
+            ctl->ints0 = A.ints;
+            ctl->ints1 = pl.dir[1].ints;
+            ctl->vals0 = v0;
+            ctl->vals1 = v1;
+            ctl->n0 = n0;
+            ctl->n1 = n1;
+            ctl->limit = lim;
+            ctl->resident = n0 + n1 <= 2;
+            mbar_init(&ctl->mbar[0], 1);
+            mbar_init(&ctl->mbar[1], 1);
+            fence_mbar_init();
+        }
+        for (int i = threadIdx.x; i < n0 + n1; i += blockDim.x)
+            ctl->rec[i] = i < n0 ? __ldg(A.swrec + q0 + i) : __ldg(pl.dir[1].swrec + q1 + (i - n0));
+        __syncthreads();
     }
-};
+    __device__ int total() const { return ctl->n0 + ctl->n1; }
 
-template <typename T>
-struct StageView {
-    T *xs;
-    const int *step_row, *ne, *rowid, *slot, *dep;
-    const T *diag, *val;
-    int S, E;
-};
-
-template <typename T>
-__device__ __forceinline__ StageView<T> stage_view(unsigned char *smem, const StageLayout &L) {
-    StageView<T> v;
-    v.xs = reinterpret_cast<T *>(smem + L.off_x);
-    const int *I = reinterpret_cast<const int *>(smem + L.off_ints);
-    v.E = I[0];
-    v.step_row = I + 1;
-    v.ne = v.step_row + (L.S + 1);
-    v.rowid = v.ne + L.nl;
-    v.slot = v.rowid + L.nl;
-    v.dep = v.slot + L.nl;
-    const T *V = reinterpret_cast<const T *>(smem + L.off_vals);
-    v.diag = V;
-    v.val = V + L.nl;
-    v.S = L.S;
-    return v;
-}
-
-template <typename T>
-__device__ __forceinline__ StageLayout stage_layout(const StagedPlan &pl, int d, int c) {
-    StageLayout L;
-    const StagedDir &D = pl.dir[d];
-    L.make<T>(__ldg(D.ns + c), __ldg(D.nl + c), __ldg(D.ne + c));
-    return L;
-}
-
-// 16-byte copy of n4 int4 words by all threads of the CTA.
-__device__ __forceinline__ void copy16(void *dst, const void *src, int n4) {
-    int4 *d = reinterpret_cast<int4 *>(dst);
-    const int4 *s = reinterpret_cast<const int4 *>(src);
-    for (int i = threadIdx.x; i < n4; i += blockDim.x) d[i] = s[i];
-}
-
-__device__ __forceinline__ void stage_ints(const StagedPlan &pl, int d, int c, const StageLayout &L, unsigned char *smem) {
-    const StagedDir &D = pl.dir[d];
-    copy16(smem + L.off_ints, D.ints + __ldg(D.ioff + c), L.nint / 4);
-}
-
-// Value of dependency d (see the block layout): local slot or a wait on another CTA's row.
-template <typename T>
-__device__ __forceinline__ bool dep_value(const StageView<T> &v, int d, const T *xg, Waiter &w, T &xv) {
-    if (d >= 0) {
-        xv = v.xs[d];
+    // Issues the copy of sequence number `issued` into buffer issued % 2. All threads call it.
+    __device__ void issue_next() {
+        if (threadIdx.x == kIssuer) {
+            const int i = (int)(issued % (unsigned int)total());
+            const int4 r = ctl->rec[i];
+            const bool second = i >= ctl->n0;
+            const unsigned int b = issued & 1u;
+            unsigned char *dst = buf + b * cap;
+            const unsigned int ib = (unsigned int)r.y * 4u, vb = (unsigned int)r.w * (unsigned int)sizeof(T);
+            ctl->nint[b] = r.y;
+            fence_async_shared();
+            mbar_expect_tx(&ctl->mbar[b], ib + vb);
+            bulk_g2s(dst, (second ? ctl->ints1 : ctl->ints0) + r.x, ib, &ctl->mbar[b]);
+            bulk_g2s(dst + ib, static_cast<const T *>(second ? ctl->vals1 : ctl->vals0) + r.z, vb, &ctl->mbar[b]);
+        }
+        issued++;
+    }
+    // Item i of the current pass: waits for its window and returns the buffer holding it.
+    // False (uniformly for the CTA) if the wait gave up.
+    __device__ bool acquire(int i, unsigned int spin, DevStatus *st, const unsigned char *&b, int &nint) {
+        unsigned int s;
+        bool ok = true;
+        if (ctl->resident) {
+            s = (unsigned int)i;
+            if (!loaded) {
+                if (i == 0)
+                    while (issued < (unsigned int)total() && issued < ctl->limit) issue_next();
+                ok = mbar_wait(&ctl->mbar[s & 1u], (s >> 1) & 1u, spin);
+            }
+        } else {
+            s = consumed;
+            while (issued < s + 2u && issued < ctl->limit) issue_next();
+            ok = mbar_wait(&ctl->mbar[s & 1u], (s >> 1) & 1u, spin);
+        }
+        if (!ok && atomicCAS(&st->code, kOk, kTimeout) == kOk) st->where = -1000000 - (int)s;
+        if (__syncthreads_or(!ok)) return false;
+        b = buf + (s & 1u) * cap;
+        nint = ctl->nint[s & 1u];
         return true;
     }
-    return wait_value<T>(xg + (-d - 1), xv, w, -d - 1);
-}
+    // After the walk of item i (which ended with a CTA barrier): refill its buffer.
+    __device__ void release(int i) {
+        if (ctl->resident) {
+            if (i == total() - 1) loaded = true;
+            return;
+        }
+        consumed++;
+        while (issued < consumed + 2u && issued < ctl->limit) issue_next();
+    }
+    // Wait (bounded) for copies still in flight, before the CTA exits.
+    __device__ void drain(unsigned int spin) {
+        const unsigned int from = ctl->resident ? (loaded ? issued : 0u) : consumed;
+        for (unsigned int s = from; s < issued; s++) mbar_wait(&ctl->mbar[s & 1u], (s >> 1) & 1u, spin);
+        __syncthreads();
+    }
+};
 
-// One row, entry stride E known at compile time (EK > 0) or read from the view (EK == 0).
-// pf holds values of remote dependencies loaded one step earlier (sentinel: wait for it now).
+// One row, entry stride known at compile time (EK > 0) or not (EK == 0). pf holds the values
+// of the row's remote dependencies loaded one step earlier (sentinel: wait for it now).
 template <typename T, bool EXACT, int EK>
-__device__ __forceinline__ bool stage_row(const StageView<T> &v, int pos, int slot, const T *xg, Waiter &w, const T *pf,
-                                          T &out) {
-    const int E = EK > 0 ? EK : v.E;
-    const int ne = v.ne[pos];
-    const int *dp = v.dep + pos * E;
-    const T *vp = v.val + pos * E;
+__device__ __forceinline__ bool chunk_row(int ne, const int *dp, const T *vp, T diag, T rhs, const T *xs, const T *xg,
+                                          Waiter &w, const T (&pf)[4], bool use_pf, T &out) {
     T sum = T(0);
     if constexpr (EK > 0) {
         int d[EK];
@@ -144,9 +201,9 @@ __device__ __forceinline__ bool stage_row(const StageView<T> &v, int pos, int sl
         for (int j = 0; j < EK; j++)
             if (j < ne) {
                 if (d[j] >= 0) {
-                    xv[j] = v.xs[d[j]];
+                    xv[j] = xs[d[j]];
                 } else {
-                    xv[j] = pf ? pf[j] : Sent<T>::value();
+                    xv[j] = use_pf ? pf[j] : Sent<T>::value();
                     if (Sent<T>::is(xv[j]) && !wait_value<T>(xg + (-d[j] - 1), xv[j], w, -d[j] - 1)) ok = false;
                 }
             }
@@ -164,7 +221,7 @@ __device__ __forceinline__ bool stage_row(const StageView<T> &v, int pos, int sl
             T xv;
             const int d = dp[j];
             if (d >= 0)
-                xv = v.xs[d];
+                xv = xs[d];
             else if (!wait_value<T>(xg + (-d - 1), xv, w, -d - 1))
                 return false;
             if constexpr (EXACT)
@@ -174,136 +231,214 @@ __device__ __forceinline__ bool stage_row(const StageView<T> &v, int pos, int sl
         }
     }
     if constexpr (EXACT)
-        out = __ddiv_rn(__dsub_rn(v.xs[slot], sum), v.diag[pos]);
+        out = __ddiv_rn(__dsub_rn(rhs, sum), diag);
     else
-        out = (v.xs[slot] - sum) * v.diag[pos];  // FP32 mode stores 1/diag
+        out = (rhs - sum) * diag;  // FP32 value blocks hold 1/diag
     return true;
 }
 
-// Issue the loads of row pos's remote dependencies (their values, or the sentinel if not yet
+// Loads of the remote dependencies of row `pos` of the chunk at I (sentinel where not yet
 // written); they complete while the CTA waits at the barrier.
-template <typename T, int EK>
-__device__ __forceinline__ void prefetch_remote(const StageView<T> &v, int pos, const T *xg, T *pf) {
+template <typename T>
+__device__ __forceinline__ void prefetch_remote(const int *I, int pos, const T *xg, T (&pf)[4]) {
 #pragma unroll
-    for (int j = 0; j < EK; j++) pf[j] = Sent<T>::value();
-    if (pos < 0) return;
-    const int ne = v.ne[pos];
-    const int *dp = v.dep + pos * EK;
+    for (int j = 0; j < 4; j++) pf[j] = Sent<T>::value();
+    const int nl = I[0], E = I[1];
+    const int ne = I[kChunkHdr + 2 * nl + pos];
+    const int *dp = I + kChunkHdr + 3 * nl + pos * E;
 #pragma unroll
-    for (int j = 0; j < EK; j++) {
-        const int d = dp[j];
-        if (j < ne && d < 0) pf[j] = Sent<T>::load(xg + (-d - 1));
+    for (int j = 0; j < 4; j++)
+        if (j < ne) {
+            const int d = dp[j];
+            if (d < 0) pf[j] = Sent<T>::load(xg + (-d - 1));
+        }
+}
+
+// The rows of one chunk (one step) of nl rows at entry stride E (EK > 0: compile-time); writes
+// each result to its slot and to its row's global slot (value-as-flag), then calls
+// on_row(row, x).
+template <typename T, bool EXACT, int EK, typename OnRow>
+__device__ __forceinline__ bool chunk_step(const int *I, const T *V, int nl, int E, T *xs, T *xg, Waiter &w,
+                                           const T (&pf)[4], bool has_pf, OnRow &on_row) {
+    const int *rowid = I + kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
+    const T *diag = V, *val = V + nl;
+    for (int pos = threadIdx.x; pos < nl; pos += blockDim.x) {
+        const int sl = slot[pos];
+        T out;
+        if (!chunk_row<T, EXACT, EK>(ne[pos], dep + pos * E, val + pos * E, diag[pos], xs[sl], xs, xg, w, pf,
+                                     has_pf && pos == (int)threadIdx.x, out))
+            return false;
+        xs[sl] = out;
+        const int row = rowid[pos];
+        Sent<T>::store(xg + row, out);
+        on_row(row, out);
+    }
+    return true;
+}
+
+// Walk one window whose chunks all have entry stride E (EK > 0: compile-time, E <= 4). The
+// next chunk's row count is carried in a register and its first rows' remote dependencies are
+// loaded before the barrier.
+template <typename T, bool EXACT, int EK, typename OnRow>
+__device__ __forceinline__ bool walk_window_e(const int *I, const int *Iend, const T *V, int E, T *xs, T *xg, Waiter &w,
+                                              bool alive, OnRow &on_row) {
+    T pf[4];
+    bool has_pf = false;
+    int nl = I[0];
+    for (;;) {
+        if (alive) alive = chunk_step<T, EXACT, EK>(I, V, nl, E, xs, xg, w, pf, has_pf, on_row);
+        const int *In = I + chunk_nint(nl, E);
+        V += chunk_nval(nl, E);
+        const int nln = In < Iend ? In[0] : 0;
+        has_pf = EK > 0 && alive && (int)threadIdx.x < nln;
+        if (has_pf) prefetch_remote<T>(In, threadIdx.x, xg, pf);
+        __syncthreads();
+        if (In >= Iend) break;
+        I = In;
+        nl = nln;
+    }
+    return alive;
+}
+
+// Walk one window (nint ints of chunk blocks, then their values) held in shared memory. All
+// chunks of a CTA share one entry stride. Every thread passes every barrier, also after a
+// failed wait, so the CTA never splits.
+template <typename T, bool EXACT, typename OnRow>
+__device__ __forceinline__ bool walk_window(const unsigned char *b, int nint, T *xs, T *xg, Waiter &w, bool alive,
+                                            OnRow on_row) {
+    const int *I = reinterpret_cast<const int *>(b);
+    const int *Iend = I + nint;
+    const T *V = reinterpret_cast<const T *>(b + (size_t)nint * 4);
+    const int E = I[1];
+    switch (E) {
+        case 1: return walk_window_e<T, EXACT, 1>(I, Iend, V, 1, xs, xg, w, alive, on_row);
+        case 2: return walk_window_e<T, EXACT, 2>(I, Iend, V, 2, xs, xg, w, alive, on_row);
+        case 3: return walk_window_e<T, EXACT, 3>(I, Iend, V, 3, xs, xg, w, alive, on_row);
+        case 4: return walk_window_e<T, EXACT, 4>(I, Iend, V, 4, xs, xg, w, alive, on_row);
+        default: return walk_window_e<T, EXACT, 0>(I, Iend, V, E, xs, xg, w, alive, on_row);
     }
 }
 
-// Step-synchronous walk: at step s thread t runs rows step_row[s] + t, + blockDim, ... UPPER
-// selects the explicit slot map. Writes x to its slot and to the global slot of its row
-// (value-as-flag) and calls on_row(row, x). Before each barrier a thread issues the loads of
-// its next row's remote dependencies, so their L2 latency overlaps the barrier. Every thread
-// passes every barrier, also after a failed wait, so the CTA never splits.
-template <typename T, bool EXACT, bool UPPER, int EK, typename OnRow>
-__device__ __forceinline__ bool staged_walk_e(const StageView<T> &v, T *xg, Waiter &w, OnRow on_row) {
-    constexpr int NP = EK > 0 ? EK : 1;
-    bool alive = true;
-    T pf[NP];
-    int rb = v.step_row[0];
-    if constexpr (EK > 0) prefetch_remote<T, EK>(v, rb + (int)threadIdx.x < v.step_row[1] ? rb + (int)threadIdx.x : -1, xg, pf);
-    for (int s = 0; s < v.S; s++) {
-        const int re = v.step_row[s + 1];
-        for (int pos = rb + (int)threadIdx.x; pos < re && alive; pos += blockDim.x) {
-            const int slot = UPPER ? v.slot[pos] : pos;
-            T out;
-            const T *use_pf = (EK > 0 && pos == rb + (int)threadIdx.x) ? pf : nullptr;
-            if (!stage_row<T, EXACT, EK>(v, pos, slot, xg, w, use_pf, out)) {
-                alive = false;
-                break;
+// Multi-right-hand-side walk (R <= kMaxRhs, runtime): slots hold R values per row
+// (xs[slot*R + r]); right-hand side r of row `row` lives at xg[r*ldx + row]. FP64, exact.
+__device__ __forceinline__ bool walk_window_multi(const unsigned char *b, int nint, double *xs, double *xg, int ldx, int R,
+                                                  Waiter &w, bool alive) {
+    const int *I = reinterpret_cast<const int *>(b);
+    const int *Iend = I + nint;
+    const double *V = reinterpret_cast<const double *>(b + (size_t)nint * 4);
+    while (I < Iend) {
+        const int nl = I[0], E = I[1];
+        const int *rowid = I + kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
+        const double *diag = V, *val = V + nl;
+        for (int pos = threadIdx.x; pos < nl && alive; pos += blockDim.x) {
+            double sum[kMaxRhs];
+#pragma unroll
+            for (int r = 0; r < kMaxRhs; r++) sum[r] = 0.0;
+            const int n_ = ne[pos];
+            for (int j = 0; j < n_ && alive; j++) {
+                const int d = dep[pos * E + j];
+                const double a = val[pos * E + j];
+#pragma unroll
+                for (int r = 0; r < kMaxRhs; r++)
+                    if (r < R) {
+                        double xv = 0.0;
+                        if (d >= 0)
+                            xv = xs[d * R + r];
+                        else if (alive && !wait_value<double>(xg + (size_t)r * ldx + (-d - 1), xv, w, -d - 1))
+                            alive = false;
+                        sum[r] = __dadd_rn(sum[r], __dmul_rn(xv, a));
+                    }
             }
-            v.xs[slot] = out;
-            const int row = v.rowid[pos];
-            Sent<T>::store(xg + row, out);
-            on_row(row, out);
+            if (!alive) break;
+            const int sl = slot[pos], row = rowid[pos];
+#pragma unroll
+            for (int r = 0; r < kMaxRhs; r++)
+                if (r < R) {
+                    const double out = __ddiv_rn(__dsub_rn(xs[sl * R + r], sum[r]), diag[pos]);
+                    xs[sl * R + r] = out;
+                    Sent<double>::store(xg + (size_t)r * ldx + row, out);
+                }
         }
-        if constexpr (EK > 0) {
-            const int nb = re + (int)threadIdx.x;
-            const int ne_ = s + 1 < v.S ? v.step_row[s + 2] : re;
-            prefetch_remote<T, EK>(v, nb < ne_ ? nb : -1, xg, pf);
-        }
-        rb = re;
+        I += chunk_nint(nl, E);
+        V += chunk_nval(nl, E);
         __syncthreads();
     }
     return alive;
 }
 
-// Dispatch on the CTA's entry stride (the 5- and 7-point stencils' lower triangles have 2 and
-// 3 off-diagonal entries per row).
-template <typename T, bool EXACT, bool UPPER, typename OnRow>
-__device__ __forceinline__ bool staged_walk(const StageView<T> &v, T *xg, Waiter &w, OnRow on_row) {
-    switch (v.E) {
-        case 0:
-        case 1: return staged_walk_e<T, EXACT, UPPER, 1>(v, xg, w, on_row);
-        case 2: return staged_walk_e<T, EXACT, UPPER, 2>(v, xg, w, on_row);
-        case 3: return staged_walk_e<T, EXACT, UPPER, 3>(v, xg, w, on_row);
-        case 4: return staged_walk_e<T, EXACT, UPPER, 4>(v, xg, w, on_row);
-        default: return staged_walk_e<T, EXACT, UPPER, 0>(v, xg, w, on_row);
-    }
-}
-
-// Standalone FP64 sweep of the caller's CSR T (values gathered through vsrcT), nrhs right-hand
-// sides one after another.
-template <bool UPPER>
-__global__ void __launch_bounds__(kStageBlock, 1) k_sweep_staged(StagedPlan pl, const double *__restrict__ tval,
-                                                                const double *__restrict__ b, int ldb, double *x, int ldx,
-                                                                int nrhs, DevStatus *st, unsigned int spin_limit,
-                                                                unsigned long long *trace) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    constexpr int d = UPPER ? 1 : 0;
+// Standalone FP64 sweep of the caller's triangular CSR (values gathered through vsrcT into the
+// packed scratch gv), right-hand sides R at a time. d = 0: lower (L), 1: upper (U = L^T).
+template <bool MULTI>
+__global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, int d, const double *__restrict__ tval,
+                                                                 double *gv, const double *__restrict__ b, int ldb,
+                                                                 double *x, int ldx, int nrhs, int R, DevStatus *st,
+                                                                 unsigned int spin, unsigned long long *trace) {
+    extern __shared__ __align__(128) unsigned char smem[];
     const int c = blockIdx.x;
-    Waiter w(spin_limit, st);
+    Waiter w(spin, st);
     trace_mark(trace, 0);
-    const StageLayout L = stage_layout<double>(pl, d, c);
-    stage_ints(pl, d, c, L, smem);
     {
-        double *V = reinterpret_cast<double *>(smem + L.off_vals);
-        const int *src = pl.dir[d].vsrcT + __ldg(pl.dir[d].voff + c);
-        for (int i = threadIdx.x; i < L.nl + L.ent; i += blockDim.x) {
-            const int si = __ldg(src + i);
-            V[i] = si >= 0 ? __ldg(tval + si) : 0.0;
-        }
+        const ChunkDir &D = d ? pl.dir[1] : pl.dir[0];
+        const int vb = __ldg(D.cval + c), ve = __ldg(D.cval + c + 1);
+        for (int i = vb + (int)threadIdx.x; i < ve; i += blockDim.x) gv[i] = src_value(tval, __ldg(D.vsrcT + i));
+        fence_async_global();
     }
-    __syncthreads();
+    const int npass = (nrhs + R - 1) / R;
+    WinStream<double> ws;
+    {
+        const ChunkDir &D = d ? pl.dir[1] : pl.dir[0];
+        ws.init(pl, d, false, gv, gv, smem, (unsigned int)(npass * (__ldg(D.swptr + c + 1) - __ldg(D.swptr + c))));
+    }
     trace_mark(trace, 1);
-    const StageView<double> v = stage_view<double>(smem, L);
-    for (int r = 0; r < nrhs; r++) {
-        const double *br = b + (size_t)r * ldb;
-        double *xr = x + (size_t)r * ldx;
-        for (int p = threadIdx.x; p < L.nl; p += blockDim.x) v.xs[UPPER ? v.slot[p] : p] = __ldg(br + v.rowid[p]);
+    double *xs = reinterpret_cast<double *>(smem);
+    const int s0 = __ldg(pl.soff + c), nl = __ldg(pl.soff + c + 1) - s0;
+    const int *srow = pl.srow + s0;
+    for (int r0 = 0; r0 < nrhs; r0 += R) {
+        const int Rb = min(R, nrhs - r0);
+        for (int k = threadIdx.x; k < nl * Rb; k += blockDim.x) {
+            const int sl = k / Rb, r = k - sl * Rb;
+            xs[k] = __ldg(b + (size_t)(r0 + r) * ldb + __ldg(srow + sl));
+        }
         __syncthreads();
-        trace_mark(trace, 2 + 2 * r);
-        staged_walk<double, true, UPPER>(v, xr, w, [](int, double) {});
-        trace_mark(trace, 3 + 2 * r);
-        __shared__ int s_bad;
-        if (threadIdx.x == 0) s_bad = ld_relaxed_u32(&st->code) != 0u;
-        __syncthreads();
-        if (s_bad) return;
+        trace_mark(trace, 2 + 2 * (r0 / R));
+        bool alive = true;
+        for (int i = 0; i < ws.total(); i++) {
+            const unsigned char *buf;
+            int nint;
+            if (!ws.acquire(i, spin, st, buf, nint)) {
+                ws.drain(spin);
+                return;
+            }
+            if (MULTI)
+                alive = walk_window_multi(buf, nint, xs, x + (size_t)r0 * ldx, ldx, Rb, w, alive);
+            else
+                alive = walk_window<double, true>(buf, nint, xs, x + (size_t)r0 * ldx, w, alive, [](int, double) {});
+            ws.release(i);
+            if (__syncthreads_or(!alive)) {
+                ws.drain(spin);
+                return;
+            }
+        }
+        trace_mark(trace, 3 + 2 * (r0 / R));
     }
+    ws.drain(spin);
 }
 
 // ---------------------------------------------------------------------------------------
-// Persistent ICCG with staged sweeps: IC0 (level-synchronous, part_kernels.cuh), packing of
-// L and U = L^T into the staged value blocks, and the pcg_opt loop
-// (test/iccg_level_merge.cpp:380-533, break at tol) in one cooperative launch of P CTAs.
+// Persistent ICCG: IC0 (level-synchronous, part_kernels.cuh), packing of L and U = L^T into
+// the chunk value slots, and the pcg_opt loop (test/iccg_level_merge.cpp:380-533, break at
+// tol) in one cooperative launch of P CTAs.
 // ---------------------------------------------------------------------------------------
-struct StagedIccgArgs {
+struct IccgArgs {
     int n;
     const int *a_rowptr, *a_colidx, *a_diag;
     const double *a_val;
     const double *b;
     double *x;
     PartView fac;     // level plan of the factorisation
-    StagedPlan pl;    // staged sweep plan (dir 0: L, dir 1: U = L^T)
-    int nv[2];        // lengths of the packed value arrays (per direction)
-    double *gv64[2];  // packed FP64 value blocks (diag | val), per direction
-    float *gv32[2];   // packed FP32 value blocks (1/diag | val), per direction
+    ChunkPlan pl;     // chunked sweep plan (dir 0: L, dir 1: U = L^T)
+    double *gv64[2];  // packed FP64 value slots, per direction
+    float *gv32[2];   // packed FP32 value slots (1/diag on the diagonal), per direction
     double *lu;
     int *gflag;
     int epoch;
@@ -318,84 +453,94 @@ struct StagedIccgArgs {
     double *out_relres;
     unsigned int spin_limit;
     unsigned long long *trace;
+    int reuse;         // 1: the value slots already hold the factors (adjoint solves)
+    const double *xf;  // with grad_a: the forward solution x
+    double *grad_a;    // if set: grad_a[e] = -x_i * xf_j for each entry e = (i, j) of A
 };
 
 // z = U^-1 L^-1 r on this CTA's rows; p = z if set_p; adds this thread's r.z to rz.
 template <typename T>
-__device__ void staged_precond(const StagedIccgArgs &A, unsigned char *smem, bool set_p, double &rz, Waiter &w) {
+__device__ bool chunk_precond(const IccgArgs &A, WinStream<T> &ws, T *xs, bool set_p, double &rz, Waiter &w) {
     const int c = blockIdx.x;
     T *yg = sizeof(T) == 8 ? (T *)A.y : (T *)A.y32;
     T *zg = sizeof(T) == 8 ? (T *)A.z : (T *)A.z32;
-    {
-        const StageLayout L = stage_layout<T>(A.pl, 0, c);
-        __syncthreads();
-        stage_ints(A.pl, 0, c, L, smem);
-        const T *gv = sizeof(T) == 8 ? (const T *)A.gv64[0] : (const T *)A.gv32[0];
-        copy16(smem + L.off_vals, gv + __ldg(A.pl.dir[0].voff + c), (((L.nl + L.ent) * (int)sizeof(T)) + 15) / 16);
-        __syncthreads();
-        const StageView<T> v = stage_view<T>(smem, L);
-        for (int p = threadIdx.x; p < L.nl; p += blockDim.x) v.xs[p] = (T)A.r[v.rowid[p]];
-        __syncthreads();
-        trace_mark(A.trace, 56);
-        staged_walk<T, sizeof(T) == 8, false>(v, yg, w, [](int, T) {});
-        trace_mark(A.trace, 57);
+    const int s0 = __ldg(A.pl.soff + c), nl = __ldg(A.pl.soff + c + 1) - s0;
+    for (int k = threadIdx.x; k < nl; k += blockDim.x) xs[k] = (T)A.r[__ldg(A.pl.srow + s0 + k)];
+    __syncthreads();
+    bool alive = true;
+    trace_mark(A.trace, 56);
+    for (int i = 0; i < ws.total(); i++) {
+        const unsigned char *buf;
+        int nint;
+        if (!ws.acquire(i, A.spin_limit, A.st, buf, nint)) return false;
+        if (i < ws.ctl->n0) {
+            alive = walk_window<T, sizeof(T) == 8>(buf, nint, xs, yg, w, alive, [](int, T) {});
+            if (i == ws.ctl->n0 - 1) trace_mark(A.trace, 57);
+        } else {
+            alive = walk_window<T, sizeof(T) == 8>(buf, nint, xs, zg, w, alive, [&](int row, T out) {
+                const double zd = (double)out;
+                rz = __dadd_rn(rz, __dmul_rn(A.r[row], zd));
+                if (set_p) A.p[row] = zd;
+            });
+        }
+        ws.release(i);
+        if (__syncthreads_or(!alive)) return false;
     }
-    {
-        const StageLayout L = stage_layout<T>(A.pl, 1, c);
-        __syncthreads();
-        stage_ints(A.pl, 1, c, L, smem);
-        const T *gv = sizeof(T) == 8 ? (const T *)A.gv64[1] : (const T *)A.gv32[1];
-        copy16(smem + L.off_vals, gv + __ldg(A.pl.dir[1].voff + c), (((L.nl + L.ent) * (int)sizeof(T)) + 15) / 16);
-        __syncthreads();
-        const StageView<T> v = stage_view<T>(smem, L);
-        // xs already holds y in every slot of this CTA
-        trace_mark(A.trace, 58);
-        staged_walk<T, sizeof(T) == 8, true>(v, zg, w, [&](int row, T out) {
-            const double zd = (double)out;
-            rz = __dadd_rn(rz, __dmul_rn(A.r[row], zd));
-            if (set_p) A.p[row] = zd;
-        });
-        trace_mark(A.trace, 59);
-    }
+    trace_mark(A.trace, 59);
+    return true;
 }
 
 // T = double: FP64 factors; T = float: FP32 factors (one instantiation each keeps the register
 // budget of each variant to one precision).
 template <typename T>
-__global__ void __launch_bounds__(kStageBlock, 1) k_iccg_staged(StagedIccgArgs A) {
+__global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     constexpr bool kMixed = sizeof(T) == 4;
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int n = A.n;
     const int W = gridDim.x * blockDim.x;
     const int gt = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned int nb = 0;
     Waiter w(A.spin_limit, A.st);
+    WinStream<T> ws;
+    ws.init(A.pl, 0, true, kMixed ? (const T *)A.gv32[0] : (const T *)A.gv64[0],
+            kMixed ? (const T *)A.gv32[1] : (const T *)A.gv64[1], smem, 0xFFFFFFFFu);
+    T *xs = reinterpret_cast<T *>(smem);
 #define BAAS_BARRIER()                                            \
     do {                                                          \
-        if (!grid_barrier(A.bar, nb, A.st, A.spin_limit)) return; \
+        if (!grid_barrier(A.bar, nb, A.st, A.spin_limit)) {       \
+            ws.drain(A.spin_limit);                               \
+            return;                                               \
+        }                                                         \
     } while (0)
 
     trace_mark(A.trace, 0);
-    const int nnz = __ldg(A.a_rowptr + n);
-    for (int e = gt; e < nnz; e += W) A.lu[e] = A.a_val[e];
-    BAAS_BARRIER();
-    trace_mark(A.trace, 1);
+    if (!A.reuse) {
+        const int nnz = __ldg(A.a_rowptr + n);
+        for (int e = gt; e < nnz; e += W) A.lu[e] = A.a_val[e];
+        BAAS_BARRIER();
+        trace_mark(A.trace, 1);
 
-    factor_part<false>(A.fac, A.a_rowptr, A.a_colidx, A.a_diag, A.lu, A.gflag, A.epoch, w, A.st);
-    BAAS_BARRIER();
-    trace_mark(A.trace, 2);
+        factor_part<false>(A.fac, A.a_rowptr, A.a_colidx, A.a_diag, A.lu, A.gflag, A.epoch, w, A.st);
+        BAAS_BARRIER();
+        trace_mark(A.trace, 2);
 
-    // pack L and U = L^T into the staged value blocks (IC0_preconditioner split, :874-891);
-    // r = b - A x; sentinels
-    for (int d = 0; d < 2; d++) {
-        const int *src = A.pl.dir[d].vsrcA;
-        for (int i = gt; i < A.nv[d]; i += W) {
-            const int si = __ldg(src + i);
-            const double v = si >= 0 ? ld_l2(A.lu + si) : 0.0;
-            A.gv64[d][i] = v;
-            A.gv32[d][i] = __double2float_rn(v);
+        // pack this CTA's value slots of L and U = L^T (IC0_preconditioner split,
+        // test/iccg_level_merge.cpp:874-891)
+        for (int d = 0; d < 2; d++) {
+            const ChunkDir &D = A.pl.dir[d];
+            const int vb = __ldg(D.cval + blockIdx.x), ve = __ldg(D.cval + blockIdx.x + 1);
+            for (int i = vb + (int)threadIdx.x; i < ve; i += blockDim.x) {
+                const int s = __ldg(D.vsrcA + i);
+                const double v = s >= 0 ? ld_l2(A.lu + s) : (s <= -2 ? ld_l2(A.lu + (-2 - s)) : 0.0);
+                if constexpr (kMixed)
+                    A.gv32[d][i] = s <= -2 ? __frcp_rn(__double2float_rn(v)) : __double2float_rn(v);
+                else
+                    A.gv64[d][i] = v;
+            }
         }
+        fence_async_global();
     }
+    // r = b - A x; sentinels
     double acc = 0.0;
     for (int i = gt; i < n; i += W) {
         double s = 0.0;
@@ -414,20 +559,14 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_staged(StagedIccgArgs A
     }
     put_partial<kStageBlock>(A.part_b, acc);
     BAAS_BARRIER();
-    if constexpr (kMixed) {
-        // FP32 value blocks hold the reciprocal diagonal (each CTA converts its own rows)
-        for (int d = 0; d < 2; d++) {
-            const int c = blockIdx.x;
-            const int vo = __ldg(A.pl.dir[d].voff + c), nl = __ldg(A.pl.dir[d].nl + c);
-            for (int p = threadIdx.x; p < nl; p += blockDim.x) A.gv32[d][vo + p] = __frcp_rn(__double2float_rn(A.gv64[d][vo + p]));
-        }
-        __threadfence_block();
-    }
     const double norm0 = sqrt(grid_total<kStageBlock>(A.part_b, gridDim.x));
     trace_mark(A.trace, 3);
 
     double rzl = 0.0;
-    staged_precond<T>(A, smem, true, rzl, w);
+    if (!chunk_precond<T>(A, ws, xs, true, rzl, w)) {
+        ws.drain(A.spin_limit);
+        return;
+    }
     trace_mark(A.trace, 4);
     put_partial<kStageBlock>(A.part_c, rzl);
     BAAS_BARRIER();
@@ -474,7 +613,10 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_staged(StagedIccgArgs A
         if (rel < A.tol) break;
 
         rzl = 0.0;
-        staged_precond<T>(A, smem, false, rzl, w);
+        if (!chunk_precond<T>(A, ws, xs, false, rzl, w)) {
+            ws.drain(A.spin_limit);
+            return;
+        }
         if (k <= 8) trace_mark(A.trace, 8 + 5 * (k - 1));
         put_partial<kStageBlock>(A.part_c, rzl);
         BAAS_BARRIER();
@@ -489,6 +631,17 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_staged(StagedIccgArgs A
         BAAS_BARRIER();
         if (k <= 8) trace_mark(A.trace, 10 + 5 * (k - 1));
     }
+    if (A.grad_a) {
+        // gradient on the sparsity pattern: dL/dA_ij = -lambda_i x_j (this launch solved for
+        // lambda = A^-T dL/dx)
+        BAAS_BARRIER();
+        for (int i = gt; i < n; i += W) {
+            const double li = -A.x[i];
+            for (int e = __ldg(A.a_rowptr + i); e < __ldg(A.a_rowptr + i + 1); e++)
+                A.grad_a[e] = __dmul_rn(li, __ldg(A.xf + __ldg(A.a_colidx + e)));
+        }
+    }
+    ws.drain(A.spin_limit);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *A.out_iters = iters;
         *A.out_relres = rel;

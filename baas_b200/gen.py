@@ -50,6 +50,10 @@ class CSR:
         """Upper triangle incl. diagonal, diagonal first in each row."""
         return from_scipy(sp.triu(self.to_scipy(), format="csr"))
 
+    def transpose(self) -> "CSR":
+        """A^T in CSR (for an IC0 factor L: U = L^T, diagonal first in each row)."""
+        return from_scipy(self.to_scipy().T.tocsr())
+
     def permuted(self, perm: np.ndarray) -> "CSR":
         """Symmetric permutation P A P^T with new row i = old row perm[i]."""
         m = self.to_scipy()[perm][:, perm]

@@ -339,6 +339,45 @@ def gpu_arm(args):
         torch.distributed.destroy_process_group()
 
 
+def profile_case(args):
+    """One kernel of the bench workload, `--warmup` untimed then `--steps` timed launches, for
+    ncu captures (`-k` on the kernel name). Prints one JSON line with the mean launch time."""
+    import torch
+
+    from baas_b200 import KERNEL_ICCG, PREC_FP32_FACTORS, PREC_FP64, DeviceCSR, Schedule, gen
+
+    A = gen.laplace3d(K_GRID, 1e-3)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    dA = DeviceCSR.from_host(A)
+    b = torch.from_numpy(gen.uniform_rhs(A.n, 1)).cuda()
+    x = torch.zeros_like(b)
+    case = args.profile_case
+    if case in ("sweep_lower", "sweep_upper"):
+        lu = dA.values.clone()
+        s.ic0(dA, lu)
+        lo = gen.CSR(A.n, A.rowptr, A.colidx, lu.cpu().numpy()).lower()
+        dT = DeviceCSR.from_host(lo if case == "sweep_lower" else lo.transpose())
+        run = (lambda: s.forward(dT, b, x)) if case == "sweep_lower" else (lambda: s.backward(dT, b, x))
+    elif case == "ic0":
+        lu = dA.values.clone()
+        run = lambda: (lu.copy_(dA.values), s.ic0(dA, lu))  # noqa: E731
+    else:
+        prec = PREC_FP32_FACTORS if case == "iccg_fp32" else PREC_FP64
+        run = lambda: (x.zero_(), s.iccg(dA, b, x, tol=TOL, maxiter=MAXITER, precision=prec))  # noqa: E731
+    for _ in range(args.warmup):
+        run()
+    ts = []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    print(json.dumps({"profile_case": case, "ms_mean": round(float(np.mean(ts)), 4), "launches": args.steps}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,9 +385,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="baas_b200", choices=["baas_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", default=None,
+                    choices=["iccg", "iccg_fp32", "ic0", "sweep_lower", "sweep_upper"],
+                    help="run one kernel of the workload only (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.profile_case:
+        profile_case(args)
     else:
         gpu_arm(args)
 

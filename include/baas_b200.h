@@ -102,9 +102,11 @@ typedef struct baas_csr {
 typedef struct baas_options {
     int nthread;      /* the reference's num_thread: virtual threads of the schedule (>= 1) */
     int spin_limit;   /* polls before a device wait gives up (0 = library default) */
-    int parts;        /* CTAs that own rows in the partitioned kernels (0 = automatic: the fewest
-                         whose rows fit in shared memory, at most one per SM) */
+    int parts;        /* CTAs that own rows in the partitioned kernels (0 = automatic: about one
+                         per 2,048 rows, at most 128 and at most one per SM) */
     int partition;    /* BAAS_PARTITION_RANGES (default) or BAAS_PARTITION_BAAS_THREADS */
+    int smem_budget;  /* bytes of shared memory per CTA for solution slots and the two plan
+                         window buffers (0 = library default, 220 KiB; at most 224 KiB) */
 } baas_options;
 
 /* How rows are given to CTAs. RANGES: contiguous row-index ranges, so every cross-CTA
@@ -141,6 +143,16 @@ void baas_destroy(baas_schedule *s);
  * memory access stays in bounds and the CUDA context stays usable. Must be called before the
  * schedule's first GPU call; `row` needs an off-diagonal entry in L. */
 baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row);
+
+/* Plan test hook (no counterpart in the reference): builds the chunked sweep plan for `parts`
+ * CTAs (0 = automatic, assuming 148 SMs) and a shared-memory budget of `smem_budget` bytes (0 =
+ * default), then runs it on the host -- CTA by CTA, each step only once all its cross-CTA
+ * dependencies are written -- checking every offset, size and index against the layout the
+ * kernels read, and writes x (host arrays; tval are the triangular factor's values, upper as
+ * in baas_sptrsv). Returns BAAS_ERR_BAD_ARG with a description on any inconsistency, and
+ * BAAS_ERR_STATE once the schedule's plan is resident on a GPU. */
+baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget, int upper, const double *tval,
+                                    const double *b, double *x);
 
 /* Forward sweep x = L^-1 b (upper = 0; L is the analysed lower triangle, diagonal LAST in each
  * row) or backward sweep x = U^-1 b (upper = 1; U has the transposed pattern, diagonal FIRST).
@@ -191,6 +203,18 @@ baas_status baas_ilu0(baas_schedule *s, const baas_csr *A, double *lu, void *str
  * BAAS_KERNEL_ICCG. */
 baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, double *x, double tol,
                       int maxiter, int precision, int *iters, double *relres, void *stream);
+
+/* Adjoint of baas_iccg (no counterpart in the reference). For x = A^-1 b and a loss L(x), with
+ * g = dL/dx: solves A^T lambda = g (lambda starts at 0) by the same preconditioned CG, reusing
+ * the IC0 factors that the previous baas_iccg call on this schedule computed -- A must hold the
+ * same values and `precision` must match that call, else BAAS_ERR_STATE. A is symmetric, so
+ * the transposed preconditioner sweeps are the forward ones. Then dL/db = lambda, and if x and
+ * grad_a are given (both or neither), the same launch writes the gradient on A's sparsity
+ * pattern, grad_a[e] = -lambda_i * x_j for every entry e = (i, j) of A (nnz doubles). All
+ * arrays are device arrays; synchronises `stream`. */
+baas_status baas_iccg_adjoint(baas_schedule *s, const baas_csr *A, const double *g, double *lambda, const double *x,
+                              double *grad_a, double tol, int maxiter, int precision, int *iters, double *relres,
+                              void *stream);
 
 /* Human-readable text for the last error on this thread (never NULL). */
 const char *baas_last_error_string(void);
