@@ -381,8 +381,8 @@ void build_chunks(baas_schedule *s) {
                 }
                 C.soff[c + 1] = (int)C.srow.size();
             }
-            // one entry stride for all of the CTA's chunks: its widest row
-            int E = 0;
+            // one entry stride for all of the CTA's chunks: its widest row (at least 1)
+            int E = 1;
             for (int pos : order) E = std::max(E, H.eptr[pos + 1] - H.eptr[pos]);
             auto emit = [&](int kb, int ke) {
                 const int nl = ke - kb;

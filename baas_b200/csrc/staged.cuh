@@ -182,120 +182,172 @@ struct WinStream {
     }
 };
 
-// One row, entry stride known at compile time (EK > 0) or not (EK == 0). pf holds the values
-// of the row's remote dependencies loaded one step earlier (sentinel: wait for it now).
+// The plan of one row of a chunk, loaded into registers before the barrier that precedes its
+// step (the plan is read-only; only the solution slots change from step to step).
+template <typename T, int EK>
+struct RowPlan {
+    int row, sl, ne;
+    int d[EK];
+    T a[EK];
+    T diag;
+};
+
+template <typename T, int EK>
+__device__ __forceinline__ void load_row(const int *I, const T *V, int nl, int pos, RowPlan<T, EK> &p) {
+    const int *rowid = I + kChunkHdr;
+    p.row = rowid[pos];
+    p.sl = rowid[nl + pos];
+    p.ne = rowid[2 * nl + pos];
+    const int *dp = rowid + 3 * nl + pos * EK;
+    const T *vp = V + nl + pos * EK;
+#pragma unroll
+    for (int j = 0; j < EK; j++) {
+        p.d[j] = dp[j];
+        p.a[j] = vp[j];
+    }
+    p.diag = V[pos];
+}
+
+// Loads of the row's remote dependencies (their values, or the sentinel if not yet written);
+// issued before the barrier, they complete while the CTA waits at it.
+template <typename T, int EK>
+__device__ __forceinline__ void load_remote(const RowPlan<T, EK> &p, const T *xg, T (&pf)[EK]) {
+#pragma unroll
+    for (int j = 0; j < EK; j++) pf[j] = (j < p.ne && p.d[j] < 0) ? Sent<T>::load(xg + (-p.d[j] - 1)) : T(0);
+}
+
+// One row: dependency values gathered without branches (local slot, or the prefetched remote
+// value), one sentinel test for the whole row, and a wait only for a remote value that was not
+// yet written when it was prefetched. EXACT: the reference's FP64 operation order with correctly
+// rounded operations; else FP32 with 1/diag.
 template <typename T, bool EXACT, int EK>
-__device__ __forceinline__ bool chunk_row(int ne, const int *dp, const T *vp, T diag, T rhs, const T *xs, const T *xg,
-                                          Waiter &w, const T (&pf)[4], bool use_pf, T &out) {
-    T sum = T(0);
-    if constexpr (EK > 0) {
-        int d[EK];
-        T a[EK], xv[EK];
+__device__ __forceinline__ bool row_compute(const RowPlan<T, EK> &p, const T (&pf)[EK], const T *xs, const T *xg,
+                                            Waiter &w, T &out) {
+    T xv[EK];
+    bool miss = false;
 #pragma unroll
-        for (int j = 0; j < EK; j++) {
-            d[j] = dp[j];
-            a[j] = vp[j];
-        }
-        bool ok = true;
-#pragma unroll
-        for (int j = 0; j < EK; j++)
-            if (j < ne) {
-                if (d[j] >= 0) {
-                    xv[j] = xs[d[j]];
-                } else {
-                    xv[j] = use_pf ? pf[j] : Sent<T>::value();
-                    if (Sent<T>::is(xv[j]) && !wait_value<T>(xg + (-d[j] - 1), xv[j], w, -d[j] - 1)) ok = false;
-                }
-            }
-        if (!ok) return false;
+    for (int j = 0; j < EK; j++) {
+        const int dj = p.d[j];
+        const T loc = xs[dj >= 0 ? dj : 0];
+        xv[j] = dj >= 0 ? loc : pf[j];
+        miss |= j < p.ne && Sent<T>::is(xv[j]);
+    }
+    if (miss) {
 #pragma unroll
         for (int j = 0; j < EK; j++)
-            if (j < ne) {
-                if constexpr (EXACT)
-                    sum = __dadd_rn(sum, __dmul_rn(xv[j], a[j]));
-                else
-                    sum = fmaf(xv[j], a[j], sum);
-            }
-    } else {
-        for (int j = 0; j < ne; j++) {
-            T xv;
-            const int d = dp[j];
-            if (d >= 0)
-                xv = xs[d];
-            else if (!wait_value<T>(xg + (-d - 1), xv, w, -d - 1))
+            if (j < p.ne && p.d[j] < 0 && Sent<T>::is(xv[j]) && !wait_value<T>(xg + (-p.d[j] - 1), xv[j], w, -p.d[j] - 1))
                 return false;
+    }
+    T sum = T(0);
+#pragma unroll
+    for (int j = 0; j < EK; j++)
+        if (j < p.ne) {
             if constexpr (EXACT)
-                sum = __dadd_rn(sum, __dmul_rn(xv, vp[j]));
+                sum = __dadd_rn(sum, __dmul_rn(xv[j], p.a[j]));
             else
-                sum = fmaf(xv, vp[j], sum);
+                sum = fmaf(xv[j], p.a[j], sum);
         }
-    }
+    const T rhs = xs[p.sl];
     if constexpr (EXACT)
-        out = __ddiv_rn(__dsub_rn(rhs, sum), diag);
+        out = __ddiv_rn(__dsub_rn(rhs, sum), p.diag);
     else
-        out = (rhs - sum) * diag;  // FP32 value blocks hold 1/diag
+        out = (rhs - sum) * p.diag;  // FP32 value blocks hold 1/diag
     return true;
 }
 
-// Loads of the remote dependencies of row `pos` of the chunk at I (sentinel where not yet
-// written); they complete while the CTA waits at the barrier.
-template <typename T>
-__device__ __forceinline__ void prefetch_remote(const int *I, int pos, const T *xg, T (&pf)[4]) {
-#pragma unroll
-    for (int j = 0; j < 4; j++) pf[j] = Sent<T>::value();
-    const int nl = I[0], E = I[1];
-    const int ne = I[kChunkHdr + 2 * nl + pos];
-    const int *dp = I + kChunkHdr + 3 * nl + pos * E;
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-        if (j < ne) {
-            const int d = dp[j];
-            if (d < 0) pf[j] = Sent<T>::load(xg + (-d - 1));
-        }
-}
-
-// The rows of one chunk (one step) of nl rows at entry stride E (EK > 0: compile-time); writes
-// each result to its slot and to its row's global slot (value-as-flag), then calls
-// on_row(row, x).
-template <typename T, bool EXACT, int EK, typename OnRow>
-__device__ __forceinline__ bool chunk_step(const int *I, const T *V, int nl, int E, T *xs, T *xg, Waiter &w,
-                                           const T (&pf)[4], bool has_pf, OnRow &on_row) {
-    const int *rowid = I + kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
-    const T *diag = V, *val = V + nl;
-    for (int pos = threadIdx.x; pos < nl; pos += blockDim.x) {
-        const int sl = slot[pos];
-        T out;
-        if (!chunk_row<T, EXACT, EK>(ne[pos], dep + pos * E, val + pos * E, diag[pos], xs[sl], xs, xg, w, pf,
-                                     has_pf && pos == (int)threadIdx.x, out))
-            return false;
-        xs[sl] = out;
-        const int row = rowid[pos];
-        Sent<T>::store(xg + row, out);
-        on_row(row, out);
-    }
-    return true;
-}
-
-// Walk one window whose chunks all have entry stride E (EK > 0: compile-time, E <= 4). The
-// next chunk's row count is carried in a register and its first rows' remote dependencies are
-// loaded before the barrier.
-template <typename T, bool EXACT, int EK, typename OnRow>
-__device__ __forceinline__ bool walk_window_e(const int *I, const int *Iend, const T *V, int E, T *xs, T *xg, Waiter &w,
-                                              bool alive, OnRow &on_row) {
-    T pf[4];
-    bool has_pf = false;
+// Walk one window whose chunks all have entry stride EK (1..4). Thread t owns row t of every
+// chunk (rows beyond the block width loop, without prefetch); its next row's plan and remote
+// values are loaded before each barrier.
+template <typename T, bool EXACT, int EK>
+__device__ __forceinline__ bool walk_window_e(const int *I, const int *Iend, const T *V, T *xs, T *xg, Waiter &w,
+                                              bool alive) {
+    const int tid = threadIdx.x;
     int nl = I[0];
+    RowPlan<T, EK> rp;
+    T pf[EK];
+    bool mine = tid < nl;
+    if (mine) {
+        load_row<T, EK>(I, V, nl, tid, rp);
+        load_remote<T, EK>(rp, xg, pf);
+    }
     for (;;) {
-        if (alive) alive = chunk_step<T, EXACT, EK>(I, V, nl, E, xs, xg, w, pf, has_pf, on_row);
-        const int *In = I + chunk_nint(nl, E);
-        V += chunk_nval(nl, E);
+        if (alive && mine) {
+            T out;
+            if (row_compute<T, EXACT, EK>(rp, pf, xs, xg, w, out)) {
+                xs[rp.sl] = out;
+                Sent<T>::store(xg + rp.row, out);
+            } else {
+                alive = false;
+            }
+        }
+        for (int pos = tid + (int)blockDim.x; alive && pos < nl; pos += blockDim.x) {
+            RowPlan<T, EK> q;
+            T qf[EK];
+            load_row<T, EK>(I, V, nl, pos, q);
+#pragma unroll
+            for (int j = 0; j < EK; j++) qf[j] = Sent<T>::value();
+            T out;
+            if (!row_compute<T, EXACT, EK>(q, qf, xs, xg, w, out)) {
+                alive = false;
+                break;
+            }
+            xs[q.sl] = out;
+            Sent<T>::store(xg + q.row, out);
+        }
+        const int *In = I + chunk_nint(nl, EK);
+        const T *Vn = V + chunk_nval(nl, EK);
         const int nln = In < Iend ? In[0] : 0;
-        has_pf = EK > 0 && alive && (int)threadIdx.x < nln;
-        if (has_pf) prefetch_remote<T>(In, threadIdx.x, xg, pf);
+        mine = tid < nln;
+        if (mine) {
+            load_row<T, EK>(In, Vn, nln, tid, rp);
+            if (alive) load_remote<T, EK>(rp, xg, pf);
+        }
         __syncthreads();
         if (In >= Iend) break;
         I = In;
+        V = Vn;
         nl = nln;
+    }
+    return alive;
+}
+
+// Any entry stride (the CTA's widest row has more than 4 entries): plain loop, waits in place.
+template <typename T, bool EXACT>
+__device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, const T *V, T *xs, T *xg, Waiter &w,
+                                                bool alive) {
+    while (I < Iend) {
+        const int nl = I[0], E = I[1];
+        const int *rowid = I + kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
+        const T *diag = V, *val = V + nl;
+        for (int pos = threadIdx.x; alive && pos < nl; pos += blockDim.x) {
+            T sum = T(0);
+            for (int j = 0; j < ne[pos]; j++) {
+                const int d = dep[pos * E + j];
+                T xv;
+                if (d >= 0) {
+                    xv = xs[d];
+                } else if (!wait_value<T>(xg + (-d - 1), xv, w, -d - 1)) {
+                    alive = false;
+                    break;
+                }
+                if constexpr (EXACT)
+                    sum = __dadd_rn(sum, __dmul_rn(xv, val[pos * E + j]));
+                else
+                    sum = fmaf(xv, val[pos * E + j], sum);
+            }
+            if (!alive) break;
+            const int sl = slot[pos];
+            T out;
+            if constexpr (EXACT)
+                out = __ddiv_rn(__dsub_rn(xs[sl], sum), diag[pos]);
+            else
+                out = (xs[sl] - sum) * diag[pos];
+            xs[sl] = out;
+            Sent<T>::store(xg + rowid[pos], out);
+        }
+        I += chunk_nint(nl, E);
+        V += chunk_nval(nl, E);
+        __syncthreads();
     }
     return alive;
 }
@@ -303,19 +355,17 @@ __device__ __forceinline__ bool walk_window_e(const int *I, const int *Iend, con
 // Walk one window (nint ints of chunk blocks, then their values) held in shared memory. All
 // chunks of a CTA share one entry stride. Every thread passes every barrier, also after a
 // failed wait, so the CTA never splits.
-template <typename T, bool EXACT, typename OnRow>
-__device__ __forceinline__ bool walk_window(const unsigned char *b, int nint, T *xs, T *xg, Waiter &w, bool alive,
-                                            OnRow on_row) {
+template <typename T, bool EXACT>
+__device__ __forceinline__ bool walk_window(const unsigned char *b, int nint, T *xs, T *xg, Waiter &w, bool alive) {
     const int *I = reinterpret_cast<const int *>(b);
     const int *Iend = I + nint;
     const T *V = reinterpret_cast<const T *>(b + (size_t)nint * 4);
-    const int E = I[1];
-    switch (E) {
-        case 1: return walk_window_e<T, EXACT, 1>(I, Iend, V, 1, xs, xg, w, alive, on_row);
-        case 2: return walk_window_e<T, EXACT, 2>(I, Iend, V, 2, xs, xg, w, alive, on_row);
-        case 3: return walk_window_e<T, EXACT, 3>(I, Iend, V, 3, xs, xg, w, alive, on_row);
-        case 4: return walk_window_e<T, EXACT, 4>(I, Iend, V, 4, xs, xg, w, alive, on_row);
-        default: return walk_window_e<T, EXACT, 0>(I, Iend, V, E, xs, xg, w, alive, on_row);
+    switch (I[1]) {
+        case 1: return walk_window_e<T, EXACT, 1>(I, Iend, V, xs, xg, w, alive);
+        case 2: return walk_window_e<T, EXACT, 2>(I, Iend, V, xs, xg, w, alive);
+        case 3: return walk_window_e<T, EXACT, 3>(I, Iend, V, xs, xg, w, alive);
+        case 4: return walk_window_e<T, EXACT, 4>(I, Iend, V, xs, xg, w, alive);
+        default: return walk_window_any<T, EXACT>(I, Iend, V, xs, xg, w, alive);
     }
 }
 
@@ -412,7 +462,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, 
             if (MULTI)
                 alive = walk_window_multi(buf, nint, xs, x + (size_t)r0 * ldx, ldx, Rb, w, alive);
             else
-                alive = walk_window<double, true>(buf, nint, xs, x + (size_t)r0 * ldx, w, alive, [](int, double) {});
+                alive = walk_window<double, true>(buf, nint, xs, x + (size_t)r0 * ldx, w, alive);
             ws.release(i);
             if (__syncthreads_or(!alive)) {
                 ws.drain(spin);
@@ -458,7 +508,8 @@ struct IccgArgs {
     double *grad_a;    // if set: grad_a[e] = -x_i * xf_j for each entry e = (i, j) of A
 };
 
-// z = U^-1 L^-1 r on this CTA's rows; p = z if set_p; adds this thread's r.z to rz.
+// z = U^-1 L^-1 r on this CTA's rows; p = z if set_p; adds this thread's share of r.z to rz
+// (a pass over the CTA's slots after the upper walk, which leaves z in them).
 template <typename T>
 __device__ bool chunk_precond(const IccgArgs &A, WinStream<T> &ws, T *xs, bool set_p, double &rz, Waiter &w) {
     const int c = blockIdx.x;
@@ -473,18 +524,17 @@ __device__ bool chunk_precond(const IccgArgs &A, WinStream<T> &ws, T *xs, bool s
         const unsigned char *buf;
         int nint;
         if (!ws.acquire(i, A.spin_limit, A.st, buf, nint)) return false;
-        if (i < ws.ctl->n0) {
-            alive = walk_window<T, sizeof(T) == 8>(buf, nint, xs, yg, w, alive, [](int, T) {});
-            if (i == ws.ctl->n0 - 1) trace_mark(A.trace, 57);
-        } else {
-            alive = walk_window<T, sizeof(T) == 8>(buf, nint, xs, zg, w, alive, [&](int row, T out) {
-                const double zd = (double)out;
-                rz = __dadd_rn(rz, __dmul_rn(A.r[row], zd));
-                if (set_p) A.p[row] = zd;
-            });
-        }
+        const bool lower = i < ws.ctl->n0;
+        alive = walk_window<T, sizeof(T) == 8>(buf, nint, xs, lower ? yg : zg, w, alive);
+        if (lower && i == ws.ctl->n0 - 1) trace_mark(A.trace, 57);
         ws.release(i);
         if (__syncthreads_or(!alive)) return false;
+    }
+    for (int k = threadIdx.x; k < nl; k += blockDim.x) {
+        const int row = __ldg(A.pl.srow + s0 + k);
+        const double zd = (double)xs[k];
+        rz = __dadd_rn(rz, __dmul_rn(A.r[row], zd));
+        if (set_p) A.p[row] = zd;
     }
     trace_mark(A.trace, 59);
     return true;
