@@ -117,8 +117,8 @@ struct ChunkHostDir {
 };
 struct ChunkHost {
     ChunkHostDir dir[2];
-    std::vector<int> soff, srow;
-    int nl_max = 0;
+    std::vector<int> soff, srow;  // the rows of each CTA
+    int slot_max = 0;             // most solution slots one CTA needs in one direction
 };
 struct ChunkDevDir {
     int *ints = nullptr, *vsrcT = nullptr, *vsrcA = nullptr, *cval = nullptr;
@@ -141,7 +141,7 @@ struct ChunkDev {
 struct WinCfg {
     int4 *rec[2] = {nullptr, nullptr};
     int *swptr[2] = {nullptr, nullptr};
-    int xs_bytes = 0, cap = 0;
+    int xs_bytes = 0, rhs_bytes = 0, cap = 0;
     size_t smem = 0;
     int nrec = 0;  // most windows of one CTA, both directions
     void release() {
@@ -342,8 +342,9 @@ void build_dir(baas_schedule *s, bool upper, PartHost &out) {
 // Chunk plan from the two position plans: per CTA, each level segment becomes as many steps as
 // its largest group has rows; step j holds the j-th row of every group of the level. A step is
 // one chunk, cut into several when its block would exceed kChunkBytes (FP64 values). All chunks
-// of a CTA and direction share one entry stride, the CTA's widest row. Slots are the rows'
-// positions in the CTA's lower-sweep order.
+// of a CTA and direction share one entry stride, the CTA's widest row. A row gets a solution slot
+// only if a later row of the same CTA reads it, and only until that last read: slots are
+// allocated by liveness, so a CTA needs about two levels' worth of them, not one per row.
 constexpr int kChunkBytes = 16 * 1024;
 
 int chunk_bytes64(int nl, int E) { return baas::chunk_nint(nl, E) * 4 + baas::chunk_nval(nl, E) * 8; }
@@ -352,9 +353,10 @@ void build_chunks(baas_schedule *s) {
     const int n = s->hs.n, P = s->P;
     ChunkHost &C = s->chk;
     C = ChunkHost();
-    std::vector<int> slot_of(n, 0);
     C.soff.assign(P + 1, 0);
     C.srow.reserve(n);
+    std::vector<int> ordidx(n, -1);  // part position -> index in the CTA's step order
+    std::vector<int> kpos_of(n, 0);  // row -> its position in its CTA's row list
     for (int d = 0; d < 2; d++) {
         const PartHost &H = d == 0 ? s->fwd : s->bwd;
         ChunkHostDir &D = C.dir[d];
@@ -375,64 +377,101 @@ void build_chunks(baas_schedule *s) {
                 }
             }
             if (d == 0) {
-                for (size_t k = 0; k < order.size(); k++) {
-                    slot_of[H.row[order[k]]] = (int)k;
-                    C.srow.push_back(H.row[order[k]]);
+                for (int pos : order) {
+                    kpos_of[H.row[pos]] = (int)C.srow.size() - C.soff[c];
+                    C.srow.push_back(H.row[pos]);
                 }
                 C.soff[c + 1] = (int)C.srow.size();
             }
+            const int no = (int)order.size();
+            for (int k = 0; k < no; k++) ordidx[order[k]] = k;
             // one entry stride for all of the CTA's chunks: its widest row (at least 1)
             int E = 1;
             for (int pos : order) E = std::max(E, H.eptr[pos + 1] - H.eptr[pos]);
-            auto emit = [&](int kb, int ke) {
-                const int nl = ke - kb;
+            // chunks: each step, cut into pieces of at most kChunkBytes
+            std::vector<std::pair<int, int>> chunks;
+            int kb = 0;
+            for (int se : step_end) {
+                int cb = kb;
+                for (int k = kb; k < se; k++)
+                    if (k > cb && chunk_bytes64(k + 1 - cb, E) > kChunkBytes) {
+                        chunks.push_back({cb, k});
+                        cb = k;
+                    }
+                if (se > cb) chunks.push_back({cb, se});
+                kb = se;
+            }
+            // liveness: the last chunk in which a row of this CTA reads each row's value
+            std::vector<int> chunk_of(no), last_use(no, -1);
+            for (size_t t = 0; t < chunks.size(); t++)
+                for (int k = chunks[t].first; k < chunks[t].second; k++) chunk_of[k] = (int)t;
+            for (int k = 0; k < no; k++) {
+                const int pos = order[k];
+                for (int e = H.eptr[pos]; e < H.eptr[pos + 1]; e++)
+                    if (H.dep[e] < 0) {
+                        const int kp = ordidx[H.cta_pos[c] + (-H.dep[e] - 1)];
+                        last_use[kp] = std::max(last_use[kp], chunk_of[k]);
+                    }
+            }
+            // slots: a row holds one from its own chunk to its last local reader's chunk; a
+            // slot freed after chunk t serves rows of chunk t+1 onwards
+            std::vector<int> slot(no, -1), free_slots;
+            std::vector<std::vector<int>> release((size_t)chunks.size() + 1);
+            int nslots = 0;
+            for (size_t t = 0; t < chunks.size(); t++) {
+                if (t > 0)
+                    for (int sl : release[t - 1]) free_slots.push_back(sl);
+                for (int k = chunks[t].first; k < chunks[t].second; k++) {
+                    if (last_use[k] < 0) continue;
+                    int sl;
+                    if (!free_slots.empty()) {
+                        sl = free_slots.back();
+                        free_slots.pop_back();
+                    } else {
+                        sl = nslots++;
+                    }
+                    slot[k] = sl;
+                    release[last_use[k]].push_back(sl);
+                }
+            }
+            C.slot_max = std::max(C.slot_max, nslots);
+            for (size_t t = 0; t < chunks.size(); t++) {
+                const int cb = chunks[t].first, ce = chunks[t].second, nl = ce - cb;
                 const size_t i0 = D.ints.size();
                 D.ints.resize(i0 + baas::chunk_nint(nl, E), 0);
                 int *I = D.ints.data() + i0;
                 I[0] = nl;
                 I[1] = E;
-                int *rowid = I + baas::kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
+                I[2] = t + 1 < chunks.size() ? chunks[t + 1].second - chunks[t + 1].first : 0;
+                int *rowid = I + baas::kChunkHdr, *sl = rowid + nl, *ne = sl + nl, *kp = ne + nl, *dep = kp + nl;
                 const size_t v0 = D.vsrcT.size();
                 D.vsrcT.resize(v0 + baas::chunk_nval(nl, E), -1);
                 D.vsrcA.resize(v0 + baas::chunk_nval(nl, E), -1);
                 int *vT = D.vsrcT.data() + v0, *vA = D.vsrcA.data() + v0;
-                for (int k = kb; k < ke; k++) {
-                    const int q = k - kb, pos = order[k], r = H.row[pos];
-                    rowid[q] = r;
-                    slot[q] = slot_of[r];
+                for (int k = cb; k < ce; k++) {
+                    const int q = k - cb, pos = order[k];
+                    rowid[q] = H.row[pos];
+                    sl[q] = slot[k];
+                    kp[q] = kpos_of[H.row[pos]];
                     ne[q] = H.eptr[pos + 1] - H.eptr[pos];
                     vT[q] = baas::diag_code(H.dsrcT[pos]);
                     vA[q] = baas::diag_code(H.dsrcA[pos]);
                     for (int j = 0; j < ne[q]; j++) {
                         const int e = H.eptr[pos] + j;
                         const int dd = H.dep[e];
-                        // local: the dependency's slot; remote: -(row + 1)
-                        dep[q * E + j] = dd < 0 ? slot_of[H.row[H.cta_pos[c] + (-dd - 1)]] : -(dd + 1);
+                        // local: the producer's slot; remote: -(row + 1)
+                        dep[q * E + j] = dd < 0 ? slot[ordidx[H.cta_pos[c] + (-dd - 1)]] : -(dd + 1);
                         vT[nl + q * E + j] = H.srcT[e];
                         vA[nl + q * E + j] = H.srcA[e];
                     }
                 }
                 D.chunk_ioff.push_back((int)D.ints.size());
                 D.chunk_voff.push_back((int)D.vsrcT.size());
-            };
-            int kb = 0;
-            for (int se : step_end) {
-                // cut the step [kb, se) into chunks of at most kChunkBytes
-                int cb = kb;
-                for (int k = kb; k < se; k++)
-                    if (k > cb && chunk_bytes64(k + 1 - cb, E) > kChunkBytes) {
-                        emit(cb, k);
-                        cb = k;
-                    }
-                if (se > cb) emit(cb, se);
-                kb = se;
             }
             D.cchunk[c + 1] = (int)D.chunk_ioff.size() - 1;
             D.cval[c + 1] = (int)D.vsrcT.size();
         }
     }
-    C.nl_max = 0;
-    for (int c = 0; c < P; c++) C.nl_max = std::max(C.nl_max, C.soff[c + 1] - C.soff[c]);
 }
 
 // Windows for values of `vbytes` bytes and R right-hand sides: each CTA's chunks grouped
@@ -441,10 +480,17 @@ void build_chunks(baas_schedule *s) {
 // as large as it allows), and never larger than the largest window formed, so that shared
 // memory the plan does not need stays L1 cache for the SpMV and vector phases.
 constexpr int kWindowTarget = 32 * 1024;
+constexpr int kStagedMinCap = 16 * 1024;
 
 bool plan_windows(const ChunkHost &C, int P, int budget, bool explicit_budget, int vbytes, int R,
-                  std::vector<int4> rec[2], std::vector<int> swptr[2], int &xs_bytes, int &cap, int &nrec) {
-    xs_bytes = (int)(((long long)C.nl_max * R * vbytes + 127) / 128 * 128);
+                  std::vector<int4> rec[2], std::vector<int> swptr[2], int &xs_bytes, int &rhs_bytes, int &cap,
+                  int &nrec) {
+    xs_bytes = (int)(((long long)C.slot_max * R * vbytes + 127) / 128 * 128);
+    // right-hand sides staged in shared memory when the CTA's rows' values fit beside the slots
+    // and two buffers of at least kStagedMinCap
+    int rows_max = 0;
+    for (int c = 0; c < P; c++) rows_max = std::max(rows_max, C.soff[c + 1] - C.soff[c]);
+    rhs_bytes = (int)(((long long)rows_max * R * vbytes + 127) / 128 * 128);
     long long big = 0;  // every chunk must fit a buffer
     for (int d = 0; d < 2; d++) {
         const ChunkHostDir &D = C.dir[d];
@@ -455,7 +501,9 @@ bool plan_windows(const ChunkHost &C, int P, int budget, bool explicit_budget, i
     // the control block holds one record per window of a CTA: reserve room for it, and grow
     // the reserve if the windows outnumber it
     for (int reserve = 1024;;) {
-        const int cap_max = ((budget - xs_bytes - reserve) / 2) & ~127;
+        if (rhs_bytes > 0 && ((budget - xs_bytes - rhs_bytes - reserve) / 2 < std::max<long long>(big, kStagedMinCap)))
+            rhs_bytes = 0;
+        const int cap_max = ((budget - xs_bytes - rhs_bytes - reserve) / 2) & ~127;
         if (cap_max < 1024 || big > cap_max) return false;
         cap = explicit_budget ? cap_max : std::min(cap_max, kWindowTarget);
         cap = std::max(cap, (int)((big + 127) / 128 * 128));
@@ -507,8 +555,9 @@ baas_status get_windows(baas_schedule *s, int vbytes, int R, WinCfg **out) {
     }
     std::vector<int4> rec[2];
     std::vector<int> swptr[2];
-    int xs_bytes = 0, cap = 0, mw = 0;
-    if (!plan_windows(s->chk, s->P, s->smem_budget, s->opt.smem_budget > 0, vbytes, R, rec, swptr, xs_bytes, cap, mw))
+    int xs_bytes = 0, rhs_bytes = 0, cap = 0, mw = 0;
+    if (!plan_windows(s->chk, s->P, s->smem_budget, s->opt.smem_budget > 0, vbytes, R, rec, swptr, xs_bytes, rhs_bytes,
+                      cap, mw))
         return fail(BAAS_ERR_BAD_ARG, "a CTA's rows do not fit its shared memory: raise `parts` or smem_budget");
     WinCfg w;
     for (int d = 0; d < 2; d++) {
@@ -516,8 +565,9 @@ baas_status get_windows(baas_schedule *s, int vbytes, int R, WinCfg **out) {
         BAAS_TRY(upload(w.swptr[d], swptr[d]));
     }
     w.xs_bytes = xs_bytes;
+    w.rhs_bytes = rhs_bytes;
     w.cap = cap;
-    w.smem = (size_t)baas::chunk_smem_bytes(xs_bytes, cap, mw);
+    w.smem = (size_t)baas::chunk_smem_bytes(xs_bytes, rhs_bytes, cap, mw);
     w.nrec = mw;
     *out = &(s->wins[key] = w);
     return BAAS_OK;
@@ -533,6 +583,7 @@ baas::ChunkPlan chunk_plan(const baas_schedule *s, const WinCfg &w) {
     p.soff = s->d_chk.soff;
     p.srow = s->d_chk.srow;
     p.xs_bytes = w.xs_bytes;
+    p.rhs_bytes = w.rhs_bytes;
     p.cap = w.cap;
     p.nrec = w.nrec;
     return p;
@@ -582,10 +633,14 @@ baas_status ensure_device(baas_schedule *s) {
     BAAS_TRY(dalloc(s->d_bar, 1));
     BAAS_CUDA(cudaMallocHost((void **)&s->h_status, sizeof(DevStatus)));
     if (getenv("BAAS_TRACE") && atoi(getenv("BAAS_TRACE")) > 0) BAAS_TRY(dalloc(s->d_trace, 2 * baas::kTraceSlots));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_sweep_chunked<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_sweep_chunked<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_iccg_chunked<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
-    BAAS_CUDA(cudaFuncSetAttribute(baas::k_iccg_chunked<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
+    {
+        const void *kerns[] = {(const void *)baas::k_sweep_chunked<false, false>, (const void *)baas::k_sweep_chunked<false, true>,
+                               (const void *)baas::k_sweep_chunked<true, false>, (const void *)baas::k_sweep_chunked<true, true>,
+                               (const void *)baas::k_iccg_chunked<double, false>, (const void *)baas::k_iccg_chunked<double, true>,
+                               (const void *)baas::k_iccg_chunked<float, false>, (const void *)baas::k_iccg_chunked<float, true>};
+        for (const void *k : kerns)
+            BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
+    }
     s->uploaded = true;
     // the single-right-hand-side FP64 windows must exist for every kind of call
     WinCfg *w = nullptr;
@@ -593,12 +648,12 @@ baas_status ensure_device(baas_schedule *s) {
     // multi-right-hand-side sweeps: the widest batch that leaves both window buffers >= 8 KiB
     s->rmax64 = 1;
     for (int R = baas::kMaxRhs; R > 1; R--) {
-        const long long xs = ((long long)s->chk.nl_max * R * 8 + 127) / 128 * 128;
+        const long long xs = ((long long)s->chk.slot_max * R * 8 + 127) / 128 * 128;
         if ((s->smem_budget - xs - 32) / 2 < 8 * 1024) continue;
         std::vector<int4> rec[2];
         std::vector<int> swptr[2];
-        int xb = 0, cap = 0, mw = 0;
-        if (plan_windows(s->chk, s->P, s->smem_budget, s->opt.smem_budget > 0, 8, R, rec, swptr, xb, cap, mw)) {
+        int xb = 0, rb = 0, cap = 0, mw = 0;
+        if (plan_windows(s->chk, s->P, s->smem_budget, s->opt.smem_budget > 0, 8, R, rec, swptr, xb, rb, cap, mw)) {
             s->rmax64 = R;
             break;
         }
@@ -787,14 +842,16 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
     const int budget = smem_budget > 0 ? std::min(smem_budget, kMaxSmemBudget) : (int)kSmemBudget;
     std::vector<int4> rec[2];
     std::vector<int> swptr[2];
-    int xs_bytes = 0, cap = 0, mw = 0;
-    if (!plan_windows(s->chk, P, budget, smem_budget > 0, 8, 1, rec, swptr, xs_bytes, cap, mw))
+    int xs_bytes = 0, rhs_bytes = 0, cap = 0, mw = 0;
+    if (!plan_windows(s->chk, P, budget, smem_budget > 0, 8, 1, rec, swptr, xs_bytes, rhs_bytes, cap, mw))
         return fail(BAAS_ERR_BAD_ARG, "emulate: a chunk does not fit the window buffer");
-    if (baas::chunk_smem_bytes(xs_bytes, cap, mw) > budget) return fail(BAAS_ERR_BAD_ARG, "emulate: shared memory over budget");
+    if (baas::chunk_smem_bytes(xs_bytes, rhs_bytes, cap, mw) > budget)
+        return fail(BAAS_ERR_BAD_ARG, "emulate: shared memory over budget");
     const int d = upper ? 1 : 0;
     const ChunkHostDir &D = s->chk.dir[d];
     const ChunkHost &C = s->chk;
     auto bad = [](const std::string &m) { return fail(BAAS_ERR_BAD_ARG, "emulate: " + m); };
+    if (s->fault_row >= 0) return fail(BAAS_ERR_STATE, "emulate: the schedule carries an injected fault");
     // packing of the value slots, as the sweep kernel does
     std::vector<double> gv(D.vsrcT.size());
     for (size_t i = 0; i < gv.size(); i++) {
@@ -804,22 +861,25 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
         gv[i] = src >= 0 ? tval[src] : 0.0;
     }
     std::vector<char> ready(n, 0);
+    // the column that entry j of row r must read: L rows ascending (diagonal last), U = L^T rows
+    // descending (diagonal first)
+    const baas::HostSchedule &hs = s->hs;
+    auto column = [&](int r, int j) {
+        return upper ? s->crow[s->cptr[r + 1] - 1 - j] : hs.l_colidx[hs.l_rowptr[r] + j];
+    };
     struct Cta {
         int q = 0, qend = 0;
         std::vector<int> ibuf;
         std::vector<double> vbuf;
         size_t ip = 0, vp = 0;
         bool loaded = false, done = false;
-        std::vector<double> xs;
-        std::vector<char> xs_done;
+        int expect_nl = -1;  // the row count the previous chunk announced for this one
     };
     std::vector<Cta> cta(P);
+    std::vector<std::vector<double>> xs(P, std::vector<double>((size_t)std::max(C.slot_max, 1), 0.0));
+    std::vector<std::vector<int>> owner(P, std::vector<int>((size_t)std::max(C.slot_max, 1), -1));
     for (int c = 0; c < P; c++) {
         Cta &K = cta[c];
-        const int s0 = C.soff[c], nl = C.soff[c + 1] - s0;
-        K.xs.resize(nl);
-        K.xs_done.assign(nl, 0);
-        for (int k = 0; k < nl; k++) K.xs[k] = b[C.srow[s0 + k]];
         K.q = swptr[d][c];
         K.qend = swptr[d][c + 1];
         K.done = K.q == K.qend;
@@ -844,13 +904,14 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
             }
             const int *I = K.ibuf.data() + K.ip;
             const int nl = I[0], E = I[1];
-            if (nl < 1 || E < 0) return bad("bad chunk header");
+            if (nl < 1 || E < 1) return bad("bad chunk header");
+            if (K.expect_nl >= 0 && K.expect_nl != nl) return bad("a chunk header announces the wrong next row count");
             if (K.ip + baas::chunk_nint(nl, E) > K.ibuf.size() || K.vp + baas::chunk_nval(nl, E) > K.vbuf.size())
                 return bad("chunk runs past its window");
-            const int *rowid = I + baas::kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
+            const int *rowid = I + baas::kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *kp = ne + nl, *dep = kp + nl;
             const double *V = K.vbuf.data() + K.vp;
             const double *diag = V, *val = V + nl;
-            const int nlc = (int)K.xs.size();
+            const int ns = C.slot_max;
             bool wait = false;
             for (int pos = 0; pos < nl && !wait; pos++) {
                 if (ne[pos] < 0 || ne[pos] > E) return bad("row entry count exceeds the chunk stride");
@@ -864,33 +925,47 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
                 }
             }
             if (wait) continue;
+            // all reads of the step happen before any of its writes (the barrier semantics)
+            std::vector<double> outs(nl);
             for (int pos = 0; pos < nl; pos++) {
-                const int sl = slot[pos], row = rowid[pos];
-                if (sl < 0 || sl >= nlc) return bad("slot out of range");
+                const int row = rowid[pos];
                 if (row < 0 || row >= n || ready[row]) return bad("row out of range or computed twice");
+                if (kp[pos] < 0 || kp[pos] >= C.soff[c + 1] - C.soff[c] || C.srow[C.soff[c] + kp[pos]] != row)
+                    return bad("a row's staging position does not name it");
                 double sum = 0.0;
                 for (int j = 0; j < ne[pos]; j++) {
                     const int dd = dep[pos * E + j];
+                    const int col = column(row, j);
                     double xv;
                     if (dd >= 0) {
-                        if (dd >= nlc || !K.xs_done[dd]) return bad("local dependency not yet computed");
-                        xv = K.xs[dd];
+                        if (dd >= ns) return bad("slot out of range");
+                        if (owner[c][dd] != col) return bad("a slot does not hold the column the row needs");
+                        xv = xs[c][dd];
                     } else {
+                        if (-dd - 1 != col) return bad("a remote dependency names the wrong column");
                         xv = x[-dd - 1];
                     }
                     sum = sum + xv * val[pos * E + j];
                 }
-                const double out = (K.xs[sl] - sum) / diag[pos];
-                K.xs[sl] = out;
-                K.xs_done[sl] = 1;
-                x[row] = out;
+                outs[pos] = (b[row] - sum) / diag[pos];
+            }
+            for (int pos = 0; pos < nl; pos++) {
+                const int sl = slot[pos], row = rowid[pos];
+                if (sl >= ns) return bad("slot out of range");
+                if (sl >= 0) {
+                    xs[c][sl] = outs[pos];
+                    owner[c][sl] = row;
+                }
+                x[row] = outs[pos];
                 ready[row] = 1;
             }
+            K.expect_nl = I[2];
             K.ip += baas::chunk_nint(nl, E);
             K.vp += baas::chunk_nval(nl, E);
             if (K.ip == K.ibuf.size()) {
                 K.loaded = false;
                 if (++K.q == K.qend) {
+                    if (K.expect_nl != 0) return bad("the last chunk announces a successor");
                     K.done = true;
                     remaining--;
                 }
@@ -956,7 +1031,9 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
     double *gv = s->d_gvT[d];
     void *args[] = {(void *)&pl, (void *)&d, (void *)&T->values, (void *)&gv, (void *)&b, (void *)&ldb, (void *)&x,
                     (void *)&ldb, (void *)&nrhs, (void *)&R, (void *)&s->d_status, (void *)&spin, (void *)&s->d_trace};
-    void *kern = R > 1 ? (void *)baas::k_sweep_chunked<true> : (void *)baas::k_sweep_chunked<false>;
+    const bool stg = w->rhs_bytes > 0;
+    void *kern = R > 1 ? (stg ? (void *)baas::k_sweep_chunked<true, true> : (void *)baas::k_sweep_chunked<true, false>)
+                       : (stg ? (void *)baas::k_sweep_chunked<false, true> : (void *)baas::k_sweep_chunked<false, false>);
     BAAS_CUDA(cudaLaunchCooperativeKernel(kern, s->P, baas::kStageBlock, args, w->smem, stream));
     dump_trace(s, upper ? "sptrsv-upper" : "sptrsv-lower", stream);
     return read_status(s, stream);
@@ -1100,7 +1177,9 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
     a.xf = xf;
     a.grad_a = grad_a;
     void *args[] = {(void *)&a};
-    void *kern = mixed ? (void *)baas::k_iccg_chunked<float> : (void *)baas::k_iccg_chunked<double>;
+    const bool stg = w->rhs_bytes > 0;
+    void *kern = mixed ? (stg ? (void *)baas::k_iccg_chunked<float, true> : (void *)baas::k_iccg_chunked<float, false>)
+                       : (stg ? (void *)baas::k_iccg_chunked<double, true> : (void *)baas::k_iccg_chunked<double, false>);
     BAAS_CUDA(cudaLaunchCooperativeKernel(kern, P, baas::kStageBlock, args, w->smem, stream));
     int it = 0;
     double rr = 0.0;

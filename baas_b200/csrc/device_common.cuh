@@ -216,6 +216,37 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned int 
     return false;
 }
 
+// Explicit shared-memory accesses for data reached through pointers the compiler cannot prove
+// to be shared (window buffers, staged arrays handed through structures): a generic access to
+// shared memory is resolved in the L1TEX unit and costs far more than ld/st.shared. Volatile,
+// so they keep their order relative to one another and to barriers; no "memory" clobber, so
+// they do not serialise the surrounding code.
+template <typename T> struct Sh;
+template <> struct Sh<int> {
+    static __device__ __forceinline__ int ld(const int *p) {
+        int v;
+        asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)));
+        return v;
+    }
+    static __device__ __forceinline__ void st(int *p, int v) { asm volatile("st.shared.s32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v)); }
+};
+template <> struct Sh<float> {
+    static __device__ __forceinline__ float ld(const float *p) {
+        float v;
+        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(smem_u32(p)));
+        return v;
+    }
+    static __device__ __forceinline__ void st(float *p, float v) { asm volatile("st.shared.f32 [%0], %1;" ::"r"(smem_u32(p)), "f"(v)); }
+};
+template <> struct Sh<double> {
+    static __device__ __forceinline__ double ld(const double *p) {
+        double v;
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
+        return v;
+    }
+    static __device__ __forceinline__ void st(double *p, double v) { asm volatile("st.shared.f64 [%0], %1;" ::"r"(smem_u32(p)), "d"(v)); }
+};
+
 // Phase tracing (BAAS_TRACE=1): thread 0 of the first and last CTA record %globaltimer (ns)
 // at phase boundaries into trace[cta_sel * kTraceSlots + k]; a NULL trace disables it.
 constexpr int kTraceSlots = 64;

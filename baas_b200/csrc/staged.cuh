@@ -8,14 +8,18 @@
 // thread k (k, k + blockDim, ... when a step is wider than the CTA).
 //
 // The plan of a step is a self-contained CHUNK (a wide step is cut into several):
-//   int block   [nl, E, 0, 0 | rowid (nl) | slot (nl) | ne (nl) | dep (nl*E)], padded to 8 ints
+//   int block   [nl, E, nl_next, 0 | rowid (nl) | slot (nl) | ne (nl) | kpos (nl) | dep (nl*E)],
+//               padded to 8 ints
 //   value block [diag (nl) | val (nl*E)], padded to 4 values
 // with E the widest row of the CTA (one stride for all of a CTA's chunks, so the walk is
 // specialised on it once per window), and row `pos` finds its entries at pos*E + j.
-// dep >= 0 is a CTA-local slot (final after the barrier that ended the producing step); dep < 0
-// is -(row+1) of a row owned by another CTA (a value-as-flag wait on its global slot). The
-// slot of a row is its position in the CTA's lower-sweep order; the lower and the upper sweep
-// use the same slots, so the upper sweep finds its right-hand side (the lower result) in place.
+// nl_next is the next chunk's row count (what the pipelined walk needs to address it early).
+// dep >= 0 is a CTA-local solution slot (final after the barrier that ended the producing
+// step); dep < 0 is -(row+1) of a row owned by another CTA (a value-as-flag wait on its global
+// result). A row has a slot (slot >= 0) only while a later row of the same CTA still has to read
+// it. kpos is the row's position in the CTA's row list: where its right-hand side sits when
+// the CTA's right-hand sides are staged in shared memory (when they fit; else they come from
+// global memory).
 //
 // A CTA's chunks are contiguous in global memory. Consecutive chunks are grouped into WINDOWS
 // that fit one of two shared-memory buffers; a window arrives through two bulk copies (ints,
@@ -30,14 +34,16 @@
 
 namespace baas {
 
-constexpr int kStageBlock = 512;
+// 256 threads: steps hold tens of rows per CTA, so more threads would only add idle warps to
+// every step barrier; and the pipelined walk gets up to 255 registers.
+constexpr int kStageBlock = 256;
 constexpr int kChunkHdr = 4;
 constexpr int kIssuer = kStageBlock - 32;  // lane 0 of the last warp issues the bulk copies
 constexpr int kMaxRhs = 8;                 // right-hand sides walked together
 
 __host__ __device__ constexpr int pad4(int x) { return (x + 3) & ~3; }
 __host__ __device__ constexpr int pad8(int x) { return (x + 7) & ~7; }
-__host__ __device__ constexpr int chunk_nint(int nl, int E) { return pad8(kChunkHdr + 3 * nl + nl * E); }
+__host__ __device__ constexpr int chunk_nint(int nl, int E) { return pad8(kChunkHdr + 4 * nl + nl * E); }
 __host__ __device__ constexpr int chunk_nval(int nl, int E) { return pad4(nl + nl * E); }
 // value-source code of a diagonal entry at position p (off-diagonals: p >= 0; padding: -1)
 __host__ __device__ constexpr int diag_code(int p) { return -2 - p; }
@@ -56,12 +62,13 @@ struct ChunkPlan {
     const int *soff;  // P + 1: slots of each CTA
     const int *srow;  // row of each slot, CTA by CTA
     int xs_bytes;     // shared-memory bytes of the solution slots
+    int rhs_bytes;    // shared-memory bytes of the staged right-hand sides (0: read from global)
     int cap;          // bytes of each window buffer
     int nrec;         // most windows of one CTA, both directions together
 };
 
-// shared memory: [slots | buffer 0 | buffer 1 | stream control block with the CTA's window
-// records]; nrec = the most windows one CTA has (both directions)
+// shared memory: [slots | staged right-hand sides | buffer 0 | buffer 1 | stream control block
+// with the CTA's window records]; nrec = the most windows one CTA has (both directions)
 struct WinCtl {
     unsigned long long mbar[2];
     int nint[2];              // int count of the window in each buffer
@@ -73,8 +80,8 @@ struct WinCtl {
     int4 rec[1];              // n0 + n1 window records {int offset, ints, value offset, values}
 };
 __host__ __device__ constexpr int win_ctl_bytes(int nrec) { return 128 + 16 * nrec; }
-__host__ __device__ constexpr int chunk_smem_bytes(int xs_bytes, int cap, int nrec) {
-    return xs_bytes + 2 * cap + win_ctl_bytes(nrec);
+__host__ __device__ constexpr int chunk_smem_bytes(int xs_bytes, int rhs_bytes, int cap, int nrec) {
+    return xs_bytes + rhs_bytes + 2 * cap + win_ctl_bytes(nrec);
 }
 
 // Value of source code s in array v (the packing of a window's value slots).
@@ -98,8 +105,8 @@ struct WinStream {
                          unsigned int lim) {
         const int c = blockIdx.x;
         cap = pl.cap;
-        buf = smem + pl.xs_bytes;
-        ctl = reinterpret_cast<WinCtl *>(smem + pl.xs_bytes + 2 * pl.cap);
+        buf = smem + pl.xs_bytes + pl.rhs_bytes;
+        ctl = reinterpret_cast<WinCtl *>(buf + 2 * pl.cap);
         issued = consumed = 0;
         loaded = false;
         const ChunkDir &A = first ? pl.dir[1] : pl.dir[0];
@@ -182,36 +189,89 @@ struct WinStream {
     }
 };
 
-// The plan of one row of a chunk, loaded into registers before the barrier that precedes its
-// step (the plan is read-only; only the solution slots change from step to step).
-template <typename T, int EK>
-struct RowPlan {
-    int row, sl, ne;
-    int d[EK];
-    T a[EK];
-    T diag;
+// Where a walk finds its right-hand sides and puts its results, and which (row, right-hand
+// side) pairs a thread computes. MR = false: one right-hand side, thread t takes rows t,
+// t + blockDim, ... of every chunk. MR = true: thread t takes right-hand side t % R of rows
+// t / R, t / R + stride, ... (stride = blockDim / R rows per pass). STG: the CTA's right-hand
+// sides are staged in shared memory at rs[kpos * R + r], and each result is written back there.
+template <typename T, typename RT, bool MR, bool STG>
+struct WalkIO {
+    T *xs;          // solution slots: xs[slot * R + r]
+    T *xg;          // results, value-as-flag: xg[r * ldx + row]
+    const RT *rhs;  // right-hand sides in global memory: rhs[r * ldr + row] (unless STG)
+    T *rs;          // staged right-hand sides (STG)
+    int ldx, ldr, R_;
+    __device__ int R() const { return MR ? R_ : 1; }
+    __device__ int stride() const { return MR ? (int)blockDim.x / R_ : (int)blockDim.x; }
+    __device__ int rr() const { return MR ? (int)threadIdx.x % R_ : 0; }
+    // this thread's first row of a chunk (a huge value: the thread is idle)
+    __device__ int lane_row() const {
+        if (!MR) return (int)threadIdx.x;
+        return (int)threadIdx.x < stride() * R_ ? (int)threadIdx.x / R_ : 0x3fffffff;
+    }
+    __device__ T *out() const { return MR ? xg + (size_t)rr() * ldx : xg; }
+    __device__ const RT *in() const { return MR ? rhs + (size_t)rr() * ldr : rhs; }
+    __device__ int slot(int sl) const { return MR ? sl * R_ + rr() : sl; }
 };
 
+// Dependency indices, entry count, row and staging position of one row: loaded one step
+// ahead, because the loads issued before the barrier need them.
+template <int EK>
+struct RowDeps {
+    int row, ne, kpos;
+    int d[EK];
+};
+// The rest of a row's plan and its right-hand side.
 template <typename T, int EK>
-__device__ __forceinline__ void load_row(const int *I, const T *V, int nl, int pos, RowPlan<T, EK> &p) {
+struct RowVals {
+    int sl;
+    T a[EK];
+    T diag, rhs;
+};
+
+template <int EK>
+__device__ __forceinline__ void load_deps(const int *I, int nl, int pos, RowDeps<EK> &p) {
     const int *rowid = I + kChunkHdr;
-    p.row = rowid[pos];
-    p.sl = rowid[nl + pos];
-    p.ne = rowid[2 * nl + pos];
-    const int *dp = rowid + 3 * nl + pos * EK;
+    p.row = Sh<int>::ld(rowid + pos);
+    p.ne = Sh<int>::ld(rowid + 2 * nl + pos);
+    p.kpos = Sh<int>::ld(rowid + 3 * nl + pos);
+    const int *dp = rowid + 4 * nl + pos * EK;
+#pragma unroll
+    for (int j = 0; j < EK; j++) p.d[j] = Sh<int>::ld(dp + j);
+}
+
+// The rest of a row's plan, and its staged right-hand side (STG).
+template <typename T, typename RT, bool RL2, bool MR, bool STG, int EK>
+__device__ __forceinline__ void load_vals(const int *I, const T *V, int nl, int pos, const RowDeps<EK> &p,
+                                          const WalkIO<T, RT, MR, STG> &io, RowVals<T, EK> &v) {
+    v.sl = Sh<int>::ld(I + kChunkHdr + nl + pos);
     const T *vp = V + nl + pos * EK;
 #pragma unroll
-    for (int j = 0; j < EK; j++) {
-        p.d[j] = dp[j];
-        p.a[j] = vp[j];
+    for (int j = 0; j < EK; j++) v.a[j] = Sh<T>::ld(vp + j);
+    v.diag = Sh<T>::ld(V + pos);
+    if constexpr (STG) v.rhs = Sh<T>::ld(io.rs + io.slot(p.kpos));
+}
+
+// A row's right-hand side: staged in shared memory, or from global memory (RL2: written
+// earlier in the same launch by this CTA, so read from L2, where those writes went).
+template <typename T, typename RT, bool RL2, bool MR, bool STG>
+__device__ __forceinline__ T load_rhs(int row, int kpos, const WalkIO<T, RT, MR, STG> &io) {
+    if constexpr (STG) {
+        return Sh<T>::ld(io.rs + io.slot(kpos));
+    } else {
+        const RT *src = io.in() + row;
+        if constexpr (RL2)
+            return (T)Sent<RT>::load(src);
+        else
+            return (T)*src;
     }
-    p.diag = V[pos];
 }
 
 // Loads of the row's remote dependencies (their values, or the sentinel if not yet written);
-// issued before the barrier, they complete while the CTA waits at it.
-template <typename T, int EK>
-__device__ __forceinline__ void load_remote(const RowPlan<T, EK> &p, const T *xg, T (&pf)[EK]) {
+// issued before a barrier, they complete while the CTA waits at it.
+template <typename T, typename RT, bool MR, bool STG, int EK>
+__device__ __forceinline__ void load_remote(const RowDeps<EK> &p, const WalkIO<T, RT, MR, STG> &io, T (&pf)[EK]) {
+    const T *xg = io.out();
 #pragma unroll
     for (int j = 0; j < EK; j++) pf[j] = (j < p.ne && p.d[j] < 0) ? Sent<T>::load(xg + (-p.d[j] - 1)) : T(0);
 }
@@ -219,16 +279,18 @@ __device__ __forceinline__ void load_remote(const RowPlan<T, EK> &p, const T *xg
 // One row: dependency values gathered without branches (local slot, or the prefetched remote
 // value), one sentinel test for the whole row, and a wait only for a remote value that was not
 // yet written when it was prefetched. EXACT: the reference's FP64 operation order with correctly
-// rounded operations; else FP32 with 1/diag.
-template <typename T, bool EXACT, int EK>
-__device__ __forceinline__ bool row_compute(const RowPlan<T, EK> &p, const T (&pf)[EK], const T *xs, const T *xg,
-                                            Waiter &w, T &out) {
+// rounded operations; else FP32 with 1/diag. Writes the slot (if a later row of the CTA reads
+// it), the staged copy (STG) and the global result.
+template <typename T, typename RT, bool MR, bool STG, bool EXACT, int EK>
+__device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<T, EK> &v, const T (&pf)[EK],
+                                            const WalkIO<T, RT, MR, STG> &io, Waiter &w) {
+    T *xg = io.out();
     T xv[EK];
     bool miss = false;
 #pragma unroll
     for (int j = 0; j < EK; j++) {
         const int dj = p.d[j];
-        const T loc = xs[dj >= 0 ? dj : 0];
+        const T loc = Sh<T>::ld(io.xs + io.slot(dj >= 0 ? dj : 0));
         xv[j] = dj >= 0 ? loc : pf[j];
         miss |= j < p.ne && Sent<T>::is(xv[j]);
     }
@@ -243,89 +305,107 @@ __device__ __forceinline__ bool row_compute(const RowPlan<T, EK> &p, const T (&p
     for (int j = 0; j < EK; j++)
         if (j < p.ne) {
             if constexpr (EXACT)
-                sum = __dadd_rn(sum, __dmul_rn(xv[j], p.a[j]));
+                sum = __dadd_rn(sum, __dmul_rn(xv[j], v.a[j]));
             else
-                sum = fmaf(xv[j], p.a[j], sum);
+                sum = fmaf(xv[j], v.a[j], sum);
         }
-    const T rhs = xs[p.sl];
+    T o;
     if constexpr (EXACT)
-        out = __ddiv_rn(__dsub_rn(rhs, sum), p.diag);
+        o = __ddiv_rn(__dsub_rn(v.rhs, sum), v.diag);
     else
-        out = (rhs - sum) * p.diag;  // FP32 value blocks hold 1/diag
+        o = (v.rhs - sum) * v.diag;  // FP32 value blocks hold 1/diag
+    if (v.sl >= 0) Sh<T>::st(io.xs + io.slot(v.sl), o);
+    if constexpr (STG) Sh<T>::st(io.rs + io.slot(p.kpos), o);
+    Sent<T>::store(xg + p.row, o);
     return true;
 }
 
-// Walk one window whose chunks all have entry stride EK (1..4). Thread t owns row t of every
-// chunk (rows beyond the block width loop, without prefetch); its next row's plan and remote
-// values are loaded before each barrier.
-template <typename T, bool EXACT, int EK>
-__device__ __forceinline__ bool walk_window_e(const int *I, const int *Iend, const T *V, T *xs, T *xg, Waiter &w,
-                                              bool alive) {
-    const int tid = threadIdx.x;
-    int nl = I[0];
-    RowPlan<T, EK> rp;
-    T pf[EK];
-    bool mine = tid < nl;
-    if (mine) {
-        load_row<T, EK>(I, V, nl, tid, rp);
-        load_remote<T, EK>(rp, xg, pf);
+// Walk one window whose chunks all have entry stride EK (1..3). At the start of step s a
+// thread issues the loads of its step-s+1 row's dependency indices; they complete while step s
+// computes, so the loads of that row's remote values (and, without staging, of its right-hand
+// side) go out before the barrier that ends step s without waiting. The rest of a row's plan is
+// loaded after the barrier, together with its dependencies' slots. Rows beyond one pass of the
+// block loop without prefetch.
+template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT, int EK>
+__device__ __forceinline__ bool walk_window_e(const int *I0, const int *Iend, const T *V0,
+                                              const WalkIO<T, RT, MR, STG> &io, Waiter &w, bool alive) {
+    const int lr = io.lane_row(), st = io.stride();
+    int nl0 = Sh<int>::ld(I0);
+    RowDeps<EK> q0, q1;
+    T pf0[EK];
+    T rhs0 = T(0), rhs1 = T(0);
+    bool m0 = lr < nl0;
+    if (m0) {
+        load_deps<EK>(I0, nl0, lr, q0);
+        load_remote<T, RT, MR, STG, EK>(q0, io, pf0);
+        if constexpr (!STG) rhs0 = load_rhs<T, RT, RL2, MR, STG>(q0.row, q0.kpos, io);
     }
     for (;;) {
-        if (alive && mine) {
-            T out;
-            if (row_compute<T, EXACT, EK>(rp, pf, xs, xg, w, out)) {
-                xs[rp.sl] = out;
-                Sent<T>::store(xg + rp.row, out);
-            } else {
-                alive = false;
-            }
+        const int *I1 = I0 + chunk_nint(nl0, EK);
+        const T *V1 = V0 + chunk_nval(nl0, EK);
+        const int nl1 = I1 < Iend ? Sh<int>::ld(I0 + 2) : 0;
+        const bool m1 = lr < nl1;
+        if (m1) load_deps<EK>(I1, nl1, lr, q1);
+        if (alive && m0) {
+            RowVals<T, EK> v;
+            load_vals<T, RT, RL2, MR, STG, EK>(I0, V0, nl0, lr, q0, io, v);
+            if constexpr (!STG) v.rhs = rhs0;
+            if (!row_compute<T, RT, MR, STG, EXACT, EK>(q0, v, pf0, io, w)) alive = false;
         }
-        for (int pos = tid + (int)blockDim.x; alive && pos < nl; pos += blockDim.x) {
-            RowPlan<T, EK> q;
+        for (int pos = lr + st; alive && pos < nl0; pos += st) {
+            RowDeps<EK> q;
+            RowVals<T, EK> v;
             T qf[EK];
-            load_row<T, EK>(I, V, nl, pos, q);
+            load_deps<EK>(I0, nl0, pos, q);
+            load_vals<T, RT, RL2, MR, STG, EK>(I0, V0, nl0, pos, q, io, v);
+            if constexpr (!STG) v.rhs = load_rhs<T, RT, RL2, MR, STG>(q.row, q.kpos, io);
 #pragma unroll
             for (int j = 0; j < EK; j++) qf[j] = Sent<T>::value();
-            T out;
-            if (!row_compute<T, EXACT, EK>(q, qf, xs, xg, w, out)) {
-                alive = false;
-                break;
-            }
-            xs[q.sl] = out;
-            Sent<T>::store(xg + q.row, out);
+            if (!row_compute<T, RT, MR, STG, EXACT, EK>(q, v, qf, io, w)) alive = false;
         }
-        const int *In = I + chunk_nint(nl, EK);
-        const T *Vn = V + chunk_nval(nl, EK);
-        const int nln = In < Iend ? In[0] : 0;
-        mine = tid < nln;
-        if (mine) {
-            load_row<T, EK>(In, Vn, nln, tid, rp);
-            if (alive) load_remote<T, EK>(rp, xg, pf);
+        if (m1 && alive) {
+            load_remote<T, RT, MR, STG, EK>(q1, io, pf0);
+            if constexpr (!STG) rhs1 = load_rhs<T, RT, RL2, MR, STG>(q1.row, q1.kpos, io);
         }
         __syncthreads();
-        if (In >= Iend) break;
-        I = In;
-        V = Vn;
-        nl = nln;
+        if (nl1 == 0) break;
+        I0 = I1;
+        V0 = V1;
+        nl0 = nl1;
+        m0 = m1;
+        q0 = q1;
+        rhs0 = rhs1;
     }
     return alive;
 }
 
-// Any entry stride (the CTA's widest row has more than 4 entries): plain loop, waits in place.
-template <typename T, bool EXACT>
-__device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, const T *V, T *xs, T *xg, Waiter &w,
-                                                bool alive) {
+// Any entry stride (the CTA's widest row has more than 3 entries): plain loop, waits in place.
+template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT>
+__device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, const T *V,
+                                                const WalkIO<T, RT, MR, STG> &io, Waiter &w, bool alive) {
+    T *xg = io.out();
     while (I < Iend) {
         const int nl = I[0], E = I[1];
-        const int *rowid = I + kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
+        const int *rowid = I + kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *kpos = ne + nl, *dep = kpos + nl;
         const T *diag = V, *val = V + nl;
-        for (int pos = threadIdx.x; alive && pos < nl; pos += blockDim.x) {
+        for (int pos = io.lane_row(); alive && pos < nl; pos += io.stride()) {
+            const int row = rowid[pos];
+            T rhs;
+            if constexpr (STG) {
+                rhs = io.rs[io.slot(kpos[pos])];
+            } else {
+                const RT *src = io.in() + row;
+                if constexpr (RL2)
+                    rhs = (T)Sent<RT>::load(src);
+                else
+                    rhs = (T)*src;
+            }
             T sum = T(0);
             for (int j = 0; j < ne[pos]; j++) {
                 const int d = dep[pos * E + j];
                 T xv;
                 if (d >= 0) {
-                    xv = xs[d];
+                    xv = io.xs[io.slot(d)];
                 } else if (!wait_value<T>(xg + (-d - 1), xv, w, -d - 1)) {
                     alive = false;
                     break;
@@ -336,14 +416,14 @@ __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, c
                     sum = fmaf(xv, val[pos * E + j], sum);
             }
             if (!alive) break;
-            const int sl = slot[pos];
-            T out;
+            T o;
             if constexpr (EXACT)
-                out = __ddiv_rn(__dsub_rn(xs[sl], sum), diag[pos]);
+                o = __ddiv_rn(__dsub_rn(rhs, sum), diag[pos]);
             else
-                out = (xs[sl] - sum) * diag[pos];
-            xs[sl] = out;
-            Sent<T>::store(xg + rowid[pos], out);
+                o = (rhs - sum) * diag[pos];
+            if (slot[pos] >= 0) io.xs[io.slot(slot[pos])] = o;
+            if constexpr (STG) io.rs[io.slot(kpos[pos])] = o;
+            Sent<T>::store(xg + row, o);
         }
         I += chunk_nint(nl, E);
         V += chunk_nval(nl, E);
@@ -355,70 +435,24 @@ __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, c
 // Walk one window (nint ints of chunk blocks, then their values) held in shared memory. All
 // chunks of a CTA share one entry stride. Every thread passes every barrier, also after a
 // failed wait, so the CTA never splits.
-template <typename T, bool EXACT>
-__device__ __forceinline__ bool walk_window(const unsigned char *b, int nint, T *xs, T *xg, Waiter &w, bool alive) {
+template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT>
+__device__ __forceinline__ bool walk_window(const unsigned char *b, int nint, const WalkIO<T, RT, MR, STG> &io,
+                                            Waiter &w, bool alive) {
     const int *I = reinterpret_cast<const int *>(b);
     const int *Iend = I + nint;
     const T *V = reinterpret_cast<const T *>(b + (size_t)nint * 4);
     switch (I[1]) {
-        case 1: return walk_window_e<T, EXACT, 1>(I, Iend, V, xs, xg, w, alive);
-        case 2: return walk_window_e<T, EXACT, 2>(I, Iend, V, xs, xg, w, alive);
-        case 3: return walk_window_e<T, EXACT, 3>(I, Iend, V, xs, xg, w, alive);
-        case 4: return walk_window_e<T, EXACT, 4>(I, Iend, V, xs, xg, w, alive);
-        default: return walk_window_any<T, EXACT>(I, Iend, V, xs, xg, w, alive);
+        case 1: return walk_window_e<T, RT, RL2, MR, STG, EXACT, 1>(I, Iend, V, io, w, alive);
+        case 2: return walk_window_e<T, RT, RL2, MR, STG, EXACT, 2>(I, Iend, V, io, w, alive);
+        case 3: return walk_window_e<T, RT, RL2, MR, STG, EXACT, 3>(I, Iend, V, io, w, alive);
+        default: return walk_window_any<T, RT, RL2, MR, STG, EXACT>(I, Iend, V, io, w, alive);
     }
-}
-
-// Multi-right-hand-side walk (R <= kMaxRhs, runtime): slots hold R values per row
-// (xs[slot*R + r]); right-hand side r of row `row` lives at xg[r*ldx + row]. FP64, exact.
-__device__ __forceinline__ bool walk_window_multi(const unsigned char *b, int nint, double *xs, double *xg, int ldx, int R,
-                                                  Waiter &w, bool alive) {
-    const int *I = reinterpret_cast<const int *>(b);
-    const int *Iend = I + nint;
-    const double *V = reinterpret_cast<const double *>(b + (size_t)nint * 4);
-    while (I < Iend) {
-        const int nl = I[0], E = I[1];
-        const int *rowid = I + kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *dep = ne + nl;
-        const double *diag = V, *val = V + nl;
-        for (int pos = threadIdx.x; pos < nl && alive; pos += blockDim.x) {
-            double sum[kMaxRhs];
-#pragma unroll
-            for (int r = 0; r < kMaxRhs; r++) sum[r] = 0.0;
-            const int n_ = ne[pos];
-            for (int j = 0; j < n_ && alive; j++) {
-                const int d = dep[pos * E + j];
-                const double a = val[pos * E + j];
-#pragma unroll
-                for (int r = 0; r < kMaxRhs; r++)
-                    if (r < R) {
-                        double xv = 0.0;
-                        if (d >= 0)
-                            xv = xs[d * R + r];
-                        else if (alive && !wait_value<double>(xg + (size_t)r * ldx + (-d - 1), xv, w, -d - 1))
-                            alive = false;
-                        sum[r] = __dadd_rn(sum[r], __dmul_rn(xv, a));
-                    }
-            }
-            if (!alive) break;
-            const int sl = slot[pos], row = rowid[pos];
-#pragma unroll
-            for (int r = 0; r < kMaxRhs; r++)
-                if (r < R) {
-                    const double out = __ddiv_rn(__dsub_rn(xs[sl * R + r], sum[r]), diag[pos]);
-                    xs[sl * R + r] = out;
-                    Sent<double>::store(xg + (size_t)r * ldx + row, out);
-                }
-        }
-        I += chunk_nint(nl, E);
-        V += chunk_nval(nl, E);
-        __syncthreads();
-    }
-    return alive;
 }
 
 // Standalone FP64 sweep of the caller's triangular CSR (values gathered through vsrcT into the
-// packed scratch gv), right-hand sides R at a time. d = 0: lower (L), 1: upper (U = L^T).
-template <bool MULTI>
+// packed scratch gv), right-hand sides R at a time (MR: R > 1; STG: staged in shared memory).
+// d = 0: lower (L), 1: upper (U = L^T).
+template <bool MR, bool STG>
 __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, int d, const double *__restrict__ tval,
                                                                  double *gv, const double *__restrict__ b, int ldb,
                                                                  double *x, int ldx, int nrhs, int R, DevStatus *st,
@@ -440,16 +474,24 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, 
         ws.init(pl, d, false, gv, gv, smem, (unsigned int)(npass * (__ldg(D.swptr + c + 1) - __ldg(D.swptr + c))));
     }
     trace_mark(trace, 1);
-    double *xs = reinterpret_cast<double *>(smem);
     const int s0 = __ldg(pl.soff + c), nl = __ldg(pl.soff + c + 1) - s0;
-    const int *srow = pl.srow + s0;
     for (int r0 = 0; r0 < nrhs; r0 += R) {
-        const int Rb = min(R, nrhs - r0);
-        for (int k = threadIdx.x; k < nl * Rb; k += blockDim.x) {
-            const int sl = k / Rb, r = k - sl * Rb;
-            xs[k] = __ldg(b + (size_t)(r0 + r) * ldb + __ldg(srow + sl));
+        WalkIO<double, double, MR, STG> io;
+        io.xs = reinterpret_cast<double *>(smem);
+        io.rs = reinterpret_cast<double *>(smem + pl.xs_bytes);
+        io.xg = x + (size_t)r0 * ldx;
+        io.rhs = b + (size_t)r0 * ldb;
+        io.ldx = ldx;
+        io.ldr = ldb;
+        io.R_ = min(R, nrhs - r0);
+        if constexpr (STG) {
+            const int Rb = io.R();
+            for (int k = threadIdx.x; k < nl * Rb; k += blockDim.x) {
+                const int kk = k / Rb, r = k - kk * Rb;
+                io.rs[k] = __ldg(b + (size_t)(r0 + r) * ldb + __ldg(pl.srow + s0 + kk));
+            }
+            __syncthreads();
         }
-        __syncthreads();
         trace_mark(trace, 2 + 2 * (r0 / R));
         bool alive = true;
         for (int i = 0; i < ws.total(); i++) {
@@ -459,10 +501,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, 
                 ws.drain(spin);
                 return;
             }
-            if (MULTI)
-                alive = walk_window_multi(buf, nint, xs, x + (size_t)r0 * ldx, ldx, Rb, w, alive);
-            else
-                alive = walk_window<double, true>(buf, nint, xs, x + (size_t)r0 * ldx, w, alive);
+            alive = walk_window<double, double, false, MR, STG, true>(buf, nint, io, w, alive);
             ws.release(i);
             if (__syncthreads_or(!alive)) {
                 ws.drain(spin);
@@ -508,31 +547,43 @@ struct IccgArgs {
     double *grad_a;    // if set: grad_a[e] = -x_i * xf_j for each entry e = (i, j) of A
 };
 
-// z = U^-1 L^-1 r on this CTA's rows; p = z if set_p; adds this thread's share of r.z to rz
-// (a pass over the CTA's slots after the upper walk, which leaves z in them).
-template <typename T>
-__device__ bool chunk_precond(const IccgArgs &A, WinStream<T> &ws, T *xs, bool set_p, double &rz, Waiter &w) {
+// z = U^-1 L^-1 r on this CTA's rows; p = z if set_p; adds this thread's share of r.z to rz in
+// a pass over the CTA's rows afterwards. STG: r is staged in shared memory, the lower walk
+// leaves y there for the upper walk, which leaves z there for the r.z pass; else the right-hand
+// sides come from r and from y (in L2) and z is read back from L2.
+template <typename T, bool STG>
+__device__ __forceinline__ bool chunk_precond(const IccgArgs &A, WinStream<T> &ws, unsigned char *smem, bool set_p, double &rz,
+                              Waiter &w) {
     const int c = blockIdx.x;
     T *yg = sizeof(T) == 8 ? (T *)A.y : (T *)A.y32;
     T *zg = sizeof(T) == 8 ? (T *)A.z : (T *)A.z32;
+    T *xs = reinterpret_cast<T *>(smem);
+    T *rs = reinterpret_cast<T *>(smem + A.pl.xs_bytes);
     const int s0 = __ldg(A.pl.soff + c), nl = __ldg(A.pl.soff + c + 1) - s0;
-    for (int k = threadIdx.x; k < nl; k += blockDim.x) xs[k] = (T)A.r[__ldg(A.pl.srow + s0 + k)];
-    __syncthreads();
+    if constexpr (STG) {
+        for (int k = threadIdx.x; k < nl; k += blockDim.x) rs[k] = (T)A.r[__ldg(A.pl.srow + s0 + k)];
+        __syncthreads();
+    }
     bool alive = true;
     trace_mark(A.trace, 56);
     for (int i = 0; i < ws.total(); i++) {
         const unsigned char *buf;
         int nint;
         if (!ws.acquire(i, A.spin_limit, A.st, buf, nint)) return false;
-        const bool lower = i < ws.ctl->n0;
-        alive = walk_window<T, sizeof(T) == 8>(buf, nint, xs, lower ? yg : zg, w, alive);
-        if (lower && i == ws.ctl->n0 - 1) trace_mark(A.trace, 57);
+        if (i < ws.ctl->n0) {
+            const WalkIO<T, double, false, STG> lo{xs, yg, A.r, rs, 0, 0, 1};
+            alive = walk_window<T, double, false, false, STG, sizeof(T) == 8>(buf, nint, lo, w, alive);
+            if (i == ws.ctl->n0 - 1) trace_mark(A.trace, 57);
+        } else {
+            const WalkIO<T, T, false, STG> up{xs, zg, yg, rs, 0, 0, 1};
+            alive = walk_window<T, T, true, false, STG, sizeof(T) == 8>(buf, nint, up, w, alive);
+        }
         ws.release(i);
         if (__syncthreads_or(!alive)) return false;
     }
     for (int k = threadIdx.x; k < nl; k += blockDim.x) {
         const int row = __ldg(A.pl.srow + s0 + k);
-        const double zd = (double)xs[k];
+        const double zd = STG ? (double)rs[k] : (double)Sent<T>::load(zg + row);
         rz = __dadd_rn(rz, __dmul_rn(A.r[row], zd));
         if (set_p) A.p[row] = zd;
     }
@@ -540,9 +591,25 @@ __device__ bool chunk_precond(const IccgArgs &A, WinStream<T> &ws, T *xs, bool s
     return true;
 }
 
-// T = double: FP64 factors; T = float: FP32 factors (one instantiation each keeps the register
-// budget of each variant to one precision).
+// This CTA's value slots of one direction from the IC0 factor lu (FP32: the diagonal as its
+// reciprocal).
 template <typename T>
+__device__ __forceinline__ void pack_factor(const ChunkDir &D, const double *lu, double *g64, float *g32) {
+    const int vb = __ldg(D.cval + blockIdx.x), ve = __ldg(D.cval + blockIdx.x + 1);
+    for (int i = vb + (int)threadIdx.x; i < ve; i += blockDim.x) {
+        const int s = __ldg(D.vsrcA + i);
+        const double v = s >= 0 ? ld_l2(lu + s) : (s <= -2 ? ld_l2(lu + (-2 - s)) : 0.0);
+        if constexpr (sizeof(T) == 4)
+            g32[i] = s <= -2 ? __frcp_rn(__double2float_rn(v)) : __double2float_rn(v);
+        else
+            g64[i] = v;
+    }
+}
+
+// T = double: FP64 factors; T = float: FP32 factors. STG: the right-hand sides of the sweeps are
+// staged in shared memory (when they fit). One instantiation per combination keeps each one's
+// register budget to what it uses.
+template <typename T, bool STG>
 __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     constexpr bool kMixed = sizeof(T) == 4;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -554,7 +621,6 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     WinStream<T> ws;
     ws.init(A.pl, 0, true, kMixed ? (const T *)A.gv32[0] : (const T *)A.gv64[0],
             kMixed ? (const T *)A.gv32[1] : (const T *)A.gv64[1], smem, 0xFFFFFFFFu);
-    T *xs = reinterpret_cast<T *>(smem);
 #define BAAS_BARRIER()                                            \
     do {                                                          \
         if (!grid_barrier(A.bar, nb, A.st, A.spin_limit)) {       \
@@ -576,18 +642,8 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
 
         // pack this CTA's value slots of L and U = L^T (IC0_preconditioner split,
         // test/iccg_level_merge.cpp:874-891)
-        for (int d = 0; d < 2; d++) {
-            const ChunkDir &D = A.pl.dir[d];
-            const int vb = __ldg(D.cval + blockIdx.x), ve = __ldg(D.cval + blockIdx.x + 1);
-            for (int i = vb + (int)threadIdx.x; i < ve; i += blockDim.x) {
-                const int s = __ldg(D.vsrcA + i);
-                const double v = s >= 0 ? ld_l2(A.lu + s) : (s <= -2 ? ld_l2(A.lu + (-2 - s)) : 0.0);
-                if constexpr (kMixed)
-                    A.gv32[d][i] = s <= -2 ? __frcp_rn(__double2float_rn(v)) : __double2float_rn(v);
-                else
-                    A.gv64[d][i] = v;
-            }
-        }
+        pack_factor<T>(A.pl.dir[0], A.lu, A.gv64[0], A.gv32[0]);
+        pack_factor<T>(A.pl.dir[1], A.lu, A.gv64[1], A.gv32[1]);
         fence_async_global();
     }
     // r = b - A x; sentinels
@@ -613,7 +669,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     trace_mark(A.trace, 3);
 
     double rzl = 0.0;
-    if (!chunk_precond<T>(A, ws, xs, true, rzl, w)) {
+    if (!chunk_precond<T, STG>(A, ws, smem, true, rzl, w)) {
         ws.drain(A.spin_limit);
         return;
     }
@@ -663,7 +719,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
         if (rel < A.tol) break;
 
         rzl = 0.0;
-        if (!chunk_precond<T>(A, ws, xs, false, rzl, w)) {
+        if (!chunk_precond<T, STG>(A, ws, smem, false, rzl, w)) {
             ws.drain(A.spin_limit);
             return;
         }

@@ -322,7 +322,7 @@ def gpu_arm(args):
             "gpu_launches": int(args.steps),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "traffic": traffic,
-                         "peak_kind": peak_kind, "kernel": "k_iccg_staged<double>",
+                         "peak_kind": peak_kind, "kernel": "k_iccg_chunked<double>",
                          "algorithmic_bytes_per_launch": int(launch_bytes)},
             "cpu_baseline": cpu,
             "clocks": clocks,

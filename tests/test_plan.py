@@ -80,4 +80,16 @@ def test_plan_rejects_tiny_budget():
     Lo, _ = _ic_lu(A)
     s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
     with pytest.raises(BaasError):
-        s.emulate_sweep(Lo, np.zeros(A.n), parts=1, smem_budget=64 * 1024)
+        s.emulate_sweep(Lo, np.zeros(A.n), parts=1, smem_budget=2048)
+
+
+def test_liveness_slots_let_one_cta_stream_a_large_plan():
+    """Slots live only until a row's last local reader, so one CTA holding all 8,000 rows (one
+    slot per row would need 64 KB for the slots alone) fits a 40 KB budget and streams its plan in windows."""
+    A = gen.laplace3d(20, 1e-3)
+    Lo, Up = _ic_lu(A)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    r = gen.uniform_rhs(A.n, 1)
+    assert np.array_equal(s.emulate_sweep(Lo, r, parts=1, smem_budget=40 * 1024), Port.lower_solve(Lo, r))
+    assert np.array_equal(s.emulate_sweep(Up, r, upper=True, parts=1, smem_budget=40 * 1024),
+                          Port.upper_solve(Up, r, descending=True))
