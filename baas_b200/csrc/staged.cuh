@@ -269,11 +269,19 @@ __device__ __forceinline__ T load_rhs(int row, int kpos, const WalkIO<T, RT, MR,
 
 // Loads of the row's remote dependencies (their values, or the sentinel if not yet written);
 // issued before a barrier, they complete while the CTA waits at it.
+// One branch per row: a row with no remote dependency (most rows) issues nothing; a row with one
+// loads every entry, pointing its local ones at its own (unused) result slot, so no entry needs
+// a branch of its own.
 template <typename T, typename RT, bool MR, bool STG, int EK>
 __device__ __forceinline__ void load_remote(const RowDeps<EK> &p, const WalkIO<T, RT, MR, STG> &io, T (&pf)[EK]) {
     const T *xg = io.out();
+    bool rem = false;
 #pragma unroll
-    for (int j = 0; j < EK; j++) pf[j] = (j < p.ne && p.d[j] < 0) ? Sent<T>::load(xg + (-p.d[j] - 1)) : T(0);
+    for (int j = 0; j < EK; j++) rem |= j < p.ne && p.d[j] < 0;
+    if (rem) {
+#pragma unroll
+        for (int j = 0; j < EK; j++) pf[j] = Sent<T>::load(xg + ((j < p.ne && p.d[j] < 0) ? -p.d[j] - 1 : p.row));
+    }
 }
 
 // One row: dependency values gathered without branches (local slot, or the prefetched remote
@@ -292,7 +300,7 @@ __device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<
         const int dj = p.d[j];
         const T loc = Sh<T>::ld(io.xs + io.slot(dj >= 0 ? dj : 0));
         xv[j] = dj >= 0 ? loc : pf[j];
-        miss |= j < p.ne && Sent<T>::is(xv[j]);
+        miss |= j < p.ne && dj < 0 && Sent<T>::is(pf[j]);
     }
     if (miss) {
 #pragma unroll
