@@ -123,6 +123,17 @@ class Schedule:
         """Test hook: the next forward sweep waits on a value nothing writes (BAAS_ERR_TIMEOUT)."""
         _native.check(_native.lib().baas_test_inject_unsatisfiable_wait(self._h, row), "inject")
 
+    def replan(self, parts: int = 0, smem_budget: int = 0, partition: int = 0, spin_limit: int = 0) -> None:
+        """Rebuild the device plan with other execution options (baas_replan), keeping the analysis."""
+        opt = _native.BaasOptions()
+        _native.lib().baas_options_default(C.byref(opt))
+        opt.nthread = self.nthread
+        opt.parts = parts
+        opt.smem_budget = smem_budget
+        opt.partition = partition
+        opt.spin_limit = spin_limit
+        _native.check(_native.lib().baas_replan(self._h, C.byref(opt)), "baas_replan")
+
     def emulate_sweep(self, T: CSR, b: np.ndarray, upper: bool = False, parts: int = 0,
                       smem_budget: int = 0) -> np.ndarray:
         """Test hook: run the chunked sweep plan on the host (no GPU) and return x."""
@@ -198,3 +209,65 @@ class Schedule:
             return it.value, rr.value
         _native.check(st, "baas_iccg_adjoint")
         return it.value, rr.value
+
+
+def batch_concat(systems) -> tuple[CSR, np.ndarray]:
+    """The block-diagonal concatenation of CSR systems and their row offsets (baas_batch_concat)."""
+    ns = len(systems)
+    arrs = [(np.ascontiguousarray(m.rowptr, dtype=np.int32), np.ascontiguousarray(m.colidx, dtype=np.int32),
+             np.ascontiguousarray(m.values, dtype=np.float64)) for m in systems]
+    cs = (_native.BaasCsr * ns)(*[_native.BaasCsr(m.n, int(a[0][-1]), _ptr(a[0]), _ptr(a[1]), _ptr(a[2]))
+                                  for m, a in zip(systems, arrs)])
+    ptrs = (C.POINTER(_native.BaasCsr) * ns)(*[C.pointer(cs[k]) for k in range(ns)])
+    L = _native.lib()
+    nnz = L.baas_batch_concat(ns, ptrs, None, None, None, None)
+    if nnz < 0:
+        raise ValueError("bad systems")
+    n = sum(m.n for m in systems)
+    rowptr = np.zeros(n + 1, dtype=np.int32)
+    colidx = np.zeros(nnz, dtype=np.int32)
+    values = np.zeros(nnz, dtype=np.float64)
+    off = np.zeros(ns + 1, dtype=np.int32)
+    L.baas_batch_concat(ns, ptrs, _ptr(rowptr), _ptr(colidx), _ptr(values), _ptr(off))
+    return CSR(n, rowptr, colidx, values), off
+
+
+class BatchSchedule(Schedule):
+    """One ICCG schedule for a batch of independent SPD systems (block-diagonal concatenation)."""
+
+    def __init__(self, systems, nthread: int = 8, spin_limit: int = 0, parts: int = 0, smem_budget: int = 0):
+        A, off = batch_concat(systems)
+        self.combined = A
+        self.sys_off = off
+        self.nsys = len(systems)
+        L = _native.lib()
+        self._rowptr, self._colidx = A.rowptr, A.colidx
+        c = _native.BaasCsr(A.n, A.nnz, _ptr(A.rowptr), _ptr(A.colidx), None)
+        opt = _native.BaasOptions()
+        L.baas_options_default(C.byref(opt))
+        opt.nthread = nthread
+        opt.spin_limit = spin_limit
+        opt.parts = parts
+        opt.smem_budget = smem_budget
+        h = C.c_void_p()
+        _native.check(L.baas_analyze_batch(C.byref(c), _ptr(off), self.nsys, C.byref(opt), C.byref(h)),
+                      "baas_analyze_batch")
+        self._h = h
+        self.n = A.n
+        self.nnz = A.nnz
+        self.kind = KERNEL_ICCG
+        self.nthread = nthread
+
+    def iccg_batched(self, A: DeviceCSR, B, X, tol: float = 1e-10, maxiter: int = 2000,
+                     precision: int = PREC_FP64, stream=None, raise_on_nonconvergence: bool = True):
+        """B, X: (nrhs, n) CUDA float64 tensors (row r = right-hand side r). Returns per-instance
+        iterations and relative residuals as (nsys, nrhs) arrays."""
+        nrhs = int(B.shape[0]) if B.dim() == 2 else 1
+        it = np.zeros(self.nsys * nrhs, dtype=np.int32)
+        rr = np.zeros(self.nsys * nrhs, dtype=np.float64)
+        c = A.c()
+        st = _native.lib().baas_iccg_batched(self._h, C.byref(c), _ptr(B), _ptr(X), nrhs, self.n, tol, maxiter,
+                                             precision, _ptr(it), _ptr(rr), _stream_ptr(stream))
+        if not (st == 5 and not raise_on_nonconvergence):
+            _native.check(st, "baas_iccg_batched")
+        return it.reshape(self.nsys, nrhs), rr.reshape(self.nsys, nrhs)

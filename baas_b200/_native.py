@@ -38,7 +38,7 @@ FIELDS = {
 EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
-    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint",
+    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan",
 ]
 
 
@@ -101,6 +101,14 @@ def lib():
     L.baas_iccg_adjoint.argtypes = [vp, C.POINTER(BaasCsr), vp, vp, vp, vp, d, i, i, C.POINTER(C.c_int),
                                     C.POINTER(C.c_double), vp]
     L.baas_iccg_adjoint.restype = i
+    L.baas_replan.argtypes = [vp, C.POINTER(BaasOptions)]
+    L.baas_replan.restype = i
+    L.baas_batch_concat.argtypes = [i, vp, vp, vp, vp, vp]
+    L.baas_batch_concat.restype = i
+    L.baas_analyze_batch.argtypes = [C.POINTER(BaasCsr), vp, i, C.POINTER(BaasOptions), C.POINTER(vp)]
+    L.baas_analyze_batch.restype = i
+    L.baas_iccg_batched.argtypes = [vp, C.POINTER(BaasCsr), vp, vp, i, i, d, i, i, vp, vp, vp]
+    L.baas_iccg_batched.restype = i
     L.baas_test_emulate_sweep.argtypes = [vp, i, i, i, vp, vp, vp]
     L.baas_test_emulate_sweep.restype = i
     _lib = L

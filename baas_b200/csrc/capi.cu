@@ -21,6 +21,7 @@
 #include "../../include/baas_b200.h"
 #include "kernels.cuh"
 #include "part_kernels.cuh"
+#include "batched.cuh"
 #include "staged.cuh"
 #include "schedule.hpp"
 
@@ -213,6 +214,21 @@ struct baas_schedule {
     double *d_relres = nullptr;
 
     unsigned long long *d_trace = nullptr;  // BAAS_TRACE=1: phase timestamps of the last launch
+
+    // batched systems (baas_analyze_batch): row offsets of the systems, and the vector-phase
+    // decomposition (built at the first batched solve)
+    std::vector<int> sys_off;
+    int nsys = 0, maxls = 0;
+    int *d_sys_off = nullptr, *d_vlo = nullptr, *d_sys_lo = nullptr, *d_nls = nullptr, *d_cta_lo = nullptr,
+        *d_cta_hi = nullptr;
+    int batch_R = 0;  // right-hand sides the batched workspace is sized for
+    double *d_br = nullptr, *d_bp = nullptr, *d_bAp = nullptr, *d_by = nullptr, *d_bz = nullptr, *d_bpart = nullptr,
+           *d_brelres = nullptr, *d_blu = nullptr;
+    float *d_by32 = nullptr, *d_bz32 = nullptr;
+    double *d_bgv64[2] = {nullptr, nullptr};
+    float *d_bgv32[2] = {nullptr, nullptr};
+    int *d_biters = nullptr;
+    unsigned int *d_active = nullptr;
 
     unsigned int spin() const { return opt.spin_limit > 0 ? (unsigned int)opt.spin_limit : kDefaultSpin; }
 };
@@ -590,6 +606,9 @@ baas::ChunkPlan chunk_plan(const baas_schedule *s, const WinCfg &w) {
 }
 
 constexpr int kMaxSmemBudget = 224 * 1024;
+// dynamic shared memory a kernel may request: B200's 227 KB per block less room for the
+// kernels' static shared memory
+constexpr int kMaxDynSmem = 227 * 1024 - 2048;
 
 baas_status ensure_device(baas_schedule *s) {
     int dev = 0;
@@ -637,9 +656,11 @@ baas_status ensure_device(baas_schedule *s) {
         const void *kerns[] = {(const void *)baas::k_sweep_chunked<false, false>, (const void *)baas::k_sweep_chunked<false, true>,
                                (const void *)baas::k_sweep_chunked<true, false>, (const void *)baas::k_sweep_chunked<true, true>,
                                (const void *)baas::k_iccg_chunked<double, false>, (const void *)baas::k_iccg_chunked<double, true>,
-                               (const void *)baas::k_iccg_chunked<float, false>, (const void *)baas::k_iccg_chunked<float, true>};
+                               (const void *)baas::k_iccg_chunked<float, false>, (const void *)baas::k_iccg_chunked<float, true>,
+                               (const void *)baas::k_iccg_batched<double, false>, (const void *)baas::k_iccg_batched<double, true>,
+                               (const void *)baas::k_iccg_batched<float, false>, (const void *)baas::k_iccg_batched<float, true>};
         for (const void *k : kerns)
-            BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemBudget));
+            BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
     }
     s->uploaded = true;
     // the single-right-hand-side FP64 windows must exist for every kind of call
@@ -979,8 +1000,9 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
     return BAAS_OK;
 }
 
-void baas_destroy(baas_schedule *s) {
-    if (!s) return;
+// Frees the schedule's device state (plan, workspaces) on its device and returns the schedule to
+// its state right after analysis; the host schedule and the batch offsets stay.
+static void release_device(baas_schedule *s) {
     if (s->uploaded) {
         int cur = -1;
         cudaGetDevice(&cur);
@@ -1000,9 +1022,43 @@ void baas_destroy(baas_schedule *s) {
             if (p) cudaFree(p);
         if (s->h_status) cudaFreeHost(s->h_status);
         if (s->d_trace) cudaFree(s->d_trace);
+        void *bptrs[] = {s->d_sys_off, s->d_vlo, s->d_sys_lo, s->d_nls, s->d_cta_lo, s->d_cta_hi, s->d_br, s->d_bp,
+                         s->d_bAp, s->d_by, s->d_bz, s->d_bpart, s->d_brelres, s->d_blu, s->d_by32, s->d_bz32,
+                         s->d_bgv64[0], s->d_bgv64[1], s->d_bgv32[0], s->d_bgv32[1], s->d_biters, s->d_active};
+        for (void *p : bptrs)
+            if (p) cudaFree(p);
         if (cur >= 0 && cur != s->device) cudaSetDevice(cur);
     }
+    baas_schedule fresh;
+    fresh.hs = std::move(s->hs);
+    fresh.opt = s->opt;
+    fresh.nnz_a = s->nnz_a;
+    fresh.nnz_l = s->nnz_l;
+    fresh.f_ord = std::move(s->f_ord);
+    fresh.cptr = std::move(s->cptr);
+    fresh.crow = std::move(s->crow);
+    fresh.cpos = std::move(s->cpos);
+    fresh.fault_row = s->fault_row;
+    fresh.sys_off = std::move(s->sys_off);
+    fresh.nsys = s->nsys;
+    *s = std::move(fresh);
+}
+
+void baas_destroy(baas_schedule *s) {
+    if (!s) return;
+    release_device(s);
     delete s;
+}
+
+baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
+    if (!s || !opt) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    if (opt->nthread != s->hs.nthread) return fail(BAAS_ERR_BAD_ARG, "nthread is fixed by the analysis");
+    if (opt->parts < 0 || opt->smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "parts and smem_budget must be >= 0");
+    if (opt->partition != BAAS_PARTITION_RANGES && opt->partition != BAAS_PARTITION_BAAS_THREADS)
+        return fail(BAAS_ERR_BAD_ARG, "unknown partition");
+    release_device(s);
+    s->opt = *opt;
+    return BAAS_OK;
 }
 
 baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const double *b, double *x, int nrhs, int ldb,
@@ -1098,6 +1154,189 @@ baas_status baas_ic0_noalloc(baas_schedule *s, const baas_csr *A, double *lu, vo
     if (hs.code == baas::kTimeout) return fail(BAAS_ERR_TIMEOUT, "a device wait ran out (at " + std::to_string(hs.where) + ")");
     if (hs.code != 0) return fail(BAAS_ERR_CUDA, "device status " + std::to_string(hs.code));
     if (hs.zero_pivots > 0) return fail(BAAS_ERR_ZERO_PIVOT, std::to_string(hs.zero_pivots) + " non-positive pivot(s)");
+    return BAAS_OK;
+}
+
+
+// ---------------------------------------------------------------------------------------
+// Batched systems (no counterpart in the reference).
+// ---------------------------------------------------------------------------------------
+int baas_batch_concat(int nsys, const baas_csr *const *sys, int *rowptr, int *colidx, double *values, int *sys_off) {
+    if (nsys < 1 || !sys) return -1;
+    long long n = 0, nnz = 0;
+    for (int k = 0; k < nsys; k++) {
+        if (!sys[k] || !sys[k]->rowptr || sys[k]->n <= 0) return -1;
+        n += sys[k]->n;
+        nnz += sys[k]->rowptr[sys[k]->n];
+    }
+    if (n > INT_MAX || nnz > INT_MAX) return -1;
+    if (!rowptr || !colidx || !sys_off) return (int)nnz;
+    int ro = 0, eo = 0;
+    rowptr[0] = 0;
+    sys_off[0] = 0;
+    for (int k = 0; k < nsys; k++) {
+        const baas_csr &m = *sys[k];
+        for (int i = 0; i < m.n; i++) {
+            for (int e = m.rowptr[i]; e < m.rowptr[i + 1]; e++) {
+                colidx[eo] = m.colidx[e] + ro;
+                if (values && m.values) values[eo] = m.values[e];
+                eo++;
+            }
+            rowptr[ro + i + 1] = eo;
+        }
+        ro += m.n;
+        sys_off[k + 1] = ro;
+    }
+    return (int)nnz;
+}
+
+baas_status baas_analyze_batch(const baas_csr *A, const int *sys_off, int nsys, const baas_options *opt,
+                               baas_schedule **out) {
+    if (!A || !sys_off || !out || nsys < 1) return fail(BAAS_ERR_BAD_ARG, "NULL argument or no systems");
+    if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
+    if (sys_off[0] != 0 || sys_off[nsys] != A->n) return fail(BAAS_ERR_BAD_ARG, "system offsets must run from 0 to n");
+    for (int k = 0; k < nsys; k++) {
+        if (sys_off[k + 1] <= sys_off[k]) return fail(BAAS_ERR_BAD_ARG, "every system needs at least one row");
+        for (int i = sys_off[k]; i < sys_off[k + 1]; i++)
+            for (int e = A->rowptr[i]; e < A->rowptr[i + 1]; e++)
+                if (A->colidx[e] < sys_off[k] || A->colidx[e] >= sys_off[k + 1])
+                    return fail(BAAS_ERR_BAD_ARG, "an entry couples two systems (the pattern must be block diagonal)");
+    }
+    BAAS_TRY(baas_analyze(A, BAAS_KERNEL_ICCG, opt, out));
+    (*out)->sys_off.assign(sys_off, sys_off + nsys + 1);
+    (*out)->nsys = nsys;
+    return BAAS_OK;
+}
+
+static baas_status batch_setup(baas_schedule *s, int R) {
+    const int n = s->hs.n, P = s->P, ns = s->nsys;
+    if (!s->d_sys_off) {
+        std::vector<int> vlo(P + 1), sys_lo(P), nls(P), cta_lo(ns, P), cta_hi(ns, -1);
+        for (int c = 0; c <= P; c++) vlo[c] = (int)(((long long)n * c) / P);
+        int maxls = 1;
+        for (int c = 0; c < P; c++) {
+            int k = 0;
+            while (k + 1 < ns && s->sys_off[k + 1] <= vlo[c]) k++;
+            sys_lo[c] = k;
+            int cnt = 0;
+            for (int q = k; q < ns && s->sys_off[q] < vlo[c + 1]; q++)
+                if (s->sys_off[q + 1] > vlo[c]) {
+                    cnt++;
+                    cta_lo[q] = std::min(cta_lo[q], c);
+                    cta_hi[q] = std::max(cta_hi[q], c);
+                }
+            nls[c] = vlo[c + 1] > vlo[c] ? cnt : 0;
+            maxls = std::max(maxls, nls[c]);
+        }
+        for (int q = 0; q < ns; q++)
+            if (cta_hi[q] < 0) return fail(BAAS_ERR_BAD_ARG, "a system has no rows");
+        s->maxls = maxls;
+        BAAS_TRY(upload(s->d_sys_off, s->sys_off));
+        BAAS_TRY(upload(s->d_vlo, vlo));
+        BAAS_TRY(upload(s->d_sys_lo, sys_lo));
+        BAAS_TRY(upload(s->d_nls, nls));
+        BAAS_TRY(upload(s->d_cta_lo, cta_lo));
+        BAAS_TRY(upload(s->d_cta_hi, cta_hi));
+        BAAS_TRY(dalloc(s->d_active, 1));
+        BAAS_TRY(dalloc(s->d_blu, (size_t)s->nnz_a));
+        for (int d = 0; d < 2; d++) {
+            BAAS_TRY(dalloc(s->d_bgv64[d], s->chk.dir[d].vsrcA.size()));
+            BAAS_TRY(dalloc(s->d_bgv32[d], s->chk.dir[d].vsrcA.size()));
+        }
+    }
+    if (s->batch_R < R) {
+        double *dp[] = {s->d_br, s->d_bp, s->d_bAp, s->d_by, s->d_bz, s->d_bpart, s->d_brelres};
+        for (double *p : dp)
+            if (p) cudaFree(p);
+        if (s->d_by32) cudaFree(s->d_by32);
+        if (s->d_bz32) cudaFree(s->d_bz32);
+        if (s->d_biters) cudaFree(s->d_biters);
+        const size_t nr = (size_t)n * R;
+        BAAS_TRY(dalloc(s->d_br, nr));
+        BAAS_TRY(dalloc(s->d_bp, nr));
+        BAAS_TRY(dalloc(s->d_bAp, nr));
+        BAAS_TRY(dalloc(s->d_by, nr));
+        BAAS_TRY(dalloc(s->d_bz, nr));
+        BAAS_TRY(dalloc(s->d_by32, nr));
+        BAAS_TRY(dalloc(s->d_bz32, nr));
+        BAAS_TRY(dalloc(s->d_bpart, (size_t)2 * P * s->maxls * R));
+        BAAS_TRY(dalloc(s->d_biters, (size_t)ns * R));
+        BAAS_TRY(dalloc(s->d_brelres, (size_t)ns * R));
+        s->batch_R = R;
+    }
+    return BAAS_OK;
+}
+
+baas_status baas_iccg_batched(baas_schedule *s, const baas_csr *A, const double *B, double *X, int nrhs, int ldb,
+                              double tol, int maxiter, int precision, int *iters, double *relres, void *stream_) {
+    if (!s || !B || !X || !iters || !relres) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    if (s->nsys < 1) return fail(BAAS_ERR_STATE, "the schedule was not made by baas_analyze_batch");
+    if (!csr_ok(A, s->hs.n, s->nnz_a)) return fail(BAAS_ERR_BAD_ARG, "matrix does not match the analysed pattern");
+    const int n = s->hs.n;
+    if (nrhs < 1 || nrhs > baas::kMaxRhs || ldb < n) return fail(BAAS_ERR_BAD_ARG, "nrhs must be 1..8 and ldb >= n");
+    if (maxiter < 0 || !(tol >= 0.0)) return fail(BAAS_ERR_BAD_ARG, "maxiter must be >= 0 and tol >= 0");
+    if (precision != BAAS_PREC_FP64 && precision != BAAS_PREC_FP32_FACTORS) return fail(BAAS_ERR_BAD_ARG, "unknown precision");
+    BAAS_TRY(ensure_device(s));
+    const bool mixed = precision == BAAS_PREC_FP32_FACTORS;
+    WinCfg *w = nullptr;
+    BAAS_TRY(get_windows(s, mixed ? 4 : 8, nrhs, &w));
+    BAAS_TRY(batch_setup(s, nrhs));
+    cudaStream_t stream = (cudaStream_t)stream_;
+    const int P = s->P;
+    BAAS_TRY(next_epoch(s, stream));
+    BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+    BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
+    const unsigned int active = (unsigned int)(s->nsys * nrhs);
+    BAAS_CUDA(cudaMemcpyAsync(s->d_active, &active, sizeof(active), cudaMemcpyHostToDevice, stream));
+
+    baas::BatchArgs a{};
+    a.n = n;
+    a.ldb = ldb;
+    a.a_rowptr = A->rowptr;
+    a.a_colidx = A->colidx;
+    a.a_diag = s->d_a_diag;
+    a.a_val = A->values;
+    a.B = B;
+    a.X = X;
+    a.fac = s->d_fwd.view(P);
+    a.pl = chunk_plan(s, *w);
+    a.bp = baas::BatchPlan{s->nsys, nrhs, s->maxls, s->d_sys_off, s->d_vlo, s->d_sys_lo, s->d_nls, s->d_cta_lo, s->d_cta_hi};
+    for (int d = 0; d < 2; d++) {
+        a.gv64[d] = s->d_bgv64[d];
+        a.gv32[d] = s->d_bgv32[d];
+    }
+    a.lu = s->d_blu;
+    a.gflag = s->d_flags;
+    a.epoch = s->epoch;
+    a.r = s->d_br;
+    a.p = s->d_bp;
+    a.Ap = s->d_bAp;
+    a.y = s->d_by;
+    a.z = s->d_bz;
+    a.y32 = s->d_by32;
+    a.z32 = s->d_bz32;
+    a.part = s->d_bpart;
+    a.bar = s->d_bar;
+    a.active = s->d_active;
+    a.st = s->d_status;
+    a.maxiter = maxiter;
+    a.tol = tol;
+    a.out_iters = s->d_biters;
+    a.out_relres = s->d_brelres;
+    a.spin_limit = s->spin();
+    a.scal_off = (int)((w->smem + 15) / 16 * 16);
+    const size_t smem = (size_t)a.scal_off + (size_t)baas::batch_scal_bytes(s->maxls);
+    if (smem > (size_t)kMaxDynSmem) return fail(BAAS_ERR_BAD_ARG, "batched solve: shared memory over budget");
+    void *args[] = {(void *)&a};
+    const bool mr = nrhs > 1;
+    void *kern = mixed ? (mr ? (void *)baas::k_iccg_batched<float, true> : (void *)baas::k_iccg_batched<float, false>)
+                       : (mr ? (void *)baas::k_iccg_batched<double, true> : (void *)baas::k_iccg_batched<double, false>);
+    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, P, baas::kStageBlock, args, smem, stream));
+    BAAS_CUDA(cudaMemcpyAsync(iters, s->d_biters, sizeof(int) * (size_t)s->nsys * nrhs, cudaMemcpyDeviceToHost, stream));
+    BAAS_CUDA(cudaMemcpyAsync(relres, s->d_brelres, sizeof(double) * (size_t)s->nsys * nrhs, cudaMemcpyDeviceToHost, stream));
+    BAAS_TRY(read_status(s, stream));
+    for (int q = 0; q < s->nsys * nrhs; q++)
+        if (!(relres[q] < tol)) return fail(BAAS_ERR_NOT_CONVERGED, "maxiter reached before tol for some instance");
     return BAAS_OK;
 }
 

@@ -79,13 +79,15 @@ template <> struct Sent<float> {
     static __device__ __forceinline__ void store(float *p, float v) { st_relaxed_u32(p, __float_as_uint(v)); }
 };
 
-// Bounded wait bookkeeping. Every 128 polls the wait also looks at the shared status word so
-// that one failure ends every waiting thread promptly. Returns false when the caller must stop.
+// Bounded wait bookkeeping: the limit applies to each wait on its own (every wait starts with
+// begin()). Every 128 polls the wait also looks at the shared status word so that one failure
+// ends every waiting thread promptly. tick() returns false when the caller must stop.
 struct Waiter {
     unsigned int polls;
     unsigned int limit;
     DevStatus *st;
     __device__ __forceinline__ Waiter(unsigned int lim, DevStatus *s) : polls(0), limit(lim), st(s) {}
+    __device__ __forceinline__ void begin() { polls = 0; }
     __device__ __forceinline__ bool tick(int where) {
         ++polls;
         if ((polls & 127u) == 0u) {
@@ -112,6 +114,7 @@ template <> struct SSent<float> {
 
 template <typename T>
 __device__ __forceinline__ bool wait_smem(const T *p, T &out, Waiter &w, int where) {
+    w.begin();
     T v = SSent<T>::load(p);
     while (Sent<T>::is(v)) {
         if (!w.tick(where)) return false;
@@ -124,6 +127,7 @@ __device__ __forceinline__ bool wait_smem(const T *p, T &out, Waiter &w, int whe
 // Wait until *p no longer holds the sentinel; returns false if the wait was abandoned.
 template <typename T>
 __device__ __forceinline__ bool wait_value(const T *p, T &out, Waiter &w, int where) {
+    w.begin();
     T v = Sent<T>::load(p);
     while (Sent<T>::is(v)) {
         if (!w.tick(where)) return false;
@@ -135,6 +139,7 @@ __device__ __forceinline__ bool wait_value(const T *p, T &out, Waiter &w, int wh
 
 // Wait until an epoch-stamped ready flag reaches `epoch` (acquire).
 __device__ __forceinline__ bool wait_flag(const int *flag, int epoch, Waiter &w, int where) {
+    w.begin();
     while (ld_acquire_s32(flag) != epoch) {
         if (!w.tick(where)) return false;
     }

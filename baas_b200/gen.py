@@ -265,3 +265,12 @@ def normal_rhs(n: int, seed: int, nrhs: int = 1) -> np.ndarray:
     rng = np.random.default_rng(seed)
     out = rng.standard_normal((nrhs, n))
     return out[0] if nrhs == 1 else out
+
+
+def batch_vardiff2d(nsys: int = 64, kmin: int = 64, kmax: int = 512, seed: int = 4) -> list:
+    """Batched configuration: nsys SPD 2-D 5-point variable-coefficient diffusion systems with grid
+    sizes k ~ U[kmin, kmax] (seeded), kappa = exp(g), g a Gaussian field (sigma 1, correlation
+    length 8 cells), each with its own field seed."""
+    rng = np.random.default_rng(seed)
+    ks = rng.integers(kmin, kmax + 1, size=nsys)
+    return [vardiff2d(int(k), seed=seed * 1000 + j) for j, k in enumerate(ks)]

@@ -137,6 +137,12 @@ double baas_schedule_analysis_ms(const baas_schedule *s);
 /* Frees the schedule and its device memory. */
 void baas_destroy(baas_schedule *s);
 
+/* Rebuilds the schedule's device execution plan with other options (parts, partition,
+ * smem_budget, spin_limit; nthread must stay as analysed) without repeating the analysis: the
+ * device plan and workspaces are freed and built again at the next GPU call. Used by the
+ * autotuner (baas_b200/autotune.py). No counterpart in the reference. */
+baas_status baas_replan(baas_schedule *s, const baas_options *opt);
+
 /* Failure-detection test hook (no counterpart in the reference, whose waits never end):
  * makes the forward sweep's row `row` wait on a value that nothing ever writes, so the next
  * forward sweep on this schedule ends with BAAS_ERR_TIMEOUT after spin_limit polls while every
@@ -215,6 +221,29 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
 baas_status baas_iccg_adjoint(baas_schedule *s, const baas_csr *A, const double *g, double *lambda, const double *x,
                               double *grad_a, double tol, int maxiter, int precision, int *iters, double *relres,
                               void *stream);
+
+/* Batched systems (no counterpart in the reference, which solves one system per call).
+ * baas_batch_concat (host arrays) concatenates nsys CSR matrices into one block-diagonal
+ * pattern: rowptr (sum n + 1), colidx and values (sum nnz; values may be NULL) and the row
+ * offsets of the systems, sys_off (nsys + 1). Returns the total nnz; with rowptr, colidx or
+ * sys_off NULL it only returns the total (for sizing); -1 on bad input. */
+int baas_batch_concat(int nsys, const baas_csr *const *sys, int *rowptr, int *colidx, double *values, int *sys_off);
+
+/* Analyses a block-diagonal SPD pattern (host arrays) of nsys systems with row offsets sys_off
+ * as one ICCG schedule: the systems' level sets merge, so one launch serves them all. Rejects a
+ * pattern with an entry between two systems. */
+baas_status baas_analyze_batch(const baas_csr *A, const int *sys_off, int nsys, const baas_options *opt,
+                               baas_schedule **out);
+
+/* Solves every system of a batch schedule for nrhs right-hand sides (1..8) with IC0-PCG in one
+ * persistent launch: A is the block-diagonal matrix (device), B and X are n x nrhs column-major
+ * device arrays (leading dimension ldb; X holds the initial guesses). Each (system, right-hand
+ * side) pair is its own CG instance, stopping once its ||r_k|| / ||r_0|| < tol; the launch ends
+ * when all have stopped or after maxiter iterations. Writes per instance (index s * nrhs + r)
+ * the iterations and the final relative residual into the HOST arrays iters and relres;
+ * BAAS_ERR_NOT_CONVERGED if any instance missed tol. precision as for baas_iccg. */
+baas_status baas_iccg_batched(baas_schedule *s, const baas_csr *A, const double *B, double *X, int nrhs, int ldb,
+                              double tol, int maxiter, int precision, int *iters, double *relres, void *stream);
 
 /* Human-readable text for the last error on this thread (never NULL). */
 const char *baas_last_error_string(void);

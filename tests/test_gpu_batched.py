@@ -1,0 +1,80 @@
+"""Batched ICCG (baas_analyze_batch + baas_iccg_batched): many independent SPD systems with several
+right-hand sides each, in one persistent launch, checked per instance against the oracle's PCG
+(iterations within +-1 for FP64 factors, solutions within 1e-8) and by independent residuals."""
+import numpy as np
+import pytest
+
+from baas_b200 import PREC_FP32_FACTORS, PREC_FP64, BatchSchedule, DeviceCSR, gen
+from oracle.oracle import Port
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _solve(systems, nrhs, precision, tol=1e-10, parts=0, seed=2):
+    import torch
+
+    s = BatchSchedule(systems, nthread=8, parts=parts)
+    A = s.combined
+    B = gen.uniform_rhs(A.n, seed, nrhs=nrhs).reshape(nrhs, A.n)
+    dA = DeviceCSR.from_host(A)
+    X = torch.zeros((nrhs, A.n), dtype=torch.float64, device="cuda")
+    it, rel = s.iccg_batched(dA, _t(B), X, tol=tol, maxiter=5000, precision=precision)
+    return s, B, X.cpu().numpy(), it, rel
+
+
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_FP32_FACTORS])
+@pytest.mark.parametrize("nrhs", [1, 4])
+def test_batched_small_matches_oracle(precision, nrhs):
+    rng = np.random.default_rng(3)
+    systems = [gen.vardiff2d(int(k), seed=10 + j) for j, k in enumerate(rng.integers(6, 40, size=7))]
+    s, B, X, it, rel = _solve(systems, nrhs, precision, parts=5)
+    assert np.all(rel < 1e-10)
+    off = s.sys_off
+    for q, m in enumerate(systems):
+        for r in range(nrhs):
+            b = B[r, off[q]:off[q + 1]]
+            xw, itw, _ = Port.pcg(m, b, tol=1e-10, maxiter=5000)
+            x = X[r, off[q]:off[q + 1]]
+            assert np.linalg.norm(x - xw) / np.linalg.norm(xw) < 1e-8
+            if precision == PREC_FP64:
+                assert abs(int(it[q, r]) - itw) <= 1
+
+
+def test_batched_zero_rhs_and_one_system():
+    import torch
+
+    systems = [gen.laplace2d(10), gen.vardiff2d(12, seed=1)]
+    s = BatchSchedule(systems, parts=3)
+    A = s.combined
+    B = gen.uniform_rhs(A.n, 5, nrhs=2).reshape(2, A.n)
+    B[1, s.sys_off[0]:s.sys_off[1]] = 0.0  # system 0, right-hand side 1: already solved
+    X = torch.zeros((2, A.n), dtype=torch.float64, device="cuda")
+    it, rel = s.iccg_batched(DeviceCSR.from_host(A), _t(B), X, tol=1e-10)
+    assert it[0, 1] == 0 and rel[0, 1] == 0.0
+    assert np.all(X[1, :100].cpu().numpy() == 0.0)
+    assert np.all(rel[:, 0] < 1e-10) and rel[1, 1] < 1e-10
+
+
+def test_batched_full_configuration():
+    """64 systems, k ~ U[64, 512], 4 right-hand sides, FP32 factors; residuals recomputed on the
+    CPU, and three systems against the oracle in FP64."""
+    systems = gen.batch_vardiff2d()
+    s, B, X, it, rel = _solve(systems, 4, PREC_FP32_FACTORS)
+    assert np.all(rel < 1e-10)
+    off = s.sys_off
+    Asp = s.combined.to_scipy()
+    for r in range(4):
+        res = B[r] - Asp @ X[r]
+        for q in range(len(systems)):
+            sl = slice(off[q], off[q + 1])
+            assert np.linalg.norm(res[sl]) / np.linalg.norm(B[r, sl]) < 1e-9
+    for q in (0, 17, 40):
+        xw, _, _ = Port.pcg(systems[q], B[0, off[q]:off[q + 1]], tol=1e-12, maxiter=20000)
+        x = X[0, off[q]:off[q + 1]]
+        assert np.linalg.norm(x - xw) / np.linalg.norm(xw) < 1e-6
