@@ -179,6 +179,118 @@ def cpu_baseline_sample():
                       f"Scheduler P2P_RULE path, nthread={cores}; analysis {t[0]:.1f} ms excluded"}
 
 
+def _event_ms(fn, reps=3, flush=None):
+    """Best CUDA-event time of fn() over reps runs (after one untimed run)."""
+    import torch
+
+    fn()
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(min(ts))
+
+
+def c1_sptrsv(flush):
+    """The 128x128 5-point lower-triangle forward sweep (SpTRSV HBM GB/s)."""
+    import torch
+
+    from baas_b200 import KERNEL_SPTRSV, DeviceCSR, Schedule, gen
+
+    L, x_true, b = gen.sptrsv_case(128, 0)
+    s = Schedule(L, kind=KERNEL_SPTRSV, nthread=8)
+    dL = DeviceCSR.from_host(L)
+    db = torch.from_numpy(b).cuda()
+    x = torch.zeros_like(db)
+    ms = _event_ms(lambda: s.forward(dL, db, x), 10, flush)
+    nbytes = 12 * L.nnz + 4 * (L.n + 1) + 16 * L.n
+    err = float(np.max(np.abs(x.cpu().numpy() - x_true)))
+    return {"workload": "sptrsv_laplace2d_128_lower", "ms": round(ms, 4), "bytes": nbytes,
+            "gbps": round(nbytes / (ms * 1e-3) / 1e9, 2), "max_abs_err_vs_x_true": err}
+
+
+def c3_ilu(flush):
+    """ILU0 of the 96^3 upwind convection-diffusion operator and its apply on 8 right-hand sides."""
+    import scipy.sparse as sp
+    import torch
+
+    from baas_b200 import KERNEL_ILU0, DeviceCSR, Schedule, gen
+
+    C = gen.convdiff3d(96)
+    s = Schedule(C, kind=KERNEL_ILU0, nthread=8)
+    dC = DeviceCSR.from_host(C)
+    lu = dC.values.clone()
+    ilu_ms = _event_ms(lambda: (lu.copy_(dC.values), s.ilu0(dC, lu)), 3, flush)
+    M = gen.CSR(C.n, C.rowptr, C.colidx, lu.cpu().numpy()).to_scipy()
+    Lo = gen.from_scipy(sp.tril(M, k=-1) + sp.identity(C.n, format="csr"))
+    Up = gen.from_scipy(sp.triu(M))
+    dL, dU = DeviceCSR.from_host(Lo), DeviceCSR.from_host(Up)
+    B = torch.from_numpy(gen.normal_rhs(C.n, 2, nrhs=8)).cuda()
+    Y = torch.zeros_like(B)
+    Z = torch.zeros_like(B)
+    fwd = _event_ms(lambda: s.forward(dL, B, Y), 5, flush)
+    bwd = _event_ms(lambda: s.backward(dU, Y, Z), 5, flush)
+    nnz_t = Lo.nnz
+    nbytes = 12 * nnz_t + 4 * (C.n + 1) + 16 * C.n * 8
+    return {"workload": "ilu0_convdiff3d_96_8rhs", "n": C.n, "nnz": C.nnz, "ilu0_ms": round(ilu_ms, 4),
+            "forward_8rhs_ms": round(fwd, 4), "backward_8rhs_ms": round(bwd, 4),
+            "sweep_bytes_8rhs": nbytes, "forward_gbps": round(nbytes / (fwd * 1e-3) / 1e9, 2),
+            "backward_gbps": round(nbytes / (bwd * 1e-3) / 1e9, 2)}
+
+
+def c4_batched():
+    """64 variable-coefficient 2-D diffusion systems (k ~ U[64, 512]) x 4 right-hand sides, FP32
+    IC0 factors, one launch; plan parameters picked by the autotuner on short trial runs."""
+    import torch
+
+    from baas_b200 import PREC_FP32_FACTORS, PREC_FP64, BatchSchedule, DeviceCSR, autotune, gen
+
+    t0 = time.time()
+    systems = gen.batch_vardiff2d()
+    s = BatchSchedule(systems, nthread=8)
+    analysis_s = time.time() - t0
+    A = s.combined
+    dA = DeviceCSR.from_host(A)
+    B = torch.from_numpy(gen.uniform_rhs(A.n, 2, nrhs=4).reshape(4, A.n)).cuda()
+    X = torch.zeros_like(B)
+
+    def trial():
+        X.zero_()
+        s.iccg_batched(dA, B, X, tol=TOL, maxiter=30, precision=PREC_FP32_FACTORS, raise_on_nonconvergence=False)
+
+    tuned = autotune.tune(s, trial, parts=(96, 128, 148), budgets=(0, 160 * 1024), repeats=1)
+
+    def full(prec):
+        X.zero_()
+        return s.iccg_batched(dA, B, X, tol=TOL, maxiter=20000, precision=prec)
+
+    it32, rel32 = full(PREC_FP32_FACTORS)
+    ms32 = _event_ms(lambda: full(PREC_FP32_FACTORS), 2)
+    x32 = X.clone()
+    it64, rel64 = full(PREC_FP64)
+    ms64 = _event_ms(lambda: full(PREC_FP64), 1)
+    x64 = X.clone()
+    off = s.sys_off
+    errs = []
+    for q in range(len(systems)):
+        a, b = int(off[q]), int(off[q + 1])
+        d = torch.linalg.norm(x32[:, a:b] - x64[:, a:b], dim=1) / torch.linalg.norm(x64[:, a:b], dim=1)
+        errs.append(float(d.max()))
+    return {"workload": "batched_vardiff2d_64sys_k64-512_4rhs", "n_total": A.n, "nnz_total": A.nnz,
+            "systems": len(systems), "rhs": 4, "ms_fp32_factors": round(ms32, 3), "ms_fp64": round(ms64, 3),
+            "iterations_fp32": {"min": int(it32.min()), "median": float(np.median(it32)), "max": int(it32.max())},
+            "max_relres": float(rel32.max()), "rel_err_vs_fp64_per_system": {"max": max(errs),
+                                                                              "median": float(np.median(errs))},
+            "autotuned": tuned["best"], "analysis_s": round(analysis_s, 2)}
+
+
 def gpu_arm(args):
     import torch
 
@@ -289,6 +401,16 @@ def gpu_arm(args):
         ee.append(e0.elapsed_time(e1))
     e2e_ms = float(np.mean(ee))
 
+    # the other configurations (1 GPU only: replicas would repeat them)
+    extras = {}
+    if world == 1 and not args.headline_only:
+        for name, fn in (("sptrsv_c1", lambda: c1_sptrsv(flush)), ("ilu0_c3", lambda: c3_ilu(flush)),
+                         ("batched_c4", c4_batched)):
+            try:
+                extras[name] = fn()
+            except Exception as e:  # a failure here must not cost the headline line
+                extras[name] = {"error": f"{type(e).__name__}: {str(e)[:160]}"}
+
     vals = torch.tensor([ms64, e2e_ms, ms32], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.all_reduce(vals, op=torch.distributed.ReduceOp.MAX)
@@ -297,13 +419,13 @@ def gpu_arm(args):
     peak, peak_kind = _peaks()
     launch_bytes = IC0_BYTES + it * ITER_BYTES
     achieved = launch_bytes / (ms64 * 1e-3) / 1e9
+    # DRAM bytes of one launch, from the ncu capture summarised in profiles/
     traffic = None
-    tp = ROOT / "profiles" / "iccg_traffic.json"
+    tp = ROOT / "profiles" / "k_iccg_chunked_laplace3d_64.md"
     if tp.exists():
-        try:
-            traffic = json.loads(tp.read_text()).get("bytes_per_solve")
-        except Exception:
-            traffic = None
+        for line in tp.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_launch:"):
+                traffic = int(line.split(":")[1])
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -331,6 +453,7 @@ def gpu_arm(args):
             "sptrsv": {"ms": round(sweep_ms, 4), "bytes": SWEEP_BYTES,
                        "gbps": round(SWEEP_BYTES / (sweep_ms * 1e-3) / 1e9, 2)},
             "analysis_ms": round(analysis_ms, 2),
+            "configs": extras,
             "wall_s_timed_region": round(wall, 3),
         }
         print(json.dumps(line))
@@ -358,6 +481,15 @@ def profile_case(args):
         lo = gen.CSR(A.n, A.rowptr, A.colidx, lu.cpu().numpy()).lower()
         dT = DeviceCSR.from_host(lo if case == "sweep_lower" else lo.transpose())
         run = (lambda: s.forward(dT, b, x)) if case == "sweep_lower" else (lambda: s.backward(dT, b, x))
+    elif case == "batched_small":
+        from baas_b200 import BatchSchedule
+
+        sb = BatchSchedule(gen.batch_vardiff2d(nsys=8, kmin=64, kmax=128), nthread=8)
+        dB = DeviceCSR.from_host(sb.combined)
+        Bb = torch.from_numpy(gen.uniform_rhs(sb.n, 2, nrhs=4).reshape(4, sb.n)).cuda()
+        Xb = torch.zeros_like(Bb)
+        run = lambda: (Xb.zero_(), sb.iccg_batched(dB, Bb, Xb, tol=TOL, maxiter=20000,  # noqa: E731
+                                                    precision=PREC_FP32_FACTORS))
     elif case == "ic0":
         lu = dA.values.clone()
         run = lambda: (lu.copy_(dA.values), s.ic0(dA, lu))  # noqa: E731
@@ -385,8 +517,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="baas_b200", choices=["baas_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true", help="skip the other configurations")
     ap.add_argument("--profile-case", default=None,
-                    choices=["iccg", "iccg_fp32", "ic0", "sweep_lower", "sweep_upper"],
+                    choices=["iccg", "iccg_fp32", "ic0", "sweep_lower", "sweep_upper", "batched_small"],
                     help="run one kernel of the workload only (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
