@@ -22,8 +22,9 @@ from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, PARTI
                       PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
 
-__all__ = ["Schedule", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV", "KERNEL_ICCG", "KERNEL_IC0",
-           "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "version"]
+__all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV",
+           "KERNEL_ICCG", "KERNEL_IC0", "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "PARTITION_RANGES",
+           "PARTITION_BAAS_THREADS", "version"]
 
 
 def version() -> str:

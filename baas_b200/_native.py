@@ -38,7 +38,7 @@ FIELDS = {
 EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
-    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan",
+    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan", "baas_test_divide",
 ]
 
 
@@ -111,6 +111,8 @@ def lib():
     L.baas_iccg_batched.restype = i
     L.baas_test_emulate_sweep.argtypes = [vp, i, i, i, vp, vp, vp]
     L.baas_test_emulate_sweep.restype = i
+    L.baas_test_divide.argtypes = [vp, vp, vp, C.c_longlong, i, vp]
+    L.baas_test_divide.restype = i
     _lib = L
     return L
 

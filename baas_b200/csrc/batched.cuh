@@ -145,22 +145,13 @@ __device__ __forceinline__ bool batch_precond(const BatchArgs &A, WinStream<T> &
     T *yg = sizeof(T) == 8 ? (T *)A.y : (T *)A.y32;
     T *zg = sizeof(T) == 8 ? (T *)A.z : (T *)A.z32;
     T *xs = reinterpret_cast<T *>(smem);
-    bool alive = true;
-    for (int i = 0; i < ws.total(); i++) {
-        const unsigned char *buf;
-        int nint;
-        if (!ws.acquire(i, A.spin_limit, A.st, buf, nint)) return false;
-        if (i < ws.ctl->n0) {
-            const WalkIO<T, double, MR, false> lo{xs, yg, A.r, nullptr, A.n, A.n, A.bp.R};
-            alive = walk_window<T, double, false, MR, false, sizeof(T) == 8>(buf, nint, lo, w, alive);
-        } else {
-            const WalkIO<T, T, MR, false> up{xs, zg, yg, nullptr, A.n, A.n, A.bp.R};
-            alive = walk_window<T, T, true, MR, false, sizeof(T) == 8>(buf, nint, up, w, alive);
-        }
-        ws.release(i);
-        if (__syncthreads_or(!alive)) return false;
+    const int n0 = ws.ctl->n0;
+    {
+        const WalkIO<T, double, MR, false> lo{xs, yg, A.r, nullptr, A.n, A.n, A.bp.R};
+        if (!walk_dir<T, double, false, MR, false, sizeof(T) == 8>(ws, 0, n0, lo, w, A.spin_limit, A.st)) return false;
     }
-    return true;
+    const WalkIO<T, T, MR, false> up{xs, zg, yg, nullptr, A.n, A.n, A.bp.R};
+    return walk_dir<T, T, true, MR, false, sizeof(T) == 8>(ws, n0, ws.total(), up, w, A.spin_limit, A.st);
 }
 
 template <typename T, bool MR>
@@ -260,14 +251,22 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_batched(BatchArgs A) {
         batch_partials(A, red & 1, [&](int a, int b, int, double (&acc)[kMaxRhs]) {
             for (int i = a + (int)threadIdx.x; i < b; i += blockDim.x) {
                 const int e0 = __ldg(A.a_rowptr + i), e1 = __ldg(A.a_rowptr + i + 1);
+                // each entry of A read once for all right-hand sides
+                double s[kMaxRhs];
+#pragma unroll
+                for (int r = 0; r < kMaxRhs; r++) s[r] = 0.0;
+                for (int e = e0; e < e1; e++) {
+                    const double v = __ldg(A.a_val + e);
+                    const int j = __ldg(A.a_colidx + e);
+#pragma unroll
+                    for (int r = 0; r < kMaxRhs; r++)
+                        if (r < R) s[r] = __dadd_rn(s[r], __dmul_rn(v, A.p[(size_t)r * n + j]));
+                }
 #pragma unroll
                 for (int r = 0; r < kMaxRhs; r++)
                     if (r < R) {
-                        const double *p = A.p + (size_t)r * n;
-                        double s = 0.0;
-                        for (int e = e0; e < e1; e++) s = __dadd_rn(s, __dmul_rn(A.a_val[e], p[__ldg(A.a_colidx + e)]));
-                        A.Ap[(size_t)r * n + i] = s;
-                        acc[r] = __dadd_rn(acc[r], __dmul_rn(p[i], s));
+                        A.Ap[(size_t)r * n + i] = s[r];
+                        acc[r] = __dadd_rn(acc[r], __dmul_rn(A.p[(size_t)r * n + i], s[r]));
                         yg[(size_t)r * n + i] = Sent<T>::value();
                     }
             }

@@ -472,13 +472,15 @@ void build_chunks(baas_schedule *s) {
                     ne[q] = H.eptr[pos + 1] - H.eptr[pos];
                     vT[q] = baas::diag_code(H.dsrcT[pos]);
                     vA[q] = baas::diag_code(H.dsrcA[pos]);
+                    vT[nl + q] = baas::rcp_code(H.dsrcT[pos]);
+                    vA[nl + q] = baas::rcp_code(H.dsrcA[pos]);
                     for (int j = 0; j < ne[q]; j++) {
                         const int e = H.eptr[pos] + j;
                         const int dd = H.dep[e];
                         // local: the producer's slot; remote: -(row + 1)
                         dep[q * E + j] = dd < 0 ? slot[ordidx[H.cta_pos[c] + (-dd - 1)]] : -(dd + 1);
-                        vT[nl + q * E + j] = H.srcT[e];
-                        vA[nl + q * E + j] = H.srcA[e];
+                        vT[2 * nl + q * E + j] = H.srcT[e];
+                        vA[2 * nl + q * E + j] = H.srcA[e];
                     }
                 }
                 D.chunk_ioff.push_back((int)D.ints.size());
@@ -783,6 +785,8 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     if (o.smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
     if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
     if (A->rowptr[A->n] != A->nnz) return fail(BAAS_ERR_BAD_ARG, "nnz != rowptr[n]");
+    // value-source codes of the sweep plan address positions below 2^30
+    if (A->nnz >= (1 << 30) - 2) return fail(BAAS_ERR_BAD_ARG, "nnz must be below 2^30 - 2");
     const baas::SchedKind sk = (baas::SchedKind)kind;
     const char *why = baas::validate_pattern(A->n, A->rowptr, A->colidx, sk);
     if (why[0]) return fail(BAAS_ERR_BAD_ARG, why);
@@ -849,6 +853,27 @@ baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row) {
     return BAAS_OK;
 }
 
+namespace {
+__global__ void k_test_divide(const double *a, const double *b, double *q, long long n, int mode) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double x = a[i], d = b[i];
+        q[i] = mode == 0 ? baas::div_rcp(x, d, baas::div_recip(d)) : __ddiv_rn(x, d);
+    }
+}
+}  // namespace
+
+baas_status baas_test_divide(const double *a, const double *b, double *q, long long n, int mode, void *stream) {
+    if (n < 0 || (n > 0 && (!a || !b || !q))) return fail(BAAS_ERR_BAD_ARG, "NULL argument or negative n");
+    if (mode != 0 && mode != 1) return fail(BAAS_ERR_BAD_ARG, "mode must be 0 or 1");
+    if (n == 0) return BAAS_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_test_divide<<<(int)blocks, 256, 0, st>>>(a, b, q, n, mode);
+    BAAS_CUDA(cudaGetLastError());
+    BAAS_CUDA(cudaStreamSynchronize(st));
+    return BAAS_OK;
+}
+
 baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget, int upper, const double *tval,
                                     const double *b, double *x) {
     if (!s || !tval || !b || !x) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
@@ -877,9 +902,10 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
     std::vector<double> gv(D.vsrcT.size());
     for (size_t i = 0; i < gv.size(); i++) {
         const int code = D.vsrcT[i];
-        const int src = code >= 0 ? code : (code <= -2 ? -2 - code : -1);
+        const bool rcp = code < -(1 << 30);
+        const int src = code >= 0 ? code : (rcp ? code - baas::kRcpBase : (code <= -2 ? -2 - code : -1));
         if (src >= s->nnz_l) return bad("value source out of range");
-        gv[i] = src >= 0 ? tval[src] : 0.0;
+        gv[i] = src >= 0 ? (rcp ? 1.0 / tval[src] : tval[src]) : 0.0;
     }
     std::vector<char> ready(n, 0);
     // the column that entry j of row r must read: L rows ascending (diagonal last), U = L^T rows
@@ -931,7 +957,7 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
                 return bad("chunk runs past its window");
             const int *rowid = I + baas::kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *kp = ne + nl, *dep = kp + nl;
             const double *V = K.vbuf.data() + K.vp;
-            const double *diag = V, *val = V + nl;
+            const double *diag = V, *rcp = V + nl, *val = V + 2 * nl;
             const int ns = C.slot_max;
             bool wait = false;
             for (int pos = 0; pos < nl && !wait; pos++) {
@@ -968,6 +994,7 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
                     }
                     sum = sum + xv * val[pos * E + j];
                 }
+                if (rcp[pos] != 1.0 / diag[pos]) return bad("a row's reciprocal slot does not match its diagonal");
                 outs[pos] = (b[row] - sum) / diag[pos];
             }
             for (int pos = 0; pos < nl; pos++) {

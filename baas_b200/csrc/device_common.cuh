@@ -221,6 +221,35 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned int 
     return false;
 }
 
+// Reciprocal stored beside a diagonal entry d for div_rcp: RN(1/d) (__drcp_rn) when
+// 2^-500 <= |d| <= 2^500, else 0, which sends every division by d to __ddiv_rn.
+__device__ __forceinline__ double div_recip(double d) {
+    const unsigned int e = ((unsigned int)__double2hiint(d) >> 20) & 0x7ffu;  // biased exponent
+    return e - (1023u - 500u) <= 999u ? __drcp_rn(d) : 0.0;
+}
+
+// Correctly rounded FP64 quotient a / b from y = div_recip(b), by Markstein's method
+// (P. Markstein, "Computation of elementary functions on the IBM RISC System/6000 processor",
+// IBM J. Res. Dev. 34(1), 1990; Muller et al., Handbook of Floating-Point Arithmetic, division
+// with an FMA): q0 = RN(a*y) lies within two ulps of a/b; one correction
+// q1 = RN(q0 + RN(a - b*q0)*y) makes it a faithful rounding; then, y being RN(1/b) and the
+// remainder a - b*q1 exact in an FMA, q2 = RN(q1 + (a - b*q1)*y) = RN(a/b). The remainders are
+// exact and nothing under- or overflows while 2^-500 <= |b| <= 2^500 (y != 0) and
+// 2^-460 <= |a| < 2^461: then 2^-961 <= |a/b| <= 2^961 and the remainders' lowest bits stay
+// above 2^-570. Otherwise (zeros, subnormals, infinities, NaNs and the far ranges) the quotient
+// comes from __ddiv_rn. The range test reads a's exponent bits and runs beside the FMA chain.
+__device__ __forceinline__ double div_rcp(double a, double b, double y) {
+    const unsigned int ea = ((unsigned int)__double2hiint(a) >> 20) & 0x7ffu;
+    const bool fast = ea - (1023u - 460u) <= 920u && y != 0.0;
+    const double q0 = __dmul_rn(a, y);
+    const double r0 = __fma_rn(-q0, b, a);
+    const double q1 = __fma_rn(r0, y, q0);
+    const double r1 = __fma_rn(-q1, b, a);
+    const double q2 = __fma_rn(r1, y, q1);
+    if (fast) return q2;
+    return __ddiv_rn(a, b);
+}
+
 // Explicit shared-memory accesses for data reached through pointers the compiler cannot prove
 // to be shared (window buffers, staged arrays handed through structures): a generic access to
 // shared memory is resolved in the L1TEX unit and costs far more than ld/st.shared. Volatile,

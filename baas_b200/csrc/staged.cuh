@@ -10,7 +10,7 @@
 // The plan of a step is a self-contained CHUNK (a wide step is cut into several):
 //   int block   [nl, E, nl_next, 0 | rowid (nl) | slot (nl) | ne (nl) | kpos (nl) | dep (nl*E)],
 //               padded to 8 ints
-//   value block [diag (nl) | val (nl*E)], padded to 4 values
+//   value block [diag (nl) | 1/diag (nl) | val (nl*E)], padded to 4 values
 // with E the widest row of the CTA (one stride for all of a CTA's chunks, so the walk is
 // specialised on it once per window), and row `pos` finds its entries at pos*E + j.
 // nl_next is the next chunk's row count (what the pipelined walk needs to address it early).
@@ -44,9 +44,12 @@ constexpr int kMaxRhs = 8;                 // right-hand sides walked together
 __host__ __device__ constexpr int pad4(int x) { return (x + 3) & ~3; }
 __host__ __device__ constexpr int pad8(int x) { return (x + 7) & ~7; }
 __host__ __device__ constexpr int chunk_nint(int nl, int E) { return pad8(kChunkHdr + 4 * nl + nl * E); }
-__host__ __device__ constexpr int chunk_nval(int nl, int E) { return pad4(nl + nl * E); }
-// value-source code of a diagonal entry at position p (off-diagonals: p >= 0; padding: -1)
+__host__ __device__ constexpr int chunk_nval(int nl, int E) { return pad4(2 * nl + nl * E); }
+// value-source codes: off-diagonal entry at position p: p; padding: -1; diagonal entry at p:
+// -2 - p; the diagonal's correctly rounded reciprocal: kRcpBase + p (positions < 2^30)
+constexpr int kRcpBase = -2147483647 - 1;
 __host__ __device__ constexpr int diag_code(int p) { return -2 - p; }
+__host__ __device__ constexpr int rcp_code(int p) { return kRcpBase + p; }
 
 struct ChunkDir {
     const int *ints;           // chunk int blocks, CTA by CTA
@@ -84,10 +87,16 @@ __host__ __device__ constexpr int chunk_smem_bytes(int xs_bytes, int rhs_bytes, 
     return xs_bytes + rhs_bytes + 2 * cap + win_ctl_bytes(nrec);
 }
 
-// Value of source code s in array v (the packing of a window's value slots).
+// Value of source code s in array v (the packing of a window's value slots); reciprocal slots
+// hold div_recip of the diagonal.
 template <typename V>
 __device__ __forceinline__ double src_value(const V *v, int s) {
-    return s >= 0 ? (double)v[s] : (s <= -2 ? (double)v[-2 - s] : 0.0);
+    if (s >= 0) return (double)v[s];
+    if (s == -1) return 0.0;
+    if (s < -(1 << 30)) {
+        return div_recip((double)v[s - kRcpBase]);
+    }
+    return (double)v[-2 - s];
 }
 
 // The stream of windows one CTA walks: the windows of direction `first`, then (two_dirs)
@@ -172,6 +181,23 @@ struct WinStream {
         nint = ctl->nint[s & 1u];
         return true;
     }
+    // The window after item i of the current pass, from one thread's view: waits (bounded) for its
+    // copy without a CTA barrier; the caller makes the outcome uniform at its next barrier. The
+    // buffer and size are returned also when the wait gave up (the caller then reads nothing).
+    __device__ bool peek(int i, unsigned int spin, const unsigned char *&b, int &nint) {
+        unsigned int s;
+        bool ok = true;
+        if (ctl->resident) {
+            s = (unsigned int)(i + 1);
+            if (!loaded) ok = mbar_wait(&ctl->mbar[s & 1u], (s >> 1) & 1u, spin);
+        } else {
+            s = consumed + 1u;
+            ok = mbar_wait(&ctl->mbar[s & 1u], (s >> 1) & 1u, spin);
+        }
+        b = buf + (s & 1u) * cap;
+        nint = ctl->rec[s % (unsigned int)total()].y;
+        return ok;
+    }
     // After the walk of item i (which ended with a CTA barrier): refill its buffer.
     __device__ void release(int i) {
         if (ctl->resident) {
@@ -226,7 +252,7 @@ template <typename T, int EK>
 struct RowVals {
     int sl;
     T a[EK];
-    T diag, rhs;
+    T diag, rcp, rhs;
 };
 
 template <int EK>
@@ -245,10 +271,11 @@ template <typename T, typename RT, bool RL2, bool MR, bool STG, int EK>
 __device__ __forceinline__ void load_vals(const int *I, const T *V, int nl, int pos, const RowDeps<EK> &p,
                                           const WalkIO<T, RT, MR, STG> &io, RowVals<T, EK> &v) {
     v.sl = Sh<int>::ld(I + kChunkHdr + nl + pos);
-    const T *vp = V + nl + pos * EK;
+    const T *vp = V + 2 * nl + pos * EK;
 #pragma unroll
     for (int j = 0; j < EK; j++) v.a[j] = Sh<T>::ld(vp + j);
     v.diag = Sh<T>::ld(V + pos);
+    if constexpr (sizeof(T) == 8) v.rcp = Sh<T>::ld(V + nl + pos);
     if constexpr (STG) v.rhs = Sh<T>::ld(io.rs + io.slot(p.kpos));
 }
 
@@ -319,7 +346,7 @@ __device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<
         }
     T o;
     if constexpr (EXACT)
-        o = __ddiv_rn(__dsub_rn(v.rhs, sum), v.diag);
+        o = div_rcp(__dsub_rn(v.rhs, sum), v.diag, v.rcp);
     else
         o = (v.rhs - sum) * v.diag;  // FP32 value blocks hold 1/diag
     if (v.sl >= 0) Sh<T>::st(io.xs + io.slot(v.sl), o);
@@ -328,16 +355,25 @@ __device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<
     return true;
 }
 
-// Walk one window whose chunks all have entry stride EK (1..3). At the start of step s a
-// thread issues the loads of its step-s+1 row's dependency indices; they complete while step s
-// computes, so the loads of that row's remote values (and, without staging, of its right-hand
-// side) go out before the barrier that ends step s without waiting. The rest of a row's plan is
-// loaded after the barrier, together with its dependencies' slots. Rows beyond one pass of the
-// block loop without prefetch.
+// Walk a direction's chunks with entry stride EK (1..3) from window item `i` (held in buf)
+// through its last window, crossing windows without a break in the step pipeline. At the start
+// of step s a thread issues the loads of its step-s+1 row's dependency indices; they complete
+// while step s computes, so the loads of that row's remote values (and, without staging, of its
+// right-hand side) go out before the barrier that ends step s without waiting. The rest of a
+// row's plan is loaded after the barrier, together with its dependencies' slots. Rows beyond one
+// pass of the block loop go without prefetch. When step s+1 opens the next window, its copy is
+// awaited at the start of step s (it was issued a window earlier), the barrier ending step s also
+// decides, for the whole CTA, whether every wait so far succeeded, and the window of step s is
+// then released for refilling. Returns with `i` on the last window walked (not released).
 template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT, int EK>
-__device__ __forceinline__ bool walk_window_e(const int *I0, const int *Iend, const T *V0,
-                                              const WalkIO<T, RT, MR, STG> &io, Waiter &w, bool alive) {
-    const int lr = io.lane_row(), st = io.stride();
+__device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsigned char *buf, int nint,
+                                           const WalkIO<T, RT, MR, STG> &io, Waiter &w, unsigned int spin,
+                                           DevStatus *st) {
+    const int lr = io.lane_row(), stp = io.stride();
+    const int *I0 = reinterpret_cast<const int *>(buf);
+    const int *Iend = I0 + nint;
+    const T *V0 = reinterpret_cast<const T *>(buf + (size_t)nint * 4);
+    bool alive = true;
     int nl0 = Sh<int>::ld(I0);
     RowDeps<EK> q0, q1;
     T pf0[EK];
@@ -349,10 +385,21 @@ __device__ __forceinline__ bool walk_window_e(const int *I0, const int *Iend, co
         if constexpr (!STG) rhs0 = load_rhs<T, RT, RL2, MR, STG>(q0.row, q0.kpos, io);
     }
     for (;;) {
+        const int nl1 = Sh<int>::ld(I0 + 2);  // 0 after the direction's last chunk
         const int *I1 = I0 + chunk_nint(nl0, EK);
         const T *V1 = V0 + chunk_nval(nl0, EK);
-        const int nl1 = I1 < Iend ? Sh<int>::ld(I0 + 2) : 0;
-        const bool m1 = lr < nl1;
+        const int *Iend1 = Iend;
+        const bool cross = nl1 != 0 && I1 == Iend;  // uniform: step s+1 opens the next window
+        bool okw = true;
+        if (cross) {
+            const unsigned char *nb;
+            int nn;
+            okw = ws.peek(i, spin, nb, nn);
+            I1 = reinterpret_cast<const int *>(nb);
+            Iend1 = I1 + nn;
+            V1 = reinterpret_cast<const T *>(nb + (size_t)nn * 4);
+        }
+        const bool m1 = okw && lr < nl1;
         if (m1) load_deps<EK>(I1, nl1, lr, q1);
         if (alive && m0) {
             RowVals<T, EK> v;
@@ -360,7 +407,7 @@ __device__ __forceinline__ bool walk_window_e(const int *I0, const int *Iend, co
             if constexpr (!STG) v.rhs = rhs0;
             if (!row_compute<T, RT, MR, STG, EXACT, EK>(q0, v, pf0, io, w)) alive = false;
         }
-        for (int pos = lr + st; alive && pos < nl0; pos += st) {
+        for (int pos = lr + stp; alive && pos < nl0; pos += stp) {
             RowDeps<EK> q;
             RowVals<T, EK> v;
             T qf[EK];
@@ -375,7 +422,15 @@ __device__ __forceinline__ bool walk_window_e(const int *I0, const int *Iend, co
             load_remote<T, RT, MR, STG, EK>(q1, io, pf0);
             if constexpr (!STG) rhs1 = load_rhs<T, RT, RL2, MR, STG>(q1.row, q1.kpos, io);
         }
-        __syncthreads();
+        if (cross) {
+            if (!okw && atomicCAS(&st->code, kOk, kTimeout) == kOk) st->where = -1000000 - i - 1;
+            if (__syncthreads_or(!okw || !alive)) return false;
+            ws.release(i);
+            i++;
+            Iend = Iend1;
+        } else {
+            __syncthreads();
+        }
         if (nl1 == 0) break;
         I0 = I1;
         V0 = V1;
@@ -395,7 +450,7 @@ __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, c
     while (I < Iend) {
         const int nl = I[0], E = I[1];
         const int *rowid = I + kChunkHdr, *slot = rowid + nl, *ne = slot + nl, *kpos = ne + nl, *dep = kpos + nl;
-        const T *diag = V, *val = V + nl;
+        const T *diag = V, *rcp = V + nl, *val = V + 2 * nl;
         for (int pos = io.lane_row(); alive && pos < nl; pos += io.stride()) {
             const int row = rowid[pos];
             T rhs;
@@ -426,7 +481,7 @@ __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, c
             if (!alive) break;
             T o;
             if constexpr (EXACT)
-                o = __ddiv_rn(__dsub_rn(rhs, sum), diag[pos]);
+                o = div_rcp(__dsub_rn(rhs, sum), diag[pos], rcp[pos]);
             else
                 o = (rhs - sum) * diag[pos];
             if (slot[pos] >= 0) io.xs[io.slot(slot[pos])] = o;
@@ -440,21 +495,39 @@ __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, c
     return alive;
 }
 
-// Walk one window (nint ints of chunk blocks, then their values) held in shared memory. All
-// chunks of a CTA share one entry stride. Every thread passes every barrier, also after a
-// failed wait, so the CTA never splits.
+// Walk the windows [i, iend) of one direction (all of a CTA's chunks in a direction share one
+// entry stride). Every thread passes every barrier, also after a failed wait, so the CTA never
+// splits; the result is uniform. Each window is released after its walk.
 template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT>
-__device__ __forceinline__ bool walk_window(const unsigned char *b, int nint, const WalkIO<T, RT, MR, STG> &io,
-                                            Waiter &w, bool alive) {
-    const int *I = reinterpret_cast<const int *>(b);
-    const int *Iend = I + nint;
-    const T *V = reinterpret_cast<const T *>(b + (size_t)nint * 4);
-    switch (I[1]) {
-        case 1: return walk_window_e<T, RT, RL2, MR, STG, EXACT, 1>(I, Iend, V, io, w, alive);
-        case 2: return walk_window_e<T, RT, RL2, MR, STG, EXACT, 2>(I, Iend, V, io, w, alive);
-        case 3: return walk_window_e<T, RT, RL2, MR, STG, EXACT, 3>(I, Iend, V, io, w, alive);
-        default: return walk_window_any<T, RT, RL2, MR, STG, EXACT>(I, Iend, V, io, w, alive);
+__device__ __forceinline__ bool walk_dir(WinStream<T> &ws, int i, int iend, const WalkIO<T, RT, MR, STG> &io,
+                                         Waiter &w, unsigned int spin, DevStatus *st) {
+    const unsigned char *b;
+    int nint;
+    if (i >= iend) return true;
+    if (!ws.acquire(i, spin, st, b, nint)) return false;
+    bool alive = true;
+    switch (Sh<int>::ld(reinterpret_cast<const int *>(b) + 1)) {
+        case 1: alive = walk_run_e<T, RT, RL2, MR, STG, EXACT, 1>(ws, i, b, nint, io, w, spin, st); break;
+        case 2: alive = walk_run_e<T, RT, RL2, MR, STG, EXACT, 2>(ws, i, b, nint, io, w, spin, st); break;
+        case 3: alive = walk_run_e<T, RT, RL2, MR, STG, EXACT, 3>(ws, i, b, nint, io, w, spin, st); break;
+        default:
+            for (;;) {
+                const int *I = reinterpret_cast<const int *>(b);
+                alive = walk_window_any<T, RT, RL2, MR, STG, EXACT>(I, I + nint,
+                                                                    reinterpret_cast<const T *>(b + (size_t)nint * 4),
+                                                                    io, w, alive);
+                if (i + 1 == iend) break;
+                ws.release(i);
+                if (__syncthreads_or(!alive)) return false;
+                if (!ws.acquire(++i, spin, st, b, nint)) return false;
+            }
     }
+    if (!alive && i + 1 < iend) {
+        // walk_run_e returned early (uniformly) at a window crossing
+        return false;
+    }
+    ws.release(i);
+    return !__syncthreads_or(!alive);
 }
 
 // Standalone FP64 sweep of the caller's triangular CSR (values gathered through vsrcT into the
@@ -501,20 +574,9 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, 
             __syncthreads();
         }
         trace_mark(trace, 2 + 2 * (r0 / R));
-        bool alive = true;
-        for (int i = 0; i < ws.total(); i++) {
-            const unsigned char *buf;
-            int nint;
-            if (!ws.acquire(i, spin, st, buf, nint)) {
-                ws.drain(spin);
-                return;
-            }
-            alive = walk_window<double, double, false, MR, STG, true>(buf, nint, io, w, alive);
-            ws.release(i);
-            if (__syncthreads_or(!alive)) {
-                ws.drain(spin);
-                return;
-            }
+        if (!walk_dir<double, double, false, MR, STG, true>(ws, 0, ws.total(), io, w, spin, st)) {
+            ws.drain(spin);
+            return;
         }
         trace_mark(trace, 3 + 2 * (r0 / R));
     }
@@ -572,22 +634,16 @@ __device__ __forceinline__ bool chunk_precond(const IccgArgs &A, WinStream<T> &w
         for (int k = threadIdx.x; k < nl; k += blockDim.x) rs[k] = (T)A.r[__ldg(A.pl.srow + s0 + k)];
         __syncthreads();
     }
-    bool alive = true;
     trace_mark(A.trace, 56);
-    for (int i = 0; i < ws.total(); i++) {
-        const unsigned char *buf;
-        int nint;
-        if (!ws.acquire(i, A.spin_limit, A.st, buf, nint)) return false;
-        if (i < ws.ctl->n0) {
-            const WalkIO<T, double, false, STG> lo{xs, yg, A.r, rs, 0, 0, 1};
-            alive = walk_window<T, double, false, false, STG, sizeof(T) == 8>(buf, nint, lo, w, alive);
-            if (i == ws.ctl->n0 - 1) trace_mark(A.trace, 57);
-        } else {
-            const WalkIO<T, T, false, STG> up{xs, zg, yg, rs, 0, 0, 1};
-            alive = walk_window<T, T, true, false, STG, sizeof(T) == 8>(buf, nint, up, w, alive);
-        }
-        ws.release(i);
-        if (__syncthreads_or(!alive)) return false;
+    const int n0 = ws.ctl->n0;
+    {
+        const WalkIO<T, double, false, STG> lo{xs, yg, A.r, rs, 0, 0, 1};
+        if (!walk_dir<T, double, false, false, STG, sizeof(T) == 8>(ws, 0, n0, lo, w, A.spin_limit, A.st)) return false;
+    }
+    trace_mark(A.trace, 57);
+    {
+        const WalkIO<T, T, false, STG> up{xs, zg, yg, rs, 0, 0, 1};
+        if (!walk_dir<T, T, true, false, STG, sizeof(T) == 8>(ws, n0, ws.total(), up, w, A.spin_limit, A.st)) return false;
     }
     for (int k = threadIdx.x; k < nl; k += blockDim.x) {
         const int row = __ldg(A.pl.srow + s0 + k);
@@ -606,11 +662,13 @@ __device__ __forceinline__ void pack_factor(const ChunkDir &D, const double *lu,
     const int vb = __ldg(D.cval + blockIdx.x), ve = __ldg(D.cval + blockIdx.x + 1);
     for (int i = vb + (int)threadIdx.x; i < ve; i += blockDim.x) {
         const int s = __ldg(D.vsrcA + i);
-        const double v = s >= 0 ? ld_l2(lu + s) : (s <= -2 ? ld_l2(lu + (-2 - s)) : 0.0);
+        const bool rcp = s < -(1 << 30), dg = s <= -2 && !rcp;
+        const int src = s >= 0 ? s : (rcp ? s - kRcpBase : (dg ? -2 - s : -1));
+        const double v = src >= 0 ? ld_l2(lu + src) : 0.0;
         if constexpr (sizeof(T) == 4)
-            g32[i] = s <= -2 ? __frcp_rn(__double2float_rn(v)) : __double2float_rn(v);
+            g32[i] = (dg || rcp) ? __frcp_rn(__double2float_rn(v)) : __double2float_rn(v);
         else
-            g64[i] = v;
+            g64[i] = rcp ? div_recip(v) : v;
     }
 }
 

@@ -160,6 +160,12 @@ baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row);
 baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget, int upper, const double *tval,
                                     const double *b, double *x);
 
+/* Division test hook (no counterpart in the reference): for i < n, q[i] = the FP64 sweep's
+ * quotient a[i] / b[i] (mode 0: from the stored reciprocal RN(1/b[i]) with Markstein's correction,
+ * as the sweeps compute it; mode 1: the IEEE correctly rounded division) on device arrays a, b, q
+ * of n doubles. Synchronises `stream` to read the status. */
+baas_status baas_test_divide(const double *a, const double *b, double *q, long long n, int mode, void *stream);
+
 /* Forward sweep x = L^-1 b (upper = 0; L is the analysed lower triangle, diagonal LAST in each
  * row) or backward sweep x = U^-1 b (upper = 1; U has the transposed pattern, diagonal FIRST).
  * Replaces Scheduler::runForwardTRSVNoPerm / runBackwardTRSVNoPerm (test/Schedule.hpp:332-347),
