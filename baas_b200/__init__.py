@@ -18,13 +18,14 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native
-from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, PARTITION_BAAS_THREADS, PARTITION_RANGES,
+from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
+                      PARTITION_RANGES,
                       PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
 
 __all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV",
            "KERNEL_ICCG", "KERNEL_IC0", "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "PARTITION_RANGES",
-           "PARTITION_BAAS_THREADS", "version"]
+           "PARTITION_BAAS_THREADS", "PARTITION_CUSTOM", "version"]
 
 
 def version() -> str:
@@ -134,6 +135,17 @@ class Schedule:
         opt.partition = partition
         opt.spin_limit = spin_limit
         _native.check(_native.lib().baas_replan(self._h, C.byref(opt)), "baas_replan")
+
+    def replan_custom(self, row_part, parts: int | None = None, smem_budget: int = 0) -> None:
+        """Rebuild the device plan with row i owned by CTA row_part[i] (baas_replan_custom); parts
+        defaults to max(row_part) + 1."""
+        rp = np.ascontiguousarray(row_part, dtype=np.int32)
+        if rp.shape != (self.n,):
+            raise ValueError("row_part needs one entry per row")
+        if parts is None:
+            parts = int(rp.max()) + 1
+        _native.check(_native.lib().baas_replan_custom(self._h, _ptr(rp), int(parts), int(smem_budget)),
+                      "baas_replan_custom")
 
     def emulate_sweep(self, T: CSR, b: np.ndarray, upper: bool = False, parts: int = 0,
                       smem_budget: int = 0) -> np.ndarray:

@@ -25,7 +25,7 @@ STATUS_NAMES = {
 
 KERNEL_SPTRSV, KERNEL_ICCG, KERNEL_IC0, KERNEL_ILU0 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32_FACTORS = 0, 1
-PARTITION_RANGES, PARTITION_BAAS_THREADS = 0, 1
+PARTITION_RANGES, PARTITION_BAAS_THREADS, PARTITION_CUSTOM = 0, 1, 2
 
 FIELDS = {
     "ngroups": 0, "nlevels": 1, "ntasks": 2, "group_ptr": 3, "group_set": 4, "level_ptr": 5,
@@ -38,7 +38,7 @@ FIELDS = {
 EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
-    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan", "baas_test_divide",
+    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan", "baas_test_divide", "baas_replan_custom",
 ]
 
 
@@ -113,6 +113,8 @@ def lib():
     L.baas_test_emulate_sweep.restype = i
     L.baas_test_divide.argtypes = [vp, vp, vp, C.c_longlong, i, vp]
     L.baas_test_divide.restype = i
+    L.baas_replan_custom.argtypes = [vp, vp, i, i]
+    L.baas_replan_custom.restype = i
     _lib = L
     return L
 

@@ -181,6 +181,7 @@ struct baas_schedule {
     // partition (built at first GPU use, when the SM count is known)
     int P = 0;
     std::vector<int> group_cta, row_cta;
+    std::vector<int> custom_part;  // BAAS_PARTITION_CUSTOM: the caller's row -> CTA map
     PartHost fwd, bwd;
     ChunkHost chk;
     int fault_row = -1;  // test hook: forward row made to wait on its own output
@@ -266,7 +267,9 @@ void build_partition(baas_schedule *s, int P) {
     const int n = h.n;
     s->P = P;
     s->group_cta.assign(h.ngroups, 0);
-    if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) {
+    if (s->opt.partition == BAAS_PARTITION_CUSTOM) {
+        for (int g = 0; g < h.ngroups; g++) s->group_cta[g] = s->custom_part[h.group_set[h.group_ptr[g]]];
+    } else if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) {
         for (int t = 0; t < h.nthread; t++)
             for (int task = h.thread_boundaries[t]; task < h.thread_boundaries[t + 1]; task++)
                 for (int q = h.task_boundaries[task]; q < h.task_boundaries[task + 1]; q++) s->group_cta[h.thread_cont_to_orig[q]] = t;
@@ -634,6 +637,8 @@ baas_status ensure_device(baas_schedule *s) {
     if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) {
         P = s->hs.nthread;
         if (s->opt.parts > 0 && s->opt.parts != P) return fail(BAAS_ERR_BAD_ARG, "BAAS_THREADS partition needs parts == nthread");
+    } else if (s->opt.partition == BAAS_PARTITION_CUSTOM) {
+        P = s->opt.parts;
     } else if (s->opt.parts > 0) {
         P = std::min(s->opt.parts, n);
     } else {
@@ -881,6 +886,7 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
     const int n = s->hs.n;
     int P = parts > 0 ? std::min(parts, n) : std::max(1, std::min({(n + 2047) / 2048, 128, 148}));
     if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) P = s->hs.nthread;
+    if (s->opt.partition == BAAS_PARTITION_CUSTOM) P = s->opt.parts;
     build_partition(s, P);
     build_dir(s, false, s->fwd);
     build_dir(s, true, s->bwd);
@@ -1068,6 +1074,7 @@ static void release_device(baas_schedule *s) {
     fresh.fault_row = s->fault_row;
     fresh.sys_off = std::move(s->sys_off);
     fresh.nsys = s->nsys;
+    fresh.custom_part = std::move(s->custom_part);
     *s = std::move(fresh);
 }
 
@@ -1081,10 +1088,29 @@ baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
     if (!s || !opt) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     if (opt->nthread != s->hs.nthread) return fail(BAAS_ERR_BAD_ARG, "nthread is fixed by the analysis");
     if (opt->parts < 0 || opt->smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "parts and smem_budget must be >= 0");
-    if (opt->partition != BAAS_PARTITION_RANGES && opt->partition != BAAS_PARTITION_BAAS_THREADS)
+    if (opt->partition == BAAS_PARTITION_CUSTOM) {
+        if (s->custom_part.empty()) return fail(BAAS_ERR_BAD_ARG, "no custom partition: use baas_replan_custom");
+        if (opt->parts != s->opt.parts) return fail(BAAS_ERR_BAD_ARG, "a custom partition fixes parts");
+    } else if (opt->partition != BAAS_PARTITION_RANGES && opt->partition != BAAS_PARTITION_BAAS_THREADS) {
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
+    }
     release_device(s);
     s->opt = *opt;
+    return BAAS_OK;
+}
+
+baas_status baas_replan_custom(baas_schedule *s, const int *row_part, int parts, int smem_budget) {
+    if (!s || !row_part) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    if (parts < 1) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 1");
+    if (smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
+    const int n = s->hs.n;
+    for (int i = 0; i < n; i++)
+        if (row_part[i] < 0 || row_part[i] >= parts) return fail(BAAS_ERR_BAD_ARG, "row_part out of [0, parts)");
+    release_device(s);
+    s->custom_part.assign(row_part, row_part + n);
+    s->opt.partition = BAAS_PARTITION_CUSTOM;
+    s->opt.parts = parts;
+    s->opt.smem_budget = smem_budget;
     return BAAS_OK;
 }
 

@@ -256,29 +256,37 @@ __device__ __forceinline__ double div_rcp(double a, double b, double y) {
 // so they keep their order relative to one another and to barriers; no "memory" clobber, so
 // they do not serialise the surrounding code.
 template <typename T> struct Sh;
+// ldu / stu take 32-bit shared-window addresses, so address arithmetic stays in 32 bits: one
+// integer add per access instead of a 64-bit generic address and its conversion.
 template <> struct Sh<int> {
-    static __device__ __forceinline__ int ld(const int *p) {
+    static __device__ __forceinline__ int ldu(unsigned int a) {
         int v;
-        asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)));
+        asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(a));
         return v;
     }
-    static __device__ __forceinline__ void st(int *p, int v) { asm volatile("st.shared.s32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v)); }
+    static __device__ __forceinline__ void stu(unsigned int a, int v) { asm volatile("st.shared.s32 [%0], %1;" ::"r"(a), "r"(v)); }
+    static __device__ __forceinline__ int ld(const int *p) { return ldu(smem_u32(p)); }
+    static __device__ __forceinline__ void st(int *p, int v) { stu(smem_u32(p), v); }
 };
 template <> struct Sh<float> {
-    static __device__ __forceinline__ float ld(const float *p) {
+    static __device__ __forceinline__ float ldu(unsigned int a) {
         float v;
-        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(smem_u32(p)));
+        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
         return v;
     }
-    static __device__ __forceinline__ void st(float *p, float v) { asm volatile("st.shared.f32 [%0], %1;" ::"r"(smem_u32(p)), "f"(v)); }
+    static __device__ __forceinline__ void stu(unsigned int a, float v) { asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v)); }
+    static __device__ __forceinline__ float ld(const float *p) { return ldu(smem_u32(p)); }
+    static __device__ __forceinline__ void st(float *p, float v) { stu(smem_u32(p), v); }
 };
 template <> struct Sh<double> {
-    static __device__ __forceinline__ double ld(const double *p) {
+    static __device__ __forceinline__ double ldu(unsigned int a) {
         double v;
-        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
         return v;
     }
-    static __device__ __forceinline__ void st(double *p, double v) { asm volatile("st.shared.f64 [%0], %1;" ::"r"(smem_u32(p)), "d"(v)); }
+    static __device__ __forceinline__ void stu(unsigned int a, double v) { asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v)); }
+    static __device__ __forceinline__ double ld(const double *p) { return ldu(smem_u32(p)); }
+    static __device__ __forceinline__ void st(double *p, double v) { stu(smem_u32(p), v); }
 };
 
 // Phase tracing (BAAS_TRACE=1): thread 0 of the first and last CTA record %globaltimer (ns)

@@ -238,6 +238,9 @@ struct WalkIO {
     __device__ T *out() const { return MR ? xg + (size_t)rr() * ldx : xg; }
     __device__ const RT *in() const { return MR ? rhs + (size_t)rr() * ldr : rhs; }
     __device__ int slot(int sl) const { return MR ? sl * R_ + rr() : sl; }
+    // shared-window addresses of slot / staged entry k (as io.slot indexes them)
+    __device__ unsigned int xs_at(int k) const { return smem_u32(xs) + (unsigned int)k * (unsigned int)sizeof(T); }
+    __device__ unsigned int rs_at(int k) const { return smem_u32(rs) + (unsigned int)k * (unsigned int)sizeof(T); }
 };
 
 // Dependency indices, entry count, row and staging position of one row: loaded one step
@@ -255,28 +258,30 @@ struct RowVals {
     T diag, rcp, rhs;
 };
 
+// I, V: shared-window addresses of the chunk's int block and value block.
 template <int EK>
-__device__ __forceinline__ void load_deps(const int *I, int nl, int pos, RowDeps<EK> &p) {
-    const int *rowid = I + kChunkHdr;
-    p.row = Sh<int>::ld(rowid + pos);
-    p.ne = Sh<int>::ld(rowid + 2 * nl + pos);
-    p.kpos = Sh<int>::ld(rowid + 3 * nl + pos);
-    const int *dp = rowid + 4 * nl + pos * EK;
+__device__ __forceinline__ void load_deps(unsigned int I, int nl, int pos, RowDeps<EK> &p) {
+    const unsigned int r = I + 4u * (unsigned int)(kChunkHdr + pos), n4 = 4u * (unsigned int)nl;
+    p.row = Sh<int>::ldu(r);
+    p.ne = Sh<int>::ldu(r + 2u * n4);
+    p.kpos = Sh<int>::ldu(r + 3u * n4);
+    const unsigned int dp = I + 4u * (unsigned int)(kChunkHdr + 4 * nl + pos * EK);
 #pragma unroll
-    for (int j = 0; j < EK; j++) p.d[j] = Sh<int>::ld(dp + j);
+    for (int j = 0; j < EK; j++) p.d[j] = Sh<int>::ldu(dp + 4u * j);
 }
 
 // The rest of a row's plan, and its staged right-hand side (STG).
 template <typename T, typename RT, bool RL2, bool MR, bool STG, int EK>
-__device__ __forceinline__ void load_vals(const int *I, const T *V, int nl, int pos, const RowDeps<EK> &p,
+__device__ __forceinline__ void load_vals(unsigned int I, unsigned int V, int nl, int pos, const RowDeps<EK> &p,
                                           const WalkIO<T, RT, MR, STG> &io, RowVals<T, EK> &v) {
-    v.sl = Sh<int>::ld(I + kChunkHdr + nl + pos);
-    const T *vp = V + 2 * nl + pos * EK;
+    constexpr unsigned int S = sizeof(T);
+    v.sl = Sh<int>::ldu(I + 4u * (unsigned int)(kChunkHdr + nl + pos));
+    const unsigned int vp = V + S * (unsigned int)(2 * nl + pos * EK);
 #pragma unroll
-    for (int j = 0; j < EK; j++) v.a[j] = Sh<T>::ld(vp + j);
-    v.diag = Sh<T>::ld(V + pos);
-    if constexpr (sizeof(T) == 8) v.rcp = Sh<T>::ld(V + nl + pos);
-    if constexpr (STG) v.rhs = Sh<T>::ld(io.rs + io.slot(p.kpos));
+    for (int j = 0; j < EK; j++) v.a[j] = Sh<T>::ldu(vp + S * j);
+    v.diag = Sh<T>::ldu(V + S * (unsigned int)pos);
+    if constexpr (sizeof(T) == 8) v.rcp = Sh<T>::ldu(V + S * (unsigned int)(nl + pos));
+    if constexpr (STG) v.rhs = Sh<T>::ldu(io.rs_at(io.slot(p.kpos)));
 }
 
 // A row's right-hand side: staged in shared memory, or from global memory (RL2: written
@@ -284,7 +289,7 @@ __device__ __forceinline__ void load_vals(const int *I, const T *V, int nl, int 
 template <typename T, typename RT, bool RL2, bool MR, bool STG>
 __device__ __forceinline__ T load_rhs(int row, int kpos, const WalkIO<T, RT, MR, STG> &io) {
     if constexpr (STG) {
-        return Sh<T>::ld(io.rs + io.slot(kpos));
+        return Sh<T>::ldu(io.rs_at(io.slot(kpos)));
     } else {
         const RT *src = io.in() + row;
         if constexpr (RL2)
@@ -325,7 +330,7 @@ __device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<
 #pragma unroll
     for (int j = 0; j < EK; j++) {
         const int dj = p.d[j];
-        const T loc = Sh<T>::ld(io.xs + io.slot(dj >= 0 ? dj : 0));
+        const T loc = Sh<T>::ldu(io.xs_at(io.slot(dj >= 0 ? dj : 0)));
         xv[j] = dj >= 0 ? loc : pf[j];
         miss |= j < p.ne && dj < 0 && Sent<T>::is(pf[j]);
     }
@@ -349,8 +354,8 @@ __device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<
         o = div_rcp(__dsub_rn(v.rhs, sum), v.diag, v.rcp);
     else
         o = (v.rhs - sum) * v.diag;  // FP32 value blocks hold 1/diag
-    if (v.sl >= 0) Sh<T>::st(io.xs + io.slot(v.sl), o);
-    if constexpr (STG) Sh<T>::st(io.rs + io.slot(p.kpos), o);
+    if (v.sl >= 0) Sh<T>::stu(io.xs_at(io.slot(v.sl)), o);
+    if constexpr (STG) Sh<T>::stu(io.rs_at(io.slot(p.kpos)), o);
     Sent<T>::store(xg + p.row, o);
     return true;
 }
@@ -369,12 +374,13 @@ template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT, int 
 __device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsigned char *buf, int nint,
                                            const WalkIO<T, RT, MR, STG> &io, Waiter &w, unsigned int spin,
                                            DevStatus *st) {
+    constexpr unsigned int S = sizeof(T);
     const int lr = io.lane_row(), stp = io.stride();
-    const int *I0 = reinterpret_cast<const int *>(buf);
-    const int *Iend = I0 + nint;
-    const T *V0 = reinterpret_cast<const T *>(buf + (size_t)nint * 4);
+    unsigned int I0 = smem_u32(buf);
+    unsigned int Iend = I0 + 4u * (unsigned int)nint;
+    unsigned int V0 = Iend;  // the value blocks follow the int blocks
     bool alive = true;
-    int nl0 = Sh<int>::ld(I0);
+    int nl0 = Sh<int>::ldu(I0);
     RowDeps<EK> q0, q1;
     T pf0[EK];
     T rhs0 = T(0), rhs1 = T(0);
@@ -385,19 +391,19 @@ __device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsig
         if constexpr (!STG) rhs0 = load_rhs<T, RT, RL2, MR, STG>(q0.row, q0.kpos, io);
     }
     for (;;) {
-        const int nl1 = Sh<int>::ld(I0 + 2);  // 0 after the direction's last chunk
-        const int *I1 = I0 + chunk_nint(nl0, EK);
-        const T *V1 = V0 + chunk_nval(nl0, EK);
-        const int *Iend1 = Iend;
+        const int nl1 = Sh<int>::ldu(I0 + 8u);  // 0 after the direction's last chunk
+        unsigned int I1 = I0 + 4u * (unsigned int)chunk_nint(nl0, EK);
+        unsigned int V1 = V0 + S * (unsigned int)chunk_nval(nl0, EK);
+        unsigned int Iend1 = Iend;
         const bool cross = nl1 != 0 && I1 == Iend;  // uniform: step s+1 opens the next window
         bool okw = true;
         if (cross) {
             const unsigned char *nb;
             int nn;
             okw = ws.peek(i, spin, nb, nn);
-            I1 = reinterpret_cast<const int *>(nb);
-            Iend1 = I1 + nn;
-            V1 = reinterpret_cast<const T *>(nb + (size_t)nn * 4);
+            I1 = smem_u32(nb);
+            Iend1 = I1 + 4u * (unsigned int)nn;
+            V1 = Iend1;
         }
         const bool m1 = okw && lr < nl1;
         if (m1) load_deps<EK>(I1, nl1, lr, q1);

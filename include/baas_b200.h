@@ -104,15 +104,18 @@ typedef struct baas_options {
     int spin_limit;   /* polls before a device wait gives up (0 = library default) */
     int parts;        /* CTAs that own rows in the partitioned kernels (0 = automatic: about one
                          per 2,048 rows, at most 128 and at most one per SM) */
-    int partition;    /* BAAS_PARTITION_RANGES (default) or BAAS_PARTITION_BAAS_THREADS */
+    int partition;    /* BAAS_PARTITION_RANGES (default), BAAS_PARTITION_BAAS_THREADS, or
+                         BAAS_PARTITION_CUSTOM (set by baas_replan_custom only) */
     int smem_budget;  /* bytes of shared memory per CTA for solution slots and the two plan
                          window buffers (0 = library default, 220 KiB; at most 224 KiB) */
 } baas_options;
 
 /* How rows are given to CTAs. RANGES: contiguous row-index ranges, so every cross-CTA
- * dependency of the lower sweep points to a later CTA. BAAS_THREADS: CTA t runs the groups the
- * four-rule mapping gives virtual thread t (requires parts == nthread or parts == 0). */
-enum { BAAS_PARTITION_RANGES = 0, BAAS_PARTITION_BAAS_THREADS = 1 };
+ * dependency of the lower sweep points to an earlier CTA. BAAS_THREADS: CTA t runs the groups the
+ * four-rule mapping gives virtual thread t (requires parts == nthread or parts == 0). CUSTOM: a
+ * caller's row-to-CTA map (baas_replan_custom). Any partition is deadlock-free: every CTA walks
+ * its rows in level order and a row only waits on rows of lower levels. */
+enum { BAAS_PARTITION_RANGES = 0, BAAS_PARTITION_BAAS_THREADS = 1, BAAS_PARTITION_CUSTOM = 2 };
 
 typedef struct baas_schedule baas_schedule;
 
@@ -142,6 +145,13 @@ void baas_destroy(baas_schedule *s);
  * device plan and workspaces are freed and built again at the next GPU call. Used by the
  * autotuner (baas_b200/autotune.py). No counterpart in the reference. */
 baas_status baas_replan(baas_schedule *s, const baas_options *opt);
+
+/* Alternate mapper (no counterpart in the reference, whose OpenMP threads are its partition):
+ * rebuilds the device plan with row i owned by CTA row_part[i], 0 <= row_part[i] < parts; a
+ * coarsened group goes with the CTA of its first row. parts must not exceed the device's SMs
+ * (checked at the next GPU call). smem_budget as in baas_options. Like baas_replan, frees the
+ * device plan; later baas_replan calls keep the map while partition stays CUSTOM. */
+baas_status baas_replan_custom(baas_schedule *s, const int *row_part, int parts, int smem_budget);
 
 /* Failure-detection test hook (no counterpart in the reference, whose waits never end):
  * makes the forward sweep's row `row` wait on a value that nothing ever writes, so the next

@@ -93,3 +93,47 @@ def test_liveness_slots_let_one_cta_stream_a_large_plan():
     assert np.array_equal(s.emulate_sweep(Lo, r, parts=1, smem_budget=40 * 1024), Port.lower_solve(Lo, r))
     assert np.array_equal(s.emulate_sweep(Up, r, upper=True, parts=1, smem_budget=40 * 1024),
                           Port.upper_solve(Up, r, descending=True))
+
+
+def _column_blocks(k, bi, bj):
+    """Row (i, j, l) of a k^3 grid (row = i + k*j + k*k*l) to the CTA of its (i // bi, j // bj)
+    block of grid columns."""
+    r = np.arange(k ** 3)
+    i, j = r % k, (r // k) % k
+    return (i // bi + ((k + bi - 1) // bi) * (j // bj)).astype(np.int32)
+
+
+@pytest.mark.parametrize("budget", [24 * 1024, 0])
+def test_custom_partition_plan(budget):
+    """A caller's row-to-CTA map (baas_replan_custom): blocks of grid columns, so cross-CTA
+    dependencies point both ways between CTAs."""
+    A = gen.laplace3d(14, 1e-3)
+    Lo, Up = _ic_lu(A)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    rp = _column_blocks(14, 4, 5)
+    s.replan_custom(rp, smem_budget=budget)
+    r = gen.uniform_rhs(A.n, 1)
+    assert np.array_equal(s.emulate_sweep(Lo, r, smem_budget=budget), Port.lower_solve(Lo, r))
+    assert np.array_equal(s.emulate_sweep(Up, r, upper=True, smem_budget=budget),
+                          Port.upper_solve(Up, r, descending=True))
+
+
+def test_custom_partition_checks():
+    from baas_b200 import PARTITION_CUSTOM, BaasError
+
+    A = gen.laplace3d(6, 1e-3)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=4)
+    rp = np.zeros(A.n, dtype=np.int32)
+    rp[::2] = 3
+    with pytest.raises(BaasError):
+        s.replan_custom(rp, parts=3)  # entries out of [0, parts)
+    with pytest.raises(ValueError):
+        s.replan_custom(rp[:-1])
+    with pytest.raises(BaasError):
+        s.replan(partition=PARTITION_CUSTOM)  # no map stored yet
+    s.replan_custom(rp)  # parts = 4, CTAs 1 and 2 own no rows
+    Lo, _ = _ic_lu(A)
+    b = gen.uniform_rhs(A.n, 3)
+    assert np.array_equal(s.emulate_sweep(Lo, b), Port.lower_solve(Lo, b))
+    s.replan(parts=4, partition=PARTITION_CUSTOM)  # keeps the map
+    assert np.array_equal(s.emulate_sweep(Lo, b), Port.lower_solve(Lo, b))
