@@ -215,6 +215,9 @@ struct baas_schedule {
     double *d_relres = nullptr;
 
     unsigned long long *d_trace = nullptr;  // BAAS_TRACE=1: phase timestamps of the last launch
+    // the initial guess of an FP64 ICCG launch, kept for its repeat with IEEE divisions
+    double *d_x0 = nullptr;
+    size_t x0_cap = 0;
 
     // batched systems (baas_analyze_batch): row offsets of the systems, and the vector-phase
     // decomposition (built at the first batched solve)
@@ -615,6 +618,43 @@ constexpr int kMaxSmemBudget = 224 * 1024;
 // kernels' static shared memory
 constexpr int kMaxDynSmem = 227 * 1024 - 2048;
 
+// The launched variants. ieee: sweep divisions by __ddiv_rn, for the repeat of a launch whose
+// div_fast divisions left their range (DevStatus::slow_div); FP32 factors never divide.
+void *sweep_kernel(bool mr, bool stg, bool ieee) {
+    if (ieee)
+        return mr ? (stg ? (void *)baas::k_sweep_chunked<true, true, true> : (void *)baas::k_sweep_chunked<true, false, true>)
+                  : (stg ? (void *)baas::k_sweep_chunked<false, true, true> : (void *)baas::k_sweep_chunked<false, false, true>);
+    return mr ? (stg ? (void *)baas::k_sweep_chunked<true, true, false> : (void *)baas::k_sweep_chunked<true, false, false>)
+              : (stg ? (void *)baas::k_sweep_chunked<false, true, false> : (void *)baas::k_sweep_chunked<false, false, false>);
+}
+void *iccg_kernel(bool mixed, bool stg, bool ieee) {
+    if (mixed) return stg ? (void *)baas::k_iccg_chunked<float, true, false> : (void *)baas::k_iccg_chunked<float, false, false>;
+    if (ieee) return stg ? (void *)baas::k_iccg_chunked<double, true, true> : (void *)baas::k_iccg_chunked<double, false, true>;
+    return stg ? (void *)baas::k_iccg_chunked<double, true, false> : (void *)baas::k_iccg_chunked<double, false, false>;
+}
+void *batched_kernel(bool mixed, bool mr, bool ieee) {
+    if (mixed) return mr ? (void *)baas::k_iccg_batched<float, true, false> : (void *)baas::k_iccg_batched<float, false, false>;
+    if (ieee) return mr ? (void *)baas::k_iccg_batched<double, true, true> : (void *)baas::k_iccg_batched<double, false, true>;
+    return mr ? (void *)baas::k_iccg_batched<double, true, false> : (void *)baas::k_iccg_batched<double, false, false>;
+}
+
+// Keeps `count` doubles from src (device) for a repeat of the launch.
+baas_status save_x0(baas_schedule *s, const double *src, size_t count, cudaStream_t stream) {
+    if (count > s->x0_cap) {
+        if (s->d_x0) cudaFree(s->d_x0);
+        s->d_x0 = nullptr;
+        s->x0_cap = 0;
+        BAAS_CUDA(cudaMalloc((void **)&s->d_x0, count * sizeof(double)));
+        s->x0_cap = count;
+    }
+    BAAS_CUDA(cudaMemcpyAsync(s->d_x0, src, count * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    return BAAS_OK;
+}
+
+// After read_status: the launch ran without a device error but some div_fast division left its
+// range, so it must be repeated with the IEEE variant.
+bool needs_ieee_repeat(const baas_schedule *s) { return s->h_status->code == 0 && s->h_status->slow_div != 0; }
+
 baas_status ensure_device(baas_schedule *s) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -660,14 +700,12 @@ baas_status ensure_device(baas_schedule *s) {
     BAAS_CUDA(cudaMallocHost((void **)&s->h_status, sizeof(DevStatus)));
     if (getenv("BAAS_TRACE") && atoi(getenv("BAAS_TRACE")) > 0) BAAS_TRY(dalloc(s->d_trace, 2 * baas::kTraceSlots));
     {
-        const void *kerns[] = {(const void *)baas::k_sweep_chunked<false, false>, (const void *)baas::k_sweep_chunked<false, true>,
-                               (const void *)baas::k_sweep_chunked<true, false>, (const void *)baas::k_sweep_chunked<true, true>,
-                               (const void *)baas::k_iccg_chunked<double, false>, (const void *)baas::k_iccg_chunked<double, true>,
-                               (const void *)baas::k_iccg_chunked<float, false>, (const void *)baas::k_iccg_chunked<float, true>,
-                               (const void *)baas::k_iccg_batched<double, false>, (const void *)baas::k_iccg_batched<double, true>,
-                               (const void *)baas::k_iccg_batched<float, false>, (const void *)baas::k_iccg_batched<float, true>};
-        for (const void *k : kerns)
-            BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+        for (int v = 0; v < 8; v++) {
+            const bool a = v & 1, b = v & 2, c = v & 4;
+            const void *kerns[] = {sweep_kernel(a, b, c), iccg_kernel(a, b, c), batched_kernel(a, b, c)};
+            for (const void *k : kerns)
+                BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+        }
     }
     s->uploaded = true;
     // the single-right-hand-side FP64 windows must exist for every kind of call
@@ -862,14 +900,20 @@ namespace {
 __global__ void k_test_divide(const double *a, const double *b, double *q, long long n, int mode) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double x = a[i], d = b[i];
-        q[i] = mode == 0 ? baas::div_rcp(x, d, baas::div_recip(d)) : __ddiv_rn(x, d);
+        if (mode == 2) {
+            bool slow = false;
+            baas::div_fast(x, d, baas::div_recip(d), slow);
+            q[i] = slow ? 1.0 : 0.0;
+        } else {
+            q[i] = mode == 0 ? baas::div_rcp(x, d, baas::div_recip(d)) : __ddiv_rn(x, d);
+        }
     }
 }
 }  // namespace
 
 baas_status baas_test_divide(const double *a, const double *b, double *q, long long n, int mode, void *stream) {
     if (n < 0 || (n > 0 && (!a || !b || !q))) return fail(BAAS_ERR_BAD_ARG, "NULL argument or negative n");
-    if (mode != 0 && mode != 1) return fail(BAAS_ERR_BAD_ARG, "mode must be 0 or 1");
+    if (mode < 0 || mode > 2) return fail(BAAS_ERR_BAD_ARG, "mode must be 0, 1 or 2");
     if (n == 0) return BAAS_OK;
     cudaStream_t st = (cudaStream_t)stream;
     const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 16);
@@ -1050,7 +1094,7 @@ static void release_device(baas_schedule *s) {
             if (s->d_gvT[d]) cudaFree(s->d_gvT[d]);
         }
         void *ptrs[] = {s->d_a_diag, s->d_status, s->d_flags, s->d_bar, s->d_lu, s->d_r, s->d_y, s->d_z, s->d_p,
-                        s->d_Ap, s->d_y32, s->d_z32, s->d_part, s->d_iters, s->d_relres};
+                        s->d_Ap, s->d_y32, s->d_z32, s->d_part, s->d_iters, s->d_relres, s->d_x0};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         if (s->h_status) cudaFreeHost(s->h_status);
@@ -1129,23 +1173,24 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
     WinCfg *w = nullptr;
     BAAS_TRY(get_windows(s, 8, R, &w));
     if (!s->d_gvT[d]) BAAS_TRY(dalloc(s->d_gvT[d], s->chk.dir[d].vsrcT.size()));
-    BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-    {
-        const int fill_blocks = (int)std::min<long long>(4LL * s->num_sms, ((long long)n * nrhs + 255) / 256);
-        baas::k_fill_sentinel<double><<<std::max(fill_blocks, 1), 256, 0, stream>>>(x, n, nrhs, ldb);
-        BAAS_CUDA(cudaGetLastError());
-    }
     baas::ChunkPlan pl = chunk_plan(s, *w);
     unsigned int spin = s->spin();
     double *gv = s->d_gvT[d];
     void *args[] = {(void *)&pl, (void *)&d, (void *)&T->values, (void *)&gv, (void *)&b, (void *)&ldb, (void *)&x,
                     (void *)&ldb, (void *)&nrhs, (void *)&R, (void *)&s->d_status, (void *)&spin, (void *)&s->d_trace};
     const bool stg = w->rhs_bytes > 0;
-    void *kern = R > 1 ? (stg ? (void *)baas::k_sweep_chunked<true, true> : (void *)baas::k_sweep_chunked<true, false>)
-                       : (stg ? (void *)baas::k_sweep_chunked<false, true> : (void *)baas::k_sweep_chunked<false, false>);
-    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, s->P, baas::kStageBlock, args, w->smem, stream));
-    dump_trace(s, upper ? "sptrsv-upper" : "sptrsv-lower", stream);
-    return read_status(s, stream);
+    for (int ieee = 0; ieee < 2; ieee++) {
+        BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+        const int fill_blocks = (int)std::min<long long>(4LL * s->num_sms, ((long long)n * nrhs + 255) / 256);
+        baas::k_fill_sentinel<double><<<std::max(fill_blocks, 1), 256, 0, stream>>>(x, n, nrhs, ldb);
+        BAAS_CUDA(cudaGetLastError());
+        BAAS_CUDA(cudaLaunchCooperativeKernel(sweep_kernel(R > 1, stg, ieee != 0), s->P, baas::kStageBlock, args, w->smem,
+                                              stream));
+        dump_trace(s, upper ? "sptrsv-upper" : "sptrsv-lower", stream);
+        const baas_status st = read_status(s, stream);
+        if (!needs_ieee_repeat(s)) return st;
+    }
+    return fail(BAAS_ERR_CUDA, "IEEE sweep reported a fast-path division");
 }
 
 static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void *stream_, bool ilu) {
@@ -1336,11 +1381,9 @@ baas_status baas_iccg_batched(baas_schedule *s, const baas_csr *A, const double 
     BAAS_TRY(batch_setup(s, nrhs));
     cudaStream_t stream = (cudaStream_t)stream_;
     const int P = s->P;
-    BAAS_TRY(next_epoch(s, stream));
-    BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-    BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
     const unsigned int active = (unsigned int)(s->nsys * nrhs);
-    BAAS_CUDA(cudaMemcpyAsync(s->d_active, &active, sizeof(active), cudaMemcpyHostToDevice, stream));
+    const size_t xcount = (size_t)(nrhs - 1) * (size_t)ldb + (size_t)n;
+    if (!mixed) BAAS_TRY(save_x0(s, X, xcount, stream));
 
     baas::BatchArgs a{};
     a.n = n;
@@ -1360,7 +1403,6 @@ baas_status baas_iccg_batched(baas_schedule *s, const baas_csr *A, const double 
     }
     a.lu = s->d_blu;
     a.gflag = s->d_flags;
-    a.epoch = s->epoch;
     a.r = s->d_br;
     a.p = s->d_bp;
     a.Ap = s->d_bAp;
@@ -1382,12 +1424,21 @@ baas_status baas_iccg_batched(baas_schedule *s, const baas_csr *A, const double 
     if (smem > (size_t)kMaxDynSmem) return fail(BAAS_ERR_BAD_ARG, "batched solve: shared memory over budget");
     void *args[] = {(void *)&a};
     const bool mr = nrhs > 1;
-    void *kern = mixed ? (mr ? (void *)baas::k_iccg_batched<float, true> : (void *)baas::k_iccg_batched<float, false>)
-                       : (mr ? (void *)baas::k_iccg_batched<double, true> : (void *)baas::k_iccg_batched<double, false>);
-    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, P, baas::kStageBlock, args, smem, stream));
-    BAAS_CUDA(cudaMemcpyAsync(iters, s->d_biters, sizeof(int) * (size_t)s->nsys * nrhs, cudaMemcpyDeviceToHost, stream));
-    BAAS_CUDA(cudaMemcpyAsync(relres, s->d_brelres, sizeof(double) * (size_t)s->nsys * nrhs, cudaMemcpyDeviceToHost, stream));
-    BAAS_TRY(read_status(s, stream));
+    for (int ieee = 0; ieee < 2; ieee++) {
+        if (ieee) BAAS_CUDA(cudaMemcpyAsync(X, s->d_x0, sizeof(double) * xcount, cudaMemcpyDeviceToDevice, stream));
+        BAAS_TRY(next_epoch(s, stream));
+        a.epoch = s->epoch;
+        BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+        BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
+        BAAS_CUDA(cudaMemcpyAsync(s->d_active, &active, sizeof(active), cudaMemcpyHostToDevice, stream));
+        BAAS_CUDA(cudaLaunchCooperativeKernel(batched_kernel(mixed, mr, ieee != 0), P, baas::kStageBlock, args, smem, stream));
+        BAAS_CUDA(cudaMemcpyAsync(iters, s->d_biters, sizeof(int) * (size_t)s->nsys * nrhs, cudaMemcpyDeviceToHost, stream));
+        BAAS_CUDA(cudaMemcpyAsync(relres, s->d_brelres, sizeof(double) * (size_t)s->nsys * nrhs, cudaMemcpyDeviceToHost,
+                                  stream));
+        BAAS_TRY(read_status(s, stream));
+        if (!needs_ieee_repeat(s)) break;
+        if (ieee) return fail(BAAS_ERR_CUDA, "IEEE batched ICCG reported a fast-path division");
+    }
     for (int q = 0; q < s->nsys * nrhs; q++)
         if (!(relres[q] < tol)) return fail(BAAS_ERR_NOT_CONVERGED, "maxiter reached before tol for some instance");
     return BAAS_OK;
@@ -1423,13 +1474,10 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
         BAAS_TRY(dalloc(s->d_relres, 1));
         s->ws_ready = true;
     }
-    BAAS_TRY(next_epoch(s, stream));
-    BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-    BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
-
     const bool mixed = precision == BAAS_PREC_FP32_FACTORS;
     WinCfg *w = nullptr;
     BAAS_TRY(get_windows(s, mixed ? 4 : 8, 1, &w));
+    if (!mixed) BAAS_TRY(save_x0(s, x, (size_t)n, stream));
     baas::IccgArgs a{};
     a.n = n;
     a.a_rowptr = A->rowptr;
@@ -1446,7 +1494,6 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
     }
     a.lu = s->d_lu;
     a.gflag = s->d_flags;
-    a.epoch = s->epoch;
     a.r = s->d_r;
     a.y = s->d_y;
     a.z = s->d_z;
@@ -1470,15 +1517,23 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
     a.grad_a = grad_a;
     void *args[] = {(void *)&a};
     const bool stg = w->rhs_bytes > 0;
-    void *kern = mixed ? (stg ? (void *)baas::k_iccg_chunked<float, true> : (void *)baas::k_iccg_chunked<float, false>)
-                       : (stg ? (void *)baas::k_iccg_chunked<double, true> : (void *)baas::k_iccg_chunked<double, false>);
-    BAAS_CUDA(cudaLaunchCooperativeKernel(kern, P, baas::kStageBlock, args, w->smem, stream));
     int it = 0;
     double rr = 0.0;
-    BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    BAAS_CUDA(cudaMemcpyAsync(&rr, s->d_relres, sizeof(double), cudaMemcpyDeviceToHost, stream));
-    dump_trace(s, "iccg", stream);
-    baas_status st = read_status(s, stream);
+    baas_status st = BAAS_OK;
+    for (int ieee = 0; ieee < 2; ieee++) {
+        if (ieee) BAAS_CUDA(cudaMemcpyAsync(x, s->d_x0, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, stream));
+        BAAS_TRY(next_epoch(s, stream));
+        a.epoch = s->epoch;
+        BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+        BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
+        BAAS_CUDA(cudaLaunchCooperativeKernel(iccg_kernel(mixed, stg, ieee != 0), P, baas::kStageBlock, args, w->smem, stream));
+        BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        BAAS_CUDA(cudaMemcpyAsync(&rr, s->d_relres, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        dump_trace(s, "iccg", stream);
+        st = read_status(s, stream);
+        if (!needs_ieee_repeat(s)) break;
+        if (ieee) return fail(BAAS_ERR_CUDA, "IEEE ICCG reported a fast-path division");
+    }
     if (iters) *iters = it;
     if (relres) *relres = rr;
     if (!reuse) s->factor_prec = st == BAAS_OK || st == BAAS_ERR_NOT_CONVERGED ? precision : -1;

@@ -15,7 +15,7 @@ struct DevStatus {
     int code;        // first error (kOk if none)
     int zero_pivots; // count of non-positive IC0 / zero ILU0 pivots
     int where;       // row or barrier index where a wait gave up
-    int pad;
+    int slow_div;    // set when an FP64 sweep division left div_fast's proven range (rerun with IEEE)
 };
 
 // --- relaxed / acquire / release accesses at GPU scope (PTX memory model) ---
@@ -86,7 +86,8 @@ struct Waiter {
     unsigned int polls;
     unsigned int limit;
     DevStatus *st;
-    __device__ __forceinline__ Waiter(unsigned int lim, DevStatus *s) : polls(0), limit(lim), st(s) {}
+    bool slow;  // this thread met a division outside div_fast's range
+    __device__ __forceinline__ Waiter(unsigned int lim, DevStatus *s) : polls(0), limit(lim), st(s), slow(false) {}
     __device__ __forceinline__ void begin() { polls = 0; }
     __device__ __forceinline__ bool tick(int where) {
         ++polls;
@@ -221,8 +222,8 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned int 
     return false;
 }
 
-// Reciprocal stored beside a diagonal entry d for div_rcp: RN(1/d) (__drcp_rn) when
-// 2^-500 <= |d| <= 2^500, else 0, which sends every division by d to __ddiv_rn.
+// Reciprocal stored beside a diagonal entry d for div_fast: RN(1/d) (__drcp_rn) when
+// 2^-500 <= |d| < 2^500, else 0, which sends every division by d to __ddiv_rn.
 __device__ __forceinline__ double div_recip(double d) {
     const unsigned int e = ((unsigned int)__double2hiint(d) >> 20) & 0x7ffu;  // biased exponent
     return e - (1023u - 500u) <= 999u ? __drcp_rn(d) : 0.0;
@@ -234,20 +235,31 @@ __device__ __forceinline__ double div_recip(double d) {
 // with an FMA): q0 = RN(a*y) lies within two ulps of a/b; one correction
 // q1 = RN(q0 + RN(a - b*q0)*y) makes it a faithful rounding; then, y being RN(1/b) and the
 // remainder a - b*q1 exact in an FMA, q2 = RN(q1 + (a - b*q1)*y) = RN(a/b). The remainders are
-// exact and nothing under- or overflows while 2^-500 <= |b| <= 2^500 (y != 0) and
+// exact and nothing under- or overflows while 2^-500 <= |b| < 2^500 (y != 0) and
 // 2^-460 <= |a| < 2^461: then 2^-961 <= |a/b| <= 2^961 and the remainders' lowest bits stay
-// above 2^-570. Otherwise (zeros, subnormals, infinities, NaNs and the far ranges) the quotient
-// comes from __ddiv_rn. The range test reads a's exponent bits and runs beside the FMA chain.
-__device__ __forceinline__ double div_rcp(double a, double b, double y) {
-    const unsigned int ea = ((unsigned int)__double2hiint(a) >> 20) & 0x7ffu;
-    const bool fast = ea - (1023u - 460u) <= 920u && y != 0.0;
+// above 2^-570. a = +0 also comes out right (+0 / b: every step keeps the zero and its sign
+// follows y); a = -0 does not (the first remainder turns it into +0). Every other a (-0,
+// subnormals, the far ranges, infinities, NaNs) and every b outside the range set `slow`, and
+// the caller must then compute the quotient with __ddiv_rn instead. The range test reads a's
+// bits and runs beside the FMA chain.
+__device__ __forceinline__ double div_fast(double a, double b, double y, bool &slow) {
+    const unsigned int hi = (unsigned int)__double2hiint(a), lo = (unsigned int)__double2loint(a);
+    const unsigned int ea = (hi >> 20) & 0x7ffu;
+    const bool fast = (ea - (1023u - 460u) <= 920u || (hi | lo) == 0u) && y != 0.0;
     const double q0 = __dmul_rn(a, y);
     const double r0 = __fma_rn(-q0, b, a);
     const double q1 = __fma_rn(r0, y, q0);
     const double r1 = __fma_rn(-q1, b, a);
     const double q2 = __fma_rn(r1, y, q1);
-    if (fast) return q2;
-    return __ddiv_rn(a, b);
+    slow |= !fast;
+    return q2;
+}
+
+// div_fast with its fall-back: always RN(a/b).
+__device__ __forceinline__ double div_rcp(double a, double b, double y) {
+    bool slow = false;
+    const double q = div_fast(a, b, y, slow);
+    return slow ? __ddiv_rn(a, b) : q;
 }
 
 // Explicit shared-memory accesses for data reached through pointers the compiler cannot prove

@@ -318,10 +318,12 @@ __device__ __forceinline__ void load_remote(const RowDeps<EK> &p, const WalkIO<T
 
 // One row: dependency values gathered without branches (local slot, or the prefetched remote
 // value), one sentinel test for the whole row, and a wait only for a remote value that was not
-// yet written when it was prefetched. EXACT: the reference's FP64 operation order with correctly
-// rounded operations; else FP32 with 1/diag. Writes the slot (if a later row of the CTA reads
-// it), the staged copy (STG) and the global result.
-template <typename T, typename RT, bool MR, bool STG, bool EXACT, int EK>
+// yet written when it was prefetched. DIV != 0: the reference's FP64 operation order with
+// correctly rounded operations, the division by div_fast (DIV == 1; a division outside its
+// range marks the thread's Waiter and the launch is repeated with DIV == 2) or by __ddiv_rn
+// (DIV == 2); DIV == 0: FP32 with 1/diag. Writes the slot (if a later row of the CTA reads it),
+// the staged copy (STG) and the global result.
+template <typename T, typename RT, bool MR, bool STG, int DIV, int EK>
 __device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<T, EK> &v, const T (&pf)[EK],
                                             const WalkIO<T, RT, MR, STG> &io, Waiter &w) {
     T *xg = io.out();
@@ -344,14 +346,16 @@ __device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<
 #pragma unroll
     for (int j = 0; j < EK; j++)
         if (j < p.ne) {
-            if constexpr (EXACT)
+            if constexpr (DIV != 0)
                 sum = __dadd_rn(sum, __dmul_rn(xv[j], v.a[j]));
             else
                 sum = fmaf(xv[j], v.a[j], sum);
         }
     T o;
-    if constexpr (EXACT)
-        o = div_rcp(__dsub_rn(v.rhs, sum), v.diag, v.rcp);
+    if constexpr (DIV == 2)
+        o = __ddiv_rn(__dsub_rn(v.rhs, sum), v.diag);
+    else if constexpr (DIV == 1)
+        o = div_fast(__dsub_rn(v.rhs, sum), v.diag, v.rcp, w.slow);
     else
         o = (v.rhs - sum) * v.diag;  // FP32 value blocks hold 1/diag
     if (v.sl >= 0) Sh<T>::stu(io.xs_at(io.slot(v.sl)), o);
@@ -370,7 +374,7 @@ __device__ __forceinline__ bool row_compute(const RowDeps<EK> &p, const RowVals<
 // awaited at the start of step s (it was issued a window earlier), the barrier ending step s also
 // decides, for the whole CTA, whether every wait so far succeeded, and the window of step s is
 // then released for refilling. Returns with `i` on the last window walked (not released).
-template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT, int EK>
+template <typename T, typename RT, bool RL2, bool MR, bool STG, int DIV, int EK>
 __device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsigned char *buf, int nint,
                                            const WalkIO<T, RT, MR, STG> &io, Waiter &w, unsigned int spin,
                                            DevStatus *st) {
@@ -411,7 +415,7 @@ __device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsig
             RowVals<T, EK> v;
             load_vals<T, RT, RL2, MR, STG, EK>(I0, V0, nl0, lr, q0, io, v);
             if constexpr (!STG) v.rhs = rhs0;
-            if (!row_compute<T, RT, MR, STG, EXACT, EK>(q0, v, pf0, io, w)) alive = false;
+            if (!row_compute<T, RT, MR, STG, DIV, EK>(q0, v, pf0, io, w)) alive = false;
         }
         for (int pos = lr + stp; alive && pos < nl0; pos += stp) {
             RowDeps<EK> q;
@@ -422,7 +426,7 @@ __device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsig
             if constexpr (!STG) v.rhs = load_rhs<T, RT, RL2, MR, STG>(q.row, q.kpos, io);
 #pragma unroll
             for (int j = 0; j < EK; j++) qf[j] = Sent<T>::value();
-            if (!row_compute<T, RT, MR, STG, EXACT, EK>(q, v, qf, io, w)) alive = false;
+            if (!row_compute<T, RT, MR, STG, DIV, EK>(q, v, qf, io, w)) alive = false;
         }
         if (m1 && alive) {
             load_remote<T, RT, MR, STG, EK>(q1, io, pf0);
@@ -449,7 +453,7 @@ __device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsig
 }
 
 // Any entry stride (the CTA's widest row has more than 3 entries): plain loop, waits in place.
-template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT>
+template <typename T, typename RT, bool RL2, bool MR, bool STG, int DIV>
 __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, const T *V,
                                                 const WalkIO<T, RT, MR, STG> &io, Waiter &w, bool alive) {
     T *xg = io.out();
@@ -479,15 +483,17 @@ __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, c
                     alive = false;
                     break;
                 }
-                if constexpr (EXACT)
+                if constexpr (DIV != 0)
                     sum = __dadd_rn(sum, __dmul_rn(xv, val[pos * E + j]));
                 else
                     sum = fmaf(xv, val[pos * E + j], sum);
             }
             if (!alive) break;
             T o;
-            if constexpr (EXACT)
-                o = div_rcp(__dsub_rn(rhs, sum), diag[pos], rcp[pos]);
+            if constexpr (DIV == 2)
+                o = __ddiv_rn(__dsub_rn(rhs, sum), diag[pos]);
+            else if constexpr (DIV == 1)
+                o = div_fast(__dsub_rn(rhs, sum), diag[pos], rcp[pos], w.slow);
             else
                 o = (rhs - sum) * diag[pos];
             if (slot[pos] >= 0) io.xs[io.slot(slot[pos])] = o;
@@ -504,7 +510,7 @@ __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, c
 // Walk the windows [i, iend) of one direction (all of a CTA's chunks in a direction share one
 // entry stride). Every thread passes every barrier, also after a failed wait, so the CTA never
 // splits; the result is uniform. Each window is released after its walk.
-template <typename T, typename RT, bool RL2, bool MR, bool STG, bool EXACT>
+template <typename T, typename RT, bool RL2, bool MR, bool STG, int DIV>
 __device__ __forceinline__ bool walk_dir(WinStream<T> &ws, int i, int iend, const WalkIO<T, RT, MR, STG> &io,
                                          Waiter &w, unsigned int spin, DevStatus *st) {
     const unsigned char *b;
@@ -513,13 +519,13 @@ __device__ __forceinline__ bool walk_dir(WinStream<T> &ws, int i, int iend, cons
     if (!ws.acquire(i, spin, st, b, nint)) return false;
     bool alive = true;
     switch (Sh<int>::ld(reinterpret_cast<const int *>(b) + 1)) {
-        case 1: alive = walk_run_e<T, RT, RL2, MR, STG, EXACT, 1>(ws, i, b, nint, io, w, spin, st); break;
-        case 2: alive = walk_run_e<T, RT, RL2, MR, STG, EXACT, 2>(ws, i, b, nint, io, w, spin, st); break;
-        case 3: alive = walk_run_e<T, RT, RL2, MR, STG, EXACT, 3>(ws, i, b, nint, io, w, spin, st); break;
+        case 1: alive = walk_run_e<T, RT, RL2, MR, STG, DIV, 1>(ws, i, b, nint, io, w, spin, st); break;
+        case 2: alive = walk_run_e<T, RT, RL2, MR, STG, DIV, 2>(ws, i, b, nint, io, w, spin, st); break;
+        case 3: alive = walk_run_e<T, RT, RL2, MR, STG, DIV, 3>(ws, i, b, nint, io, w, spin, st); break;
         default:
             for (;;) {
                 const int *I = reinterpret_cast<const int *>(b);
-                alive = walk_window_any<T, RT, RL2, MR, STG, EXACT>(I, I + nint,
+                alive = walk_window_any<T, RT, RL2, MR, STG, DIV>(I, I + nint,
                                                                     reinterpret_cast<const T *>(b + (size_t)nint * 4),
                                                                     io, w, alive);
                 if (i + 1 == iend) break;
@@ -533,13 +539,15 @@ __device__ __forceinline__ bool walk_dir(WinStream<T> &ws, int i, int iend, cons
         return false;
     }
     ws.release(i);
+    if (DIV == 1 && w.slow) st->slow_div = 1;
     return !__syncthreads_or(!alive);
 }
 
 // Standalone FP64 sweep of the caller's triangular CSR (values gathered through vsrcT into the
 // packed scratch gv), right-hand sides R at a time (MR: R > 1; STG: staged in shared memory).
-// d = 0: lower (L), 1: upper (U = L^T).
-template <bool MR, bool STG>
+// d = 0: lower (L), 1: upper (U = L^T). IEEE: divide with __ddiv_rn (the repeat of a launch
+// whose div_fast divisions left their range); else div_fast.
+template <bool MR, bool STG, bool IEEE>
 __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, int d, const double *__restrict__ tval,
                                                                  double *gv, const double *__restrict__ b, int ldb,
                                                                  double *x, int ldx, int nrhs, int R, DevStatus *st,
@@ -580,7 +588,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, 
             __syncthreads();
         }
         trace_mark(trace, 2 + 2 * (r0 / R));
-        if (!walk_dir<double, double, false, MR, STG, true>(ws, 0, ws.total(), io, w, spin, st)) {
+        if (!walk_dir<double, double, false, MR, STG, IEEE ? 2 : 1>(ws, 0, ws.total(), io, w, spin, st)) {
             ws.drain(spin);
             return;
         }
@@ -623,11 +631,15 @@ struct IccgArgs {
     double *grad_a;    // if set: grad_a[e] = -x_i * xf_j for each entry e = (i, j) of A
 };
 
+// Division mode of a walk over factors of type T (FP32 factors multiply by 1/diag).
+template <typename T, bool IEEE>
+constexpr int kDiv = sizeof(T) == 8 ? (IEEE ? 2 : 1) : 0;
+
 // z = U^-1 L^-1 r on this CTA's rows; p = z if set_p; adds this thread's share of r.z to rz in
 // a pass over the CTA's rows afterwards. STG: r is staged in shared memory, the lower walk
 // leaves y there for the upper walk, which leaves z there for the r.z pass; else the right-hand
 // sides come from r and from y (in L2) and z is read back from L2.
-template <typename T, bool STG>
+template <typename T, bool STG, bool IEEE>
 __device__ __forceinline__ bool chunk_precond(const IccgArgs &A, WinStream<T> &ws, unsigned char *smem, bool set_p, double &rz,
                               Waiter &w) {
     const int c = blockIdx.x;
@@ -644,12 +656,12 @@ __device__ __forceinline__ bool chunk_precond(const IccgArgs &A, WinStream<T> &w
     const int n0 = ws.ctl->n0;
     {
         const WalkIO<T, double, false, STG> lo{xs, yg, A.r, rs, 0, 0, 1};
-        if (!walk_dir<T, double, false, false, STG, sizeof(T) == 8>(ws, 0, n0, lo, w, A.spin_limit, A.st)) return false;
+        if (!walk_dir<T, double, false, false, STG, kDiv<T, IEEE>>(ws, 0, n0, lo, w, A.spin_limit, A.st)) return false;
     }
     trace_mark(A.trace, 57);
     {
         const WalkIO<T, T, false, STG> up{xs, zg, yg, rs, 0, 0, 1};
-        if (!walk_dir<T, T, true, false, STG, sizeof(T) == 8>(ws, n0, ws.total(), up, w, A.spin_limit, A.st)) return false;
+        if (!walk_dir<T, T, true, false, STG, kDiv<T, IEEE>>(ws, n0, ws.total(), up, w, A.spin_limit, A.st)) return false;
     }
     for (int k = threadIdx.x; k < nl; k += blockDim.x) {
         const int row = __ldg(A.pl.srow + s0 + k);
@@ -680,8 +692,9 @@ __device__ __forceinline__ void pack_factor(const ChunkDir &D, const double *lu,
 
 // T = double: FP64 factors; T = float: FP32 factors. STG: the right-hand sides of the sweeps are
 // staged in shared memory (when they fit). One instantiation per combination keeps each one's
-// register budget to what it uses.
-template <typename T, bool STG>
+// register budget to what it uses. IEEE (FP64 factors only): sweep divisions by __ddiv_rn, for the
+// repeat of a launch whose div_fast divisions left their range.
+template <typename T, bool STG, bool IEEE>
 __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     constexpr bool kMixed = sizeof(T) == 4;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -741,7 +754,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     trace_mark(A.trace, 3);
 
     double rzl = 0.0;
-    if (!chunk_precond<T, STG>(A, ws, smem, true, rzl, w)) {
+    if (!chunk_precond<T, STG, IEEE>(A, ws, smem, true, rzl, w)) {
         ws.drain(A.spin_limit);
         return;
     }
@@ -791,7 +804,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
         if (rel < A.tol) break;
 
         rzl = 0.0;
-        if (!chunk_precond<T, STG>(A, ws, smem, false, rzl, w)) {
+        if (!chunk_precond<T, STG, IEEE>(A, ws, smem, false, rzl, w)) {
             ws.drain(A.spin_limit);
             return;
         }

@@ -170,10 +170,12 @@ baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row);
 baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget, int upper, const double *tval,
                                     const double *b, double *x);
 
-/* Division test hook (no counterpart in the reference): for i < n, q[i] = the FP64 sweep's
- * quotient a[i] / b[i] (mode 0: from the stored reciprocal RN(1/b[i]) with Markstein's correction,
- * as the sweeps compute it; mode 1: the IEEE correctly rounded division) on device arrays a, b, q
- * of n doubles. Synchronises `stream` to read the status. */
+/* Division test hook (no counterpart in the reference), on device arrays a, b, q of n doubles.
+ * mode 0: q[i] = a[i] / b[i] as the FP64 sweeps compute it -- Markstein's correction on the stored
+ * reciprocal of b[i] where that is proven exact, else the IEEE division (the sweeps get the latter
+ * by repeating the launch with IEEE divisions); mode 1: the IEEE correctly rounded division;
+ * mode 2: q[i] = 1 where the fast path declines (a repeat would follow), else 0.
+ * Synchronises `stream` to read the status. */
 baas_status baas_test_divide(const double *a, const double *b, double *q, long long n, int mode, void *stream);
 
 /* Forward sweep x = L^-1 b (upper = 0; L is the analysed lower triangle, diagonal LAST in each

@@ -99,3 +99,75 @@ def test_special_and_boundary_values():
     ea = rng.integers(-960, 960, n)
     eb = np.clip(ea + rng.integers(-970, 970, n), -960, 959)
     _check(np.ldexp(_mantissa(rng, n), ea), np.ldexp(_mantissa(rng, n), eb))
+
+
+def test_fast_path_declines_exactly_outside_its_range():
+    """mode 2 reports the quotients div_fast declines: a = -0, |a| < 2^-460, |a| >= 2^461,
+    non-finite a, and divisors outside [2^-500, 2^500); a = +0 and ordinary values stay fast."""
+    a = np.array([1.0, -3.5, 0.0, -0.0, 2.0 ** -460, 2.0 ** -461, 2.0 ** 460, 2.0 ** 461, 5e-324, np.inf, np.nan,
+                  1.0, 1.0, 1.0, 1.0])
+    b = np.array([3.0, 7.0, 2.0, 2.0, 1.5, 1.5, 1.5, 1.5, 1.5, 1.5, 1.5, 2.0 ** 499, 2.0 ** 500, 2.0 ** -500,
+                  2.0 ** -501])
+    want = np.array([0, 0, 0, 1, 0, 1, 0, 1, 1, 1, 1, 0, 1, 0, 1], dtype=np.float64)
+    assert np.array_equal(_divide(a, b, 2), want)
+    _check(a, b)
+
+
+def _bits(x):
+    return np.ascontiguousarray(x, dtype=np.float64).view(np.int64)
+
+
+def test_sweep_repeats_with_ieee_division():
+    """A right-hand side of -0.0 on rows without dependencies: div_fast would return +0, so the
+    sweep must notice and repeat with IEEE divisions; the result matches the oracle bit for bit,
+    signs of zeros included."""
+    import torch
+
+    from baas_b200 import KERNEL_SPTRSV, DeviceCSR, Schedule, gen
+    from oracle.oracle import Port
+
+    L, _, b = gen.sptrsv_case(48, 0)
+    b = b.copy()
+    b[:5] = -0.0
+    s = Schedule(L, kind=KERNEL_SPTRSV, nthread=8)
+    x = torch.zeros(L.n, dtype=torch.float64, device="cuda")
+    s.forward(DeviceCSR.from_host(L), torch.from_numpy(b).cuda(), x)
+    want = Port.lower_solve(L, b)
+    assert np.signbit(want[0])
+    assert np.array_equal(_bits(x.cpu().numpy()), _bits(want))
+
+
+def test_iccg_and_batched_repeat_with_ieee_division():
+    """ICCG with b[0] = -0.0 starts its first lower sweep with -0 / L00 and must repeat the launch
+    with IEEE divisions; the iterate equals the one for b[0] = +0.0 (both are IEEE-exact runs of
+    the same iteration) and so does the iteration count. Same for a batched solve."""
+    import torch
+
+    from baas_b200 import KERNEL_ICCG, BatchSchedule, DeviceCSR, Schedule, gen
+
+    A = gen.laplace3d(12, 1e-3)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    dA = DeviceCSR.from_host(A)
+    out = []
+    for z in (0.0, -0.0):
+        b = gen.uniform_rhs(A.n, 1)
+        b[0] = z
+        x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+        it, rel = s.iccg(dA, torch.from_numpy(b).cuda(), x, tol=1e-10)
+        out.append((it, x.cpu().numpy()))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+
+    systems = [gen.laplace2d(9), gen.vardiff2d(11, seed=2)]
+    bs = BatchSchedule(systems, parts=3)
+    C = bs.combined
+    dC = DeviceCSR.from_host(C)
+    res = []
+    for z in (0.0, -0.0):
+        B = gen.uniform_rhs(C.n, 7, nrhs=2).reshape(2, C.n)
+        B[0, bs.sys_off[1]] = z
+        X = torch.zeros((2, C.n), dtype=torch.float64, device="cuda")
+        it, rel = bs.iccg_batched(dC, torch.from_numpy(B).cuda(), X, tol=1e-10)
+        res.append((it.copy(), X.cpu().numpy()))
+    assert np.array_equal(res[0][0], res[1][0])
+    assert np.array_equal(res[0][1], res[1][1])
