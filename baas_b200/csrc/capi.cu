@@ -77,6 +77,10 @@ struct PartHost {
     std::vector<int> cta_seg, seg_item, item_pos, cta_pos, row, eptr, dep;
     std::vector<int> srcT, dsrcT;  // positions in the caller's triangular CSR (L or U)
     std::vector<int> srcA, dsrcA;  // positions in A's value array (IC0 factor on A's pattern)
+    // factorisations (forward direction): per entry, the A position of its pivot (the diagonal
+    // of the row it depends on) and its column-match pairs in merge order (mptr ranges of
+    // mpair = {offset in the own row, A position in the other row})
+    std::vector<int> epiv, mptr, mpair;
     int max_local = 0;
 };
 
@@ -84,9 +88,13 @@ struct PartDev {
     int *cta_seg = nullptr, *seg_item = nullptr, *item_pos = nullptr, *cta_pos = nullptr;
     int *row = nullptr, *eptr = nullptr, *dep = nullptr;
     int *srcT = nullptr, *dsrcT = nullptr, *srcA = nullptr, *dsrcA = nullptr;
-    baas::PartView view(int P) const { return baas::PartView{P, cta_seg, seg_item, item_pos, cta_pos, row, eptr, dep}; }
+    int *epiv = nullptr, *mptr = nullptr, *mpair = nullptr;
+    baas::PartView view(int P) const {
+        return baas::PartView{P, cta_seg, seg_item, item_pos, cta_pos, row, eptr, dep, epiv, mptr,
+                              reinterpret_cast<const int2 *>(mpair)};
+    }
     void release() {
-        int *ptrs[] = {cta_seg, seg_item, item_pos, cta_pos, row, eptr, dep, srcT, dsrcT, srcA, dsrcA};
+        int *ptrs[] = {cta_seg, seg_item, item_pos, cta_pos, row, eptr, dep, srcT, dsrcT, srcA, dsrcA, epiv, mptr, mpair};
         for (int *p : ptrs)
             if (p) cudaFree(p);
         *this = PartDev();
@@ -101,6 +109,11 @@ baas_status upload_part(PartDev &d, const PartHost &h) {
     BAAS_TRY(upload(d.row, h.row));
     BAAS_TRY(upload(d.eptr, h.eptr));
     BAAS_TRY(upload(d.dep, h.dep));
+    if (!h.mptr.empty()) {
+        BAAS_TRY(upload(d.epiv, h.epiv));
+        BAAS_TRY(upload(d.mptr, h.mptr));
+        BAAS_TRY(upload(d.mpair, h.mpair));
+    }
     BAAS_TRY(upload(d.srcT, h.srcT));
     BAAS_TRY(upload(d.dsrcT, h.dsrcT));
     BAAS_TRY(upload(d.srcA, h.srcA));
@@ -354,6 +367,39 @@ void build_dir(baas_schedule *s, bool upper, PartHost &out) {
             out.dsrcA[pos] = h.l_src[s->cpos[cb]];
         }
         out.eptr[pos + 1] = (int)out.dep.size();
+    }
+    if (!upper && h.kind != baas::SchedKind::SpTRSV) {
+        // factorisation entries: entry t of a row is A position rb + t (the row's lower part,
+        // ascending). IC0 (merge/IC.cpp sparse_dot_product): row i's entry at column j pairs with
+        // row j's entries of equal column, both lower parts; ILU0 (merge/ILU.cpp): entry t with
+        // column c updates row i's later entries whose column row c holds in its upper part.
+        const bool ilu = h.kind == baas::SchedKind::ILU0;
+        const std::vector<int> &rp = h.a_rowptr, &ci = h.a_colidx, &dg = h.a_diagptr;
+        out.epiv.assign(out.dep.size(), 0);
+        out.mptr.assign(out.dep.size() + 1, 0);
+        out.mpair.clear();
+        for (int pos = 0; pos < n; pos++) {
+            const int r = out.row[pos], rb = rp[r], di = dg[r], re = rp[r + 1];
+            for (int t = 0; t < di - rb; t++) {
+                const int e = out.eptr[pos] + t, j = ci[rb + t];
+                out.epiv[e] = dg[j];
+                int a = ilu ? rb + t + 1 : rb, ae = ilu ? re : di;
+                int b = ilu ? dg[j] + 1 : rp[j], be = ilu ? rp[j + 1] : dg[j];
+                while (a < ae && b < be) {
+                    if (ci[a] == ci[b]) {
+                        out.mpair.push_back(a - rb);
+                        out.mpair.push_back(b);
+                        a++;
+                        b++;
+                    } else if (ci[a] < ci[b]) {
+                        a++;
+                    } else {
+                        b++;
+                    }
+                }
+                out.mptr[e + 1] = (int)(out.mpair.size() / 2);
+            }
+        }
     }
     if (!upper && s->fault_row >= 0) {
         for (int pos = 0; pos < n; pos++)

@@ -37,6 +37,11 @@ struct PartView {
     const int *row;       // position -> row
     const int *eptr;      // position -> off-diagonal entries [eptr[pos], eptr[pos+1])
     const int *dep;       // entry -> encoded dependency
+    // factorisations: entry -> A position of its pivot (the other row's diagonal), and its
+    // column-match pairs [mptr[e], mptr[e+1]) of mpair = {offset in the own row, A position}
+    const int *epiv;
+    const int *mptr;
+    const int2 *mpair;
 };
 
 // Walks this CTA's level segments; `row_fn(pos, slot)` computes one row (false = give up).
@@ -165,15 +170,125 @@ __device__ __forceinline__ bool ilu0_row_part(const PartView &pv, int pos, int i
     return true;
 }
 
+// Rows of at most kFacRegs entries (the lower part for IC0, the whole row for ILU0) run from
+// registers: the row's values and all its pivots are loaded at once (after the waits for remote
+// rows), the column matches come from the host-built pair lists instead of a merge loop over
+// column indices, and the row is written back once. Same operations in the same order as
+// ic0_row_part / ilu0_row_part, so the factor is bit-identical.
+constexpr int kFacRegs = 8;
+
+__device__ __forceinline__ double pick(const double (&v)[kFacRegs], int k) {
+    double r = 0.0;
+#pragma unroll
+    for (int u = 0; u < kFacRegs; u++) r = u == k ? v[u] : r;
+    return r;
+}
+
+// Waits for the rows of the entries [rb, rb + ne) that another CTA computes (their flags, by
+// column index, as ic0_row_part / ilu0_row_part wait).
+__device__ __forceinline__ bool wait_remote(const PartView &pv, int e0, int rb, int ne, const int *__restrict__ colidx,
+                                            const int *gflag, int epoch, Waiter &w, int i) {
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++)
+        if (t < ne && __ldg(pv.dep + e0 + t) >= 0 && !wait_flag(gflag + __ldg(colidx + rb + t), epoch, w, i)) return false;
+    return true;
+}
+
+__device__ __forceinline__ bool ic0_row_reg(const PartView &pv, int pos, int i, int rb, int di,
+                                            const int *__restrict__ colidx, double *lu, const int *gflag, int epoch,
+                                            Waiter &w, DevStatus *st) {
+    const int ne = di - rb, e0 = __ldg(pv.eptr + pos);
+    if (!wait_remote(pv, e0, rb, ne, colidx, gflag, epoch, w, i)) return false;
+    double v[kFacRegs], piv[kFacRegs];
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++) {
+        v[t] = piv[t] = 0.0;
+        if (t < ne) {
+            v[t] = lu[rb + t];
+            const int pj = __ldg(pv.epiv + e0 + t);
+            piv[t] = __ldg(pv.dep + e0 + t) < 0 ? ldv<true>(lu + pj) : ldv<false>(lu + pj);
+        }
+    }
+    const double dval = lu[di];
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++)
+        if (t < ne) {
+            const bool loc = __ldg(pv.dep + e0 + t) < 0;
+            double dp = 0.0;
+            for (int m = __ldg(pv.mptr + e0 + t), m1 = __ldg(pv.mptr + e0 + t + 1); m < m1; m++) {
+                const int2 pr = __ldg(pv.mpair + m);
+                const double bv = loc ? ldv<true>(lu + pr.y) : ldv<false>(lu + pr.y);
+                dp = __dadd_rn(dp, __dmul_rn(pick(v, pr.x), bv));
+            }
+            v[t] = __ddiv_rn(__dsub_rn(v[t], dp), piv[t]);
+        }
+    double dv = 0.0;
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++)
+        if (t < ne) {
+            dv = __dadd_rn(dv, __dmul_rn(v[t], v[t]));
+            lu[rb + t] = v[t];
+        }
+    const double tt = __dsub_rn(dval, dv);
+    if (tt > 0.0)
+        lu[di] = __dsqrt_rn(tt);
+    else
+        atomicAdd(&st->zero_pivots, 1);
+    return true;
+}
+
+__device__ __forceinline__ bool ilu0_row_reg(const PartView &pv, int pos, int i, int rb, int di, int re,
+                                             const int *__restrict__ colidx, double *lu, const int *gflag, int epoch,
+                                             Waiter &w, DevStatus *st) {
+    const int nlow = di - rb, nrow = re - rb, e0 = __ldg(pv.eptr + pos);
+    if (!wait_remote(pv, e0, rb, nlow, colidx, gflag, epoch, w, i)) return false;
+    double v[kFacRegs], piv[kFacRegs];
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++) {
+        v[t] = piv[t] = 0.0;
+        if (t < nrow) v[t] = lu[rb + t];
+        if (t < nlow) {
+            const int pj = __ldg(pv.epiv + e0 + t);
+            piv[t] = __ldg(pv.dep + e0 + t) < 0 ? ldv<true>(lu + pj) : ldv<false>(lu + pj);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++)
+        if (t < nlow) {
+            const bool loc = __ldg(pv.dep + e0 + t) < 0;
+            if (piv[t] == 0.0) atomicAdd(&st->zero_pivots, 1);
+            const double tmp = __ddiv_rn(v[t], piv[t]);
+            v[t] = tmp;
+            for (int m = __ldg(pv.mptr + e0 + t), m1 = __ldg(pv.mptr + e0 + t + 1); m < m1; m++) {
+                const int2 pr = __ldg(pv.mpair + m);
+                const double bv = loc ? ldv<true>(lu + pr.y) : ldv<false>(lu + pr.y);
+                const double u = __dsub_rn(pick(v, pr.x), __dmul_rn(tmp, bv));
+#pragma unroll
+                for (int q = 0; q < kFacRegs; q++)
+                    if (q == pr.x) v[q] = u;
+            }
+        }
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++)
+        if (t < nrow) lu[rb + t] = v[t];
+    return true;
+}
+
 template <bool ILU>
 __device__ __forceinline__ bool factor_part(const PartView &pv, const int *rowptr, const int *colidx, const int *diagptr,
                                             double *lu, int *gflag, int epoch, Waiter &w, DevStatus *st) {
     return walk_levels(pv, [&](int pos, int) {
         const int row = __ldg(pv.row + pos);
-        const bool ok = ILU ? ilu0_row_part(pv, pos, row, rowptr, colidx, diagptr, lu, gflag, epoch, w, st)
-                            : ic0_row_part(pv, pos, row, rowptr, colidx, diagptr, lu, gflag, epoch, w, st);
+        const int rb = __ldg(rowptr + row), di = __ldg(diagptr + row), re = __ldg(rowptr + row + 1);
+        bool ok;
+        if constexpr (ILU)
+            ok = re - rb <= kFacRegs ? ilu0_row_reg(pv, pos, row, rb, di, re, colidx, lu, gflag, epoch, w, st)
+                                     : ilu0_row_part(pv, pos, row, rowptr, colidx, diagptr, lu, gflag, epoch, w, st);
+        else
+            ok = di - rb <= kFacRegs ? ic0_row_reg(pv, pos, row, rb, di, colidx, lu, gflag, epoch, w, st)
+                                     : ic0_row_part(pv, pos, row, rowptr, colidx, diagptr, lu, gflag, epoch, w, st);
         if (!ok) return false;
-        __threadfence();
+        // the release store orders this thread's writes of the row before the flag
         st_release_s32(gflag + row, epoch);
         return true;
     });
