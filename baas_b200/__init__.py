@@ -18,14 +18,16 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native
-from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
+from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, MAPPING_COST_SPLIT,
+                      MAPPING_COST_SPLIT_BARRIER, MAPPING_FOUR_RULE, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
                       PARTITION_RANGES,
                       PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
 
 __all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV",
            "KERNEL_ICCG", "KERNEL_IC0", "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "PARTITION_RANGES",
-           "PARTITION_BAAS_THREADS", "PARTITION_CUSTOM", "version"]
+           "PARTITION_BAAS_THREADS", "PARTITION_CUSTOM", "MAPPING_FOUR_RULE", "MAPPING_COST_SPLIT",
+           "MAPPING_COST_SPLIT_BARRIER", "version"]
 
 
 def version() -> str:
@@ -78,7 +80,7 @@ class Schedule:
     """
 
     def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
-                 parts: int = 0, partition: int = 0, smem_budget: int = 0):
+                 parts: int = 0, partition: int = 0, smem_budget: int = 0, mapping: int = 0):
         L = _native.lib()
         self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
         self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
@@ -90,6 +92,7 @@ class Schedule:
         opt.parts = parts
         opt.partition = partition
         opt.smem_budget = smem_budget
+        opt.mapping = mapping
         h = C.c_void_p()
         _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
         self._h = h
@@ -97,6 +100,7 @@ class Schedule:
         self.nnz = int(self._rowptr[-1])
         self.kind = kind
         self.nthread = nthread
+        self.mapping = mapping
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -130,6 +134,7 @@ class Schedule:
         opt = _native.BaasOptions()
         _native.lib().baas_options_default(C.byref(opt))
         opt.nthread = self.nthread
+        opt.mapping = self.mapping
         opt.parts = parts
         opt.smem_budget = smem_budget
         opt.partition = partition

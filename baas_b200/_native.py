@@ -26,6 +26,7 @@ STATUS_NAMES = {
 KERNEL_SPTRSV, KERNEL_ICCG, KERNEL_IC0, KERNEL_ILU0 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32_FACTORS = 0, 1
 PARTITION_RANGES, PARTITION_BAAS_THREADS, PARTITION_CUSTOM = 0, 1, 2
+MAPPING_FOUR_RULE, MAPPING_COST_SPLIT, MAPPING_COST_SPLIT_BARRIER = 0, 1, 2
 
 FIELDS = {
     "ngroups": 0, "nlevels": 1, "ntasks": 2, "group_ptr": 3, "group_set": 4, "level_ptr": 5,
@@ -38,7 +39,7 @@ FIELDS = {
 EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
-    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan", "baas_test_divide", "baas_replan_custom",
+    "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan", "baas_test_divide", "baas_replan_custom", "baas_csr_read_mtx", "baas_csr_free",
 ]
 
 
@@ -49,7 +50,7 @@ class BaasCsr(C.Structure):
 
 class BaasOptions(C.Structure):
     _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("parts", C.c_int),
-                ("partition", C.c_int), ("smem_budget", C.c_int)]
+                ("partition", C.c_int), ("smem_budget", C.c_int), ("mapping", C.c_int)]
 
 
 class BaasError(RuntimeError):
@@ -115,6 +116,10 @@ def lib():
     L.baas_test_divide.restype = i
     L.baas_replan_custom.argtypes = [vp, vp, i, i]
     L.baas_replan_custom.restype = i
+    L.baas_csr_read_mtx.argtypes = [C.c_char_p, C.POINTER(BaasCsr)]
+    L.baas_csr_read_mtx.restype = i
+    L.baas_csr_free.argtypes = [C.POINTER(BaasCsr)]
+    L.baas_csr_free.restype = None
     _lib = L
     return L
 

@@ -27,6 +27,10 @@
 
 using baas::DevStatus;
 
+namespace baas {
+baas_status set_error(baas_status code, const std::string &msg);
+}
+
 namespace {
 
 thread_local std::string g_err;
@@ -304,13 +308,13 @@ void build_partition(baas_schedule *s, int P) {
 // ascending. Backward (U = L^T): the exact reverse.
 void build_dir(baas_schedule *s, bool upper, PartHost &out) {
     const baas::HostSchedule &h = s->hs;
-    const int n = h.n, P = s->P, nl = h.nlevels;
+    const int n = h.n, P = s->P, nl = (int)h.exec_level_ptr.size() - 1;
     out = PartHost();
     // per CTA: list of (level, group) in processing order
     std::vector<std::vector<std::pair<int, int>>> items(P);
     for (int li = 0; li < nl; li++) {
         const int l = upper ? nl - 1 - li : li;
-        const int qb = h.level_ptr[l], qe = h.level_ptr[l + 1];
+        const int qb = h.exec_level_ptr[l], qe = h.exec_level_ptr[l + 1];
         for (int qi = 0; qi < qe - qb; qi++) {
             const int q = upper ? qe - 1 - qi : qb + qi;
             const int g = h.perm_to_orig[q];
@@ -854,9 +858,17 @@ void baas_options_default(baas_options *opt) {
     opt->parts = 0;
     opt->partition = BAAS_PARTITION_RANGES;
     opt->smem_budget = 0;
+    opt->mapping = BAAS_MAPPING_FOUR_RULE;
 }
 
 const char *baas_last_error_string(void) { return g_err.c_str(); }
+
+}  // extern "C"
+
+// error reporting for the library's other host sources (mtx.cpp)
+baas_status baas::set_error(baas_status code, const std::string &msg) { return fail(code, msg); }
+
+extern "C" {
 
 const char *baas_version(void) { return "baas_b200 0.2.0 (sm_100a)"; }
 
@@ -872,6 +884,10 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     if (o.parts < 0) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 0");
     if (o.smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
+    if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_COST_SPLIT_BARRIER)
+        return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
+    if (o.mapping != BAAS_MAPPING_FOUR_RULE && kind != BAAS_KERNEL_ICCG)
+        return fail(BAAS_ERR_BAD_ARG, "the cost-split mappings are the Scheduler's (kind BAAS_KERNEL_ICCG)");
     if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
     if (A->rowptr[A->n] != A->nnz) return fail(BAAS_ERR_BAD_ARG, "nnz != rowptr[n]");
     // value-source codes of the sweep plan address positions below 2^30
@@ -882,7 +898,7 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     baas_schedule *s = new baas_schedule();
     s->opt = o;
     s->nnz_a = A->nnz;
-    baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread);
+    baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping);
     s->nnz_l = (int)s->hs.l_colidx.size();
     if (sk != baas::SchedKind::SpTRSV && s->nnz_a != 2 * s->nnz_l - A->n) {
         delete s;
@@ -1177,6 +1193,7 @@ void baas_destroy(baas_schedule *s) {
 baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
     if (!s || !opt) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     if (opt->nthread != s->hs.nthread) return fail(BAAS_ERR_BAD_ARG, "nthread is fixed by the analysis");
+    if (opt->mapping != s->opt.mapping) return fail(BAAS_ERR_BAD_ARG, "mapping is fixed by the analysis");
     if (opt->parts < 0 || opt->smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "parts and smem_budget must be >= 0");
     if (opt->partition == BAAS_PARTITION_CUSTOM) {
         if (s->custom_part.empty()) return fail(BAAS_ERR_BAD_ARG, "no custom partition: use baas_replan_custom");

@@ -212,6 +212,7 @@ void level_sets(const Csx &dag, HostSchedule &s) {
     }
     s.nlevels = lvl;
     s.level_ptr.assign(lptr.begin(), lptr.begin() + lvl + 1);
+    s.exec_level_ptr = s.level_ptr;
     for (int l = 0; l < lvl; l++) std::sort(q.begin() + s.level_ptr[l], q.begin() + s.level_ptr[l + 1]);
     s.perm_to_orig.assign(q.begin(), q.begin() + n);
     s.perm.assign(n, 0);
@@ -258,6 +259,117 @@ void threads_per_level(HostSchedule &s) {
         }
         s.nthread_per_level[l] = t;
     }
+}
+
+// Stages 8-9 of the cost-split mapping, the Scheduler's P2P algorithm (test/Schedule.hpp:233-240,
+// 263-265). Level merge (level_merge_group, merge/LevelMerge.cpp:372-421): threads per level by
+// level_nthreads_group (:264-294; rule :102-114: one thread below 40 rows or at most 12 groups,
+// else max(ceil(rows / 10), groups) capped by the thread count; a single level gets
+// min(groups, threads)), then consecutive single-thread levels are merged by the reference's
+// two-pointer scan, and the merged levels number their groups from 0 (constructLevelMerge
+// :423-452).
+void merge_levels_group(HostSchedule &s) {
+    const int nl = s.nlevels, nc = s.nthread;
+    const std::vector<int> lp = s.level_ptr;
+    std::vector<int> t(nl, 1);
+    if (nl == 1) {
+        t[0] = std::min(lp[1] - lp[0], nc);
+    } else {
+        for (int l = 0; l < nl; l++) {
+            const int groups = lp[l + 1] - lp[l];
+            int rows = 0;
+            for (int p = lp[l]; p < lp[l + 1]; p++) {
+                const int g = s.perm_to_orig[p];
+                rows += s.group_ptr[g + 1] - s.group_ptr[g];
+            }
+            t[l] = (rows < 40 || groups <= 12) ? 1 : std::min(std::max((rows + 9) / 10, groups), nc);
+        }
+    }
+    std::vector<int> mptr(nl + 1, 0);
+    int m = 0;
+    for (int i = 1; i < nl;) {
+        if (t[i] == 1 && t[i] == t[m]) {
+            i++;
+        } else {
+            m++;
+            t[m] = t[i];
+            mptr[m] = lp[i];
+            i++;
+        }
+    }
+    m++;
+    mptr[m] = lp[nl];
+    s.nlevels = m;
+    s.level_ptr.assign(mptr.begin(), mptr.begin() + m + 1);
+    s.nthread_per_level.assign(t.begin(), t.begin() + m);
+    for (int l = 0; l < m; l++)
+        for (int j = s.level_ptr[l]; j < s.level_ptr[l + 1]; j++) s.node_to_level[s.perm_to_orig[j]] = l;
+}
+
+// Task::constructTask (merge/LevelTask.cpp:42-196): each level's groups are cut into up to
+// nthread_per_level contiguous ranges of about equal cost (a lower_bound on the level's running
+// cost for multiples of ceil-divided load; a search that starts past the level's end finds
+// nothing, as std::lower_bound does on an empty range), one task per non-empty range of a thread
+// (barrier: one task per level and thread, empty or not).
+void cost_split_map(HostSchedule &s, bool barrier) {
+    const int nl = s.nlevels, nt = s.nthread, nodes = s.ngroups;
+    const int *lp = s.level_ptr.data();
+    const int *p2o = s.perm_to_orig.data();
+    std::vector<std::pair<int, int>> rows((size_t)nl * nt);
+    std::vector<double> cb((size_t)nodes + nt, 0.0);
+    for (int l = 0; l < nl; l++) {
+        const int exec = s.nthread_per_level[l], lb = lp[l], le = lp[l + 1];
+        double load = 0;
+        for (int i = lb; i < le; i++) {
+            cb[i] = load;
+            load += s.cost[p2o[i]];
+        }
+        const double per = (load + exec - 1) / exec;
+        int pre = lb, r = lb, t;
+        for (t = 0; t < exec; t++) {
+            const int nr = r <= le ? (int)(std::lower_bound(cb.begin() + r, cb.begin() + le, (t + 1) * per) - cb.begin()) : r;
+            r = nr;
+            const int b = pre, e = std::min(r, le);
+            pre = e;
+            rows[(size_t)t * nl + l] = {b, e};
+            ++r;
+        }
+        for (t = exec; t < nt; t++) rows[(size_t)t * nl + l] = {le, le};
+    }
+    std::vector<int> rsum(nt + 1, 0);
+    s.thread_boundaries.assign(nt + 1, 0);
+    for (int tid = 0; tid < nt; tid++) {
+        int sum = 0, cnt = 0;
+        for (int l = 0; l < nl; l++) {
+            const int d = rows[(size_t)tid * nl + l].second - rows[(size_t)tid * nl + l].first;
+            sum += d;
+            if (barrier || d) cnt++;
+        }
+        rsum[tid + 1] = sum;
+        s.thread_boundaries[tid + 1] = cnt;
+    }
+    for (int tid = 0; tid < nt; tid++) {
+        rsum[tid + 1] += rsum[tid];
+        s.thread_boundaries[tid + 1] += s.thread_boundaries[tid];
+    }
+    s.ntasks = s.thread_boundaries[nt];
+    s.task_boundaries.assign(s.ntasks + 1, 0);
+    s.thread_cont_to_orig.assign(nodes, 0);
+    s.orig_to_thread_cont.assign(nodes, 0);
+    for (int tid = 0; tid < nt; tid++) {
+        int off = rsum[tid], task = s.thread_boundaries[tid];
+        for (int l = 0; l < nl; l++) {
+            const auto &rg = rows[(size_t)tid * nl + l];
+            if (!barrier && rg.second <= rg.first) continue;
+            s.task_boundaries[task++] = off;
+            for (int j = rg.first; j < rg.second; j++) {
+                s.orig_to_thread_cont[p2o[j]] = off;
+                s.thread_cont_to_orig[off] = p2o[j];
+                off++;
+            }
+        }
+    }
+    s.task_boundaries[s.ntasks] = nodes;
 }
 
 // Stage 9: four-rule mapping of groups to virtual threads, then the merge of consecutive
@@ -546,7 +658,8 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
     return "";
 }
 
-void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread) {
+void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
+                    Mapping mapping) {
     auto t0 = std::chrono::steady_clock::now();
     s = HostSchedule();
     s.kind = kind;
@@ -602,12 +715,18 @@ void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
             s.cost[g] += 1 * (s.l_rowptr[r + 1] - s.l_rowptr[r]);
         }
 
-    level_sets(fdag, s);       // stage 7
-    threads_per_level(s);      // stage 8
+    level_sets(fdag, s);  // stage 7
+    if (mapping == Mapping::FourRule)
+        threads_per_level(s);  // stage 8
+    else
+        merge_levels_group(s);
     for (int g = 0; g < s.ngroups; g++)  // test/Schedule.hpp:72-79
         std::sort(s.group_set.begin() + s.group_ptr[g], s.group_set.begin() + s.group_ptr[g + 1]);
     Csx dag_csr = transpose(fdag);  // parents of each group, then the group itself
-    four_rule_map(s, dag_csr);      // stage 9
+    if (mapping == Mapping::FourRule)
+        four_rule_map(s, dag_csr);  // stage 9
+    else
+        cost_split_map(s, mapping == Mapping::CostSplitBarrier);
     task_dags(s, dag_csr);          // stage 10
     s.fdag_ptr = std::move(fdag.ptr);
     s.fdag_set = std::move(fdag.idx);

@@ -38,6 +38,10 @@ struct HostSchedule {
     int ntasks = 0;
     std::vector<int> group_ptr, group_set;            // rows ascending inside each group
     std::vector<int> level_ptr, perm_to_orig, node_to_level, perm;  // LevelSet
+    // the dependency levels of the group DAG (Kahn levels, before any merge): the GPU plans run
+    // a level's groups in parallel, so they follow these even when the exported level set is
+    // the merged one (the cost-split mapping's merged levels chain dependent groups)
+    std::vector<int> exec_level_ptr;
     std::vector<int> nthread_per_level;
     std::vector<int> thread_boundaries, task_boundaries;
     std::vector<int> thread_cont_to_orig, orig_to_thread_cont;
@@ -53,7 +57,14 @@ struct HostSchedule {
 // Returns an empty string when valid, else the reason.
 const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedKind kind);
 
+// How groups are mapped to virtual threads: the BAAS four-rule mapping (P2P_RULE), or the
+// Scheduler's P2P algorithm -- level merge plus a cost-balanced contiguous split per level
+// (Task::constructTask), with one task per non-empty range or, in barrier mode, one per level
+// and thread.
+enum class Mapping { FourRule = 0, CostSplit = 1, CostSplitBarrier = 2 };
+
 // Runs stages 1-10. `rowptr`/`colidx` are host arrays of the analysed matrix.
-void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread);
+void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
+                    Mapping mapping = Mapping::FourRule);
 
 }  // namespace baas

@@ -274,3 +274,41 @@ def batch_vardiff2d(nsys: int = 64, kmin: int = 64, kmax: int = 512, seed: int =
     rng = np.random.default_rng(seed)
     ks = rng.integers(kmin, kmax + 1, size=nsys)
     return [vardiff2d(int(k), seed=seed * 1000 + j) for j, k in enumerate(ks)]
+
+
+def read_mtx(path) -> CSR:
+    """A coordinate MatrixMarket file as a CSR, through the library's reader
+    (baas_csr_read_mtx: symmetric storage expanded, each row sorted by column)."""
+    import ctypes as C
+
+    from . import _native
+
+    m = _native.BaasCsr()
+    _native.check(_native.lib().baas_csr_read_mtx(str(path).encode(), C.byref(m)), "baas_csr_read_mtx")
+    try:
+        n, nnz = m.n, m.nnz
+        rowptr = np.ctypeslib.as_array(C.cast(m.rowptr, C.POINTER(C.c_int32)), shape=(n + 1,)).copy()
+        colidx = np.ctypeslib.as_array(C.cast(m.colidx, C.POINTER(C.c_int32)), shape=(max(nnz, 1),))[:nnz].copy()
+        values = np.ctypeslib.as_array(C.cast(m.values, C.POINTER(C.c_double)), shape=(max(nnz, 1),))[:nnz].copy()
+    finally:
+        _native.lib().baas_csr_free(C.byref(m))
+    return CSR(n, rowptr, colidx, values)
+
+
+def write_mtx(A: CSR, path, symmetric: bool = False, field: str = "real") -> None:
+    """Write A as a coordinate MatrixMarket file: every entry ('general'), or the lower triangle
+    with 'symmetric' storage. Values are written with 17 significant digits, so a read gives back
+    the same doubles."""
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    keep = rows >= A.colidx if symmetric else np.ones(A.nnz, dtype=bool)
+    r, c, v = rows[keep], A.colidx[keep], A.values[keep]
+    with open(path, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate {field} {'symmetric' if symmetric else 'general'}\n")
+        f.write("% written by baas_b200.gen.write_mtx\n")
+        f.write(f"{A.n} {A.n} {len(r)}\n")
+        if field == "pattern":
+            for i, j in zip(r, c):
+                f.write(f"{i + 1} {j + 1}\n")
+        else:
+            for i, j, x in zip(r, c, v):
+                f.write(f"{i + 1} {j + 1} {x:.17g}\n")

@@ -108,7 +108,19 @@ typedef struct baas_options {
                          BAAS_PARTITION_CUSTOM (set by baas_replan_custom only) */
     int smem_budget;  /* bytes of shared memory per CTA for solution slots and the two plan
                          window buffers (0 = library default, 220 KiB; at most 224 KiB) */
+    int mapping;      /* BAAS_MAPPING_FOUR_RULE (default) or, for BAAS_KERNEL_ICCG, one of the
+                         cost-split mappings; fixed by the analysis */
 } baas_options;
+
+/* How the analysis maps groups to the reference's virtual threads (Schedule::ALG_SCHEDULE,
+ * test/Schedule.hpp:31-37, 263-281). FOUR_RULE: P2P_RULE, the BAAS four-rule mapping
+ * (merge/LevelTask.cpp:2295-2684). COST_SPLIT: P2P -- level merge (merge/LevelMerge.cpp:372-421)
+ * and a cost-balanced contiguous split of every merged level (Task::constructTask,
+ * merge/LevelTask.cpp:42-196), one task per non-empty range. COST_SPLIT_BARRIER: the same split
+ * with the barrier-mode task layout (Task(ngroups, true): one task per level and thread). The
+ * cost-split mappings are the Scheduler's (kind BAAS_KERNEL_ICCG only). The GPU plan does not
+ * depend on the mapping except through BAAS_PARTITION_BAAS_THREADS. */
+enum { BAAS_MAPPING_FOUR_RULE = 0, BAAS_MAPPING_COST_SPLIT = 1, BAAS_MAPPING_COST_SPLIT_BARRIER = 2 };
 
 /* How rows are given to CTAs. RANGES: contiguous row-index ranges, so every cross-CTA
  * dependency of the lower sweep points to an earlier CTA. BAAS_THREADS: CTA t runs the groups the
@@ -139,6 +151,17 @@ double baas_schedule_analysis_ms(const baas_schedule *s);
 
 /* Frees the schedule and its device memory. */
 void baas_destroy(baas_schedule *s);
+
+/* MatrixMarket ingestion. Replaces SPM::CSR(const char *fileName) (spm/CSR.cpp:90-112), which
+ * reads through loadMatrixMarket_mmio_highlevel_coo (spm/COO.cpp:322-338), mmio_allinone_coo
+ * (spm/mmio_highlevel.cpp:748-921) and dcoo2csr (spm/COO.cpp:222-317). Reads a coordinate
+ * MatrixMarket file (real, integer or pattern values; general, symmetric or hermitian storage,
+ * the latter two expanded to both triangles) into a host CSR with each row sorted by column.
+ * The arrays match the reference reader's for every file without repeated (row, column)
+ * entries; a repeated entry is BAAS_ERR_BAD_ARG here (the reference's order for it is
+ * unspecified). The library allocates the arrays: release them with baas_csr_free. */
+baas_status baas_csr_read_mtx(const char *path, baas_csr *out);
+void baas_csr_free(baas_csr *mat);
 
 /* Rebuilds the schedule's device execution plan with other options (parts, partition,
  * smem_budget, spin_limit; nthread must stay as analysed) without repeating the analysis: the

@@ -35,7 +35,8 @@
 
 namespace baas_b200 {
 
-// test/Schedule.hpp:31-37. Only P2P_RULE (the BAAS four-rule mapping) is built.
+// test/Schedule.hpp:31-37. P2P_RULE (the BAAS four-rule mapping) and P2P (level merge and a
+// cost-balanced split per level) are built; P2P_MAPPING and P2P_TIME are not.
 enum ALG_SCHEDULE { P2P, P2P_MAPPING, P2P_TIME, P2P_RULE };
 
 namespace detail {
@@ -113,7 +114,9 @@ class Scheduler {
         : csrA_(csrA), num_thread_(num_thread) {
         if (!isSymmetric) throw std::runtime_error("Scheduler: only the symmetric (IC0/ICCG) schedule is built");
         if (isTRSVPerm) throw std::runtime_error("Scheduler: the permuted (isTRSVPerm) variant is not built");
-        if (alg != P2P_RULE) throw std::runtime_error("Scheduler: only P2P_RULE (the BAAS four-rule mapping) is built");
+        if (alg != P2P_RULE && alg != P2P)
+            throw std::runtime_error("Scheduler: P2P_MAPPING and P2P_TIME are not built (P2P_RULE, P2P are)");
+        mapping_ = alg == P2P ? BAAS_MAPPING_COST_SPLIT : BAAS_MAPPING_FOUR_RULE;
     }
     ~Scheduler() { baas_destroy(s_); }
     Scheduler(const Scheduler &) = delete;
@@ -124,6 +127,7 @@ class Scheduler {
         baas_options o;
         baas_options_default(&o);
         o.nthread = num_thread_;
+        o.mapping = mapping_;
         const baas_csr a = detail::host_pattern(csrA_);
         baas_destroy(s_);
         s_ = nullptr;
@@ -165,6 +169,7 @@ class Scheduler {
     }
     const CSR *csrA_;
     int num_thread_;
+    int mapping_ = BAAS_MAPPING_FOUR_RULE;
     baas_schedule *s_ = nullptr;
     detail::DevCsr dA_, dL_, dU_;
     detail::DevBuf<double> dlu_, db_, dx_;

@@ -69,16 +69,42 @@ class Ref:
             L.ref_dot.restype = _d
             L.ref_pcg.argtypes = [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _i, _d, _vp, _vp]
             L.ref_pcg.restype = _i
+            L.ref_set_mapping.argtypes = [_i]
+            L.ref_mtx_read.argtypes = [C.c_char_p, _vp, _vp]
+            L.ref_mtx_read.restype = _vp
+            L.ref_mtx_copy.argtypes = [_vp, _vp, _vp, _vp]
+            L.ref_mtx_free.argtypes = [_vp]
             cls._lib = L
         return cls._lib
 
+    @staticmethod
+    def read_mtx(path):
+        """The reference's own MatrixMarket reader (SPM::CSR(fileName), spm/CSR.cpp:90-112)."""
+        from baas_b200.gen import CSR as _CSR
+
+        L = Ref.lib()
+        n, nnz = C.c_int(0), C.c_int(0)
+        h = L.ref_mtx_read(str(path).encode(), C.byref(n), C.byref(nnz))
+        try:
+            rowptr = np.zeros(n.value + 1, dtype=np.int32)
+            colidx = np.zeros(nnz.value, dtype=np.int32)
+            values = np.zeros(nnz.value, dtype=np.float64)
+            L.ref_mtx_copy(h, _p(rowptr), _p(colidx), _p(values))
+        finally:
+            L.ref_mtx_free(h)
+        return _CSR(n.value, rowptr, colidx, values)
+
     class Schedule:
-        def __init__(self, kind: int, A, nthread: int):
+        def __init__(self, kind: int, A, nthread: int, mapping: int = 0):
             L = Ref.lib()
             self.rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
             self.colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
             self.n = A.n
-            self.h = L.ref_schedule_build(kind, A.n, _p(self.rowptr), _p(self.colidx), nthread)
+            L.ref_set_mapping(mapping)
+            try:
+                self.h = L.ref_schedule_build(kind, A.n, _p(self.rowptr), _p(self.colidx), nthread)
+            finally:
+                L.ref_set_mapping(0)
 
         def __del__(self):
             if getattr(self, "h", None):

@@ -48,11 +48,33 @@ namespace refdrv
     // they are cleared here first.
     struct OpenScheduler : public Schedule::Scheduler
     {
-        OpenScheduler(const CSR *A, int nthread)
-            : Schedule::Scheduler(A, true, false, Schedule::ALG_SCHEDULE::P2P_RULE, nthread)
+        OpenScheduler(const CSR *A, int nthread, Schedule::ALG_SCHEDULE alg = Schedule::ALG_SCHEDULE::P2P_RULE)
+            : Schedule::Scheduler(A, true, false, alg, nthread)
         {
             csrA_perm = nullptr;
             x_perm = nullptr;
+            // the P2P branch of preprocessing() fills levelset_merge through level_merge_group
+            // (test/Schedule.hpp:233-240) but nothing allocates it: the reference's own P2P
+            // Scheduler writes through an unset pointer. Allocate it here.
+            if (alg == Schedule::ALG_SCHEDULE::P2P)
+                levelset_merge = new LevelSet();
+        }
+        // The barrier-mode task layout of the P2P split: the same calls preprocessing() makes
+        // after the level merge (test/Schedule.hpp:263-291), with Task(ngroups, true).
+        void rebuild_barrier_tasks()
+        {
+            delete task;
+            delete taskSchedule;
+            delete taskDAG;
+            taskDAG = new DAG();
+            task = new Merge::Task(ngroups, true);
+            task->constructTask(levelset_merge, cost.data(), num_thread, nthread_per_level);
+            DAG *dag_csr = DAG::inverseDAG(*dag_group);
+            task->constructTaskDAGParallel(dag_group, dag_csr, taskDAG, num_thread, false);
+            taskSchedule = new Merge::TaskSchedule(taskDAG->getNodeNum(), taskDAG->DAG_ptr.back());
+            taskSchedule->constructTaskSchedule(taskDAG);
+            delete dag_csr;
+            taskSchedule->constructInverseSchedule(taskDAG);
         }
         LevelSet *lvl() { return levelset_merge; }
         int *ntpl() { return nthread_per_level; }
@@ -175,8 +197,15 @@ namespace refdrv
 
 using namespace refdrv;
 
+// the mapping the next ICCG schedule build uses (ref_set_mapping)
+static int g_mapping = BAAS_MAPPING_FOUR_RULE;
+
 extern "C"
 {
+    /* BAAS_MAPPING_*: FOUR_RULE builds the Scheduler with P2P_RULE, COST_SPLIT with P2P, and
+     * COST_SPLIT_BARRIER with P2P followed by the barrier-mode task layout. */
+    void ref_set_mapping(int mapping) { g_mapping = mapping; }
+
     /* kind: a baas_kernel value. The matrix is the lower triangle incl. diagonal (diagonal last
      * in each row) for BAAS_KERNEL_SPTRSV and the full matrix for the other kinds. */
     void *ref_schedule_build(int kind, int n, const int *rowptr, const int *colidx, int nthread)
@@ -195,8 +224,12 @@ extern "C"
         auto t0 = std::chrono::steady_clock::now();
         if (kind == BAAS_KERNEL_ICCG)
         {
-            h->scheduler = new OpenScheduler(h->A, nthread);
+            const Schedule::ALG_SCHEDULE alg = g_mapping == BAAS_MAPPING_FOUR_RULE ? Schedule::ALG_SCHEDULE::P2P_RULE
+                                                                                  : Schedule::ALG_SCHEDULE::P2P;
+            h->scheduler = new OpenScheduler(h->A, nthread, alg);
             h->scheduler->preprocessing();
+            if (g_mapping == BAAS_MAPPING_COST_SPLIT_BARRIER)
+                h->scheduler->rebuild_barrier_tasks();
         }
         else if (kind == BAAS_KERNEL_SPTRSV)
         {
@@ -519,4 +552,23 @@ extern "C"
         delete sch;
         return iters;
     }
+
+    // MatrixMarket reading through the reference's own SPM::CSR(const char *fileName)
+    // (spm/CSR.cpp:90-112): open, then copy the arrays out, then free.
+    void *ref_mtx_read(const char *path, int *n, int *nnz)
+    {
+        CSR *A = new CSR(path);
+        *n = A->m;
+        *nnz = A->rowptr[A->m] - A->rowptr[0];
+        return A;
+    }
+    void ref_mtx_copy(void *h, int *rowptr, int *colidx, double *values)
+    {
+        const CSR *A = static_cast<const CSR *>(h);
+        const int nnz = A->rowptr[A->m] - A->rowptr[0];
+        std::memcpy(rowptr, A->rowptr, sizeof(int) * (size_t)(A->m + 1));
+        std::memcpy(colidx, A->colidx, sizeof(int) * (size_t)nnz);
+        std::memcpy(values, A->values, sizeof(double) * (size_t)nnz);
+    }
+    void ref_mtx_free(void *h) { delete static_cast<CSR *>(h); }
 }

@@ -102,6 +102,19 @@ int main(int argc, char **argv) {
         return fail("isTRSVPerm accepted");
     } catch (const std::runtime_error &) {
     }
+    try {
+        baas_b200::Scheduler<CSR> bad(&A, true, false, baas_b200::P2P_TIME, 8);
+        return fail("P2P_TIME accepted");
+    } catch (const std::runtime_error &) {
+    }
+    // the P2P algorithm (level merge + cost split): a different task layout on the same groups
+    baas_b200::Scheduler<CSR> p2p(&A, true, false, baas_b200::P2P, 8);
+    p2p.preprocessing();
+    int ntasks_rule = 0, ntasks_p2p = 0, ngroups_p2p = 0;
+    baas_schedule_export(sch.handle(), BAAS_FIELD_NTASKS, &ntasks_rule);
+    baas_schedule_export(p2p.handle(), BAAS_FIELD_NTASKS, &ntasks_p2p);
+    baas_schedule_export(p2p.handle(), BAAS_FIELD_NGROUPS, &ngroups_p2p);
+    if (ngroups_p2p != ngroups || ntasks_p2p <= 0 || ntasks_p2p == ntasks_rule) return fail("P2P schedule");
     if (analysis_only) {
         std::printf("OK analysis ngroups=%d\n", ngroups);
         return 0;
@@ -118,6 +131,9 @@ int main(int argc, char **argv) {
     sch.runIC0(&A, lu.data());
     if (orc_ic0(n, A.rowptr, A.colidx, diag.data(), want.data()) != 0) return fail("oracle pivots");
     if (std::memcmp(lu.data(), want.data(), sizeof(double) * nnz) != 0) return fail("runIC0");
+    std::vector<double> lu2(A.va);
+    p2p.runIC0(&A, lu2.data());
+    if (std::memcmp(lu2.data(), want.data(), sizeof(double) * nnz) != 0) return fail("runIC0 (P2P)");
 
     CSR L, U;
     split(A, lu, L, U);

@@ -28,7 +28,7 @@ from oracle.oracle import FIELDS, Ref  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 
-# (name, kind, matrix factory, thread counts)
+# (name, kind, matrix factory, thread counts[, mapping: BAAS_MAPPING_*, default the four-rule one])
 SCHEDULE_CASES = [
     ("lap2d_12_lower", 0, lambda: gen.laplace2d(12).lower(), (1, 3, 4)),
     ("lap3d_6", 1, lambda: gen.laplace3d(6, 1e-3), (2, 4)),
@@ -36,6 +36,9 @@ SCHEDULE_CASES = [
     ("convdiff_5_ilu0", 3, lambda: gen.convdiff3d(5), (3,)),
     ("knn_200", 1, lambda: gen.knn_stiffness(nodes=200, k=12, seed=3), (4,)),
     ("lap3d_6_perm", 1, lambda: gen.laplace3d(6, 1e-3).permuted(gen.random_symmetric_permutation(216, 5)), (4,)),
+    # the Scheduler's P2P algorithm: level merge + cost split, and its barrier-mode task layout
+    ("lap3d_8_p2p", 1, lambda: gen.laplace3d(8, 1e-3), (3, 8), 1),
+    ("knn_200_p2p_barrier", 1, lambda: gen.knn_stiffness(nodes=200, k=12, seed=3), (4,), 2),
 ]
 
 
@@ -49,13 +52,16 @@ def schedule_digest(arrs: dict) -> str:
 
 def main() -> None:
     sched = {}
-    for name, kind, mk, threads in SCHEDULE_CASES:
+    for case in SCHEDULE_CASES:
+        name, kind, mk, threads = case[:4]
+        mapping = case[4] if len(case) > 4 else 0
         A = mk()
         sched[f"{name}__rowptr"] = A.rowptr
         sched[f"{name}__colidx"] = A.colidx
         sched[f"{name}__kind"] = np.array([kind], dtype=np.int32)
+        sched[f"{name}__mapping"] = np.array([mapping], dtype=np.int32)
         for nt in threads:
-            s = Ref.Schedule(kind, A, nt)
+            s = Ref.Schedule(kind, A, nt, mapping=mapping)
             for f in FIELDS:
                 sched[f"{name}__t{nt}__{f}"] = s.export(f)
     # full-size C1 schedule digests

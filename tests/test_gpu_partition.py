@@ -55,3 +55,25 @@ def test_custom_partition_sweeps_ic0_iccg(blocks):
     lu = dA.values.clone()
     f.ic0(dA, lu)
     assert np.array_equal(lu.cpu().numpy(), lu_o)
+
+
+@pytest.mark.parametrize("mapping", [1, 2])
+def test_cost_split_mapping_on_gpu(mapping):
+    """ICCG and the sweeps with CTA t running virtual thread t of the Scheduler's P2P mapping."""
+    import torch
+
+    from baas_b200 import PARTITION_BAAS_THREADS
+
+    A = gen.laplace3d(16, 1e-3)
+    b = gen.uniform_rhs(A.n, 1)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=16, partition=PARTITION_BAAS_THREADS, mapping=mapping)
+    dA = DeviceCSR.from_host(A)
+    x = _t(np.zeros(A.n))
+    it, rel = s.iccg(dA, _t(b), x, tol=1e-10, maxiter=2000)
+    xo, ito, _ = Port.pcg(A, b, tol=1e-10)
+    assert abs(it - ito) <= 1 and rel < 1e-10
+    lu_o, _ = Port.ic0(A)
+    Lo = gen.CSR(A.n, A.rowptr, A.colidx, lu_o).lower()
+    y = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    s.forward(DeviceCSR.from_host(Lo), _t(b), y)
+    assert np.array_equal(y.cpu().numpy(), Port.lower_solve(Lo, b))

@@ -137,3 +137,14 @@ def test_custom_partition_checks():
     assert np.array_equal(s.emulate_sweep(Lo, b), Port.lower_solve(Lo, b))
     s.replan(parts=4, partition=PARTITION_CUSTOM)  # keeps the map
     assert np.array_equal(s.emulate_sweep(Lo, b), Port.lower_solve(Lo, b))
+
+
+@pytest.mark.parametrize("mapping", [1, 2])
+def test_cost_split_mapping_thread_partition_plan(mapping):
+    """CTA t runs virtual thread t of the Scheduler's P2P mapping (cost split per merged level)."""
+    A = gen.laplace3d(10, 1e-3)
+    Lo, Up = _ic_lu(A)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=12, partition=PARTITION_BAAS_THREADS, mapping=mapping)
+    r = gen.uniform_rhs(A.n, 1)
+    assert np.array_equal(s.emulate_sweep(Lo, r), Port.lower_solve(Lo, r))
+    assert np.array_equal(s.emulate_sweep(Up, r, upper=True), Port.upper_solve(Up, r, descending=True))

@@ -35,7 +35,8 @@ def test_schedule_matches_reference_golden(name, nt):
     A = gen.CSR(int(len(z[f"{name}__rowptr"]) - 1), z[f"{name}__rowptr"], z[f"{name}__colidx"],
                 np.ones(len(z[f"{name}__colidx"])))
     kind = int(z[f"{name}__kind"][0])
-    s = Schedule(A, kind=kind, nthread=nt)
+    mapping = int(z[f"{name}__mapping"][0]) if f"{name}__mapping" in z.files else 0
+    s = Schedule(A, kind=kind, nthread=nt, mapping=mapping)
     for f in FIELDS:
         want = z[f"{name}__t{nt}__{f}"]
         got = s.export(f)
@@ -80,6 +81,37 @@ def test_schedule_matches_live_reference(case, ref_lib):
         ref = ref_lib.Schedule(kind, A, nt).arrays()
         for f in FIELDS:
             assert np.array_equal(ours[f], ref[f]), f"kind={kind} nthread={nt} field {f}"
+
+
+MAPPED = [
+    lambda: gen.laplace3d(12, 1e-3),
+    lambda: gen.knn_stiffness(nodes=600, k=12, seed=3),
+    lambda: gen.vardiff2d(48, seed=5),
+]
+
+
+@pytest.mark.parametrize("mapping", [1, 2])
+@pytest.mark.parametrize("case", range(len(MAPPED)))
+def test_cost_split_mappings_match_live_reference(case, mapping, ref_lib):
+    """The Scheduler's P2P algorithm (level merge + Task::constructTask) and its barrier-mode
+    task layout, every exported array against the reference's."""
+    A = MAPPED[case]()
+    for nt in (3, 8, 16):
+        ours = Schedule(A, kind=KERNEL_ICCG, nthread=nt, mapping=mapping).arrays()
+        ref = ref_lib.Schedule(KERNEL_ICCG, A, nt, mapping=mapping).arrays()
+        for f in FIELDS:
+            assert np.array_equal(ours[f], ref[f]), f"mapping={mapping} nthread={nt} field {f}"
+
+
+def test_mapping_checks():
+    from baas_b200 import BaasError
+
+    with pytest.raises(BaasError):
+        Schedule(gen.laplace2d(8).lower(), kind=KERNEL_SPTRSV, mapping=1)  # the Scheduler's (ICCG) only
+    with pytest.raises(BaasError):
+        Schedule(gen.laplace3d(4, 1e-3), kind=KERNEL_ICCG, mapping=3)
+    s = Schedule(gen.laplace3d(4, 1e-3), kind=KERNEL_ICCG, mapping=1)
+    s.replan(parts=2)  # keeps the analysed mapping
 
 
 def test_schedule_invariants():
