@@ -884,10 +884,10 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     if (o.parts < 0) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 0");
     if (o.smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
-    if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_COST_SPLIT_BARRIER)
+    if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_FINISH_TIME)
         return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
     if (o.mapping != BAAS_MAPPING_FOUR_RULE && kind != BAAS_KERNEL_ICCG)
-        return fail(BAAS_ERR_BAD_ARG, "the cost-split mappings are the Scheduler's (kind BAAS_KERNEL_ICCG)");
+        return fail(BAAS_ERR_BAD_ARG, "the P2P, barrier and P2P_TIME mappings are the Scheduler's (kind BAAS_KERNEL_ICCG)");
     if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
     if (A->rowptr[A->n] != A->nnz) return fail(BAAS_ERR_BAD_ARG, "nnz != rowptr[n]");
     // value-source codes of the sweep plan address positions below 2^30

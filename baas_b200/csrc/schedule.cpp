@@ -372,6 +372,73 @@ void cost_split_map(HostSchedule &s, bool barrier) {
     s.task_boundaries[s.ntasks] = nodes;
 }
 
+// The common end of the level-by-level mappers (four-rule, finish-time): runs of consecutive
+// single-thread levels merge into the run's first task (merge/LevelTask.cpp:2646-2676, the same
+// scan at :1858-1894), then taskMapToBoundaries (:198-304, non-barrier form) turns the per-level
+// thread ranges of by_level_thread into thread/task boundaries and both permutations.
+void finish_mapping(HostSchedule &s, std::vector<std::pair<int, int>> &task_rows, const std::vector<int> &by_level_thread,
+                    std::vector<int> level_single) {
+    const int nl = s.nlevels, nt = s.nthread, nodes = s.ngroups;
+    {
+        std::vector<int> run_start(nl + 1, 0), ntpl(s.nthread_per_level);
+        int m = 0;
+        for (int lvl = 1; lvl < nl;) {
+            if (ntpl[lvl] == 1 && ntpl[m] == 1) {
+                auto &pre = task_rows[(size_t)level_single[m] * nl + run_start[m]];
+                auto &post = task_rows[(size_t)level_single[lvl] * nl + lvl];
+                pre.second = post.second;
+                post = {0, 0};
+                lvl++;
+            } else {
+                m++;
+                ntpl[m] = ntpl[lvl];
+                level_single[m] = level_single[lvl];
+                run_start[m] = lvl;
+                lvl++;
+            }
+        }
+    }
+
+    // taskMapToBoundaries, non-barrier form (merge/LevelTask.cpp:198-304)
+    std::vector<int> rows_before(nt + 1, 0);
+    s.thread_boundaries.assign(nt + 1, 0);
+    for (int t = 0; t < nt; t++) {
+        int sum = 0, cnt = 0;
+        for (int l = 0; l < nl; l++) {
+            const auto &tr = task_rows[(size_t)t * nl + l];
+            const int d = tr.second - tr.first;
+            sum += d;
+            if (d) ++cnt;
+        }
+        rows_before[t + 1] = sum;
+        s.thread_boundaries[t + 1] = cnt;
+    }
+    for (int t = 0; t < nt; t++) {
+        rows_before[t + 1] += rows_before[t];
+        s.thread_boundaries[t + 1] += s.thread_boundaries[t];
+    }
+    s.ntasks = s.thread_boundaries[nt];
+    s.task_boundaries.assign(s.ntasks + 1, 0);
+    s.orig_to_thread_cont.assign(nodes, 0);
+    s.thread_cont_to_orig.assign(nodes, 0);
+    for (int t = 0; t < nt; t++) {
+        int row = rows_before[t], task = s.thread_boundaries[t];
+        for (int l = 0; l < nl; l++) {
+            const auto &tr = task_rows[(size_t)t * nl + l];
+            if (tr.second > tr.first) {
+                s.task_boundaries[task++] = row;
+                for (int j = tr.first; j < tr.second; j++) {
+                    s.orig_to_thread_cont[by_level_thread[j]] = row;
+                    s.thread_cont_to_orig[row] = by_level_thread[j];
+                    row++;
+                }
+            }
+        }
+    }
+    s.task_boundaries[s.ntasks] = nodes;
+}
+
+
 // Stage 9: four-rule mapping of groups to virtual threads, then the merge of consecutive
 // single-thread levels and the conversion to thread/task boundaries.
 //
@@ -545,64 +612,96 @@ void four_rule_map(HostSchedule &s, const Csx &dag_csr) {
         }
     }
 
-    // merge runs of single-thread levels into the run's first task (merge/LevelTask.cpp:2646-2676)
-    {
-        std::vector<int> run_start(nl + 1, 0), ntpl(s.nthread_per_level);
-        int m = 0;
-        for (int lvl = 1; lvl < nl;) {
-            if (ntpl[lvl] == 1 && ntpl[m] == 1) {
-                auto &pre = task_rows[(size_t)level_single[m] * nl + run_start[m]];
-                auto &post = task_rows[(size_t)level_single[lvl] * nl + lvl];
-                pre.second = post.second;
-                post = {0, 0};
-                lvl++;
-            } else {
-                m++;
-                ntpl[m] = ntpl[lvl];
-                level_single[m] = level_single[lvl];
-                run_start[m] = lvl;
-                lvl++;
-            }
-        }
-    }
+    finish_mapping(s, task_rows, by_level_thread, level_single);
+}
 
-    // taskMapToBoundaries, non-barrier form (merge/LevelTask.cpp:198-304)
-    std::vector<int> rows_before(nt + 1, 0);
-    s.thread_boundaries.assign(nt + 1, 0);
-    for (int t = 0; t < nt; t++) {
-        int sum = 0, cnt = 0;
-        for (int l = 0; l < nl; l++) {
-            const auto &tr = task_rows[(size_t)t * nl + l];
-            const int d = tr.second - tr.first;
-            sum += d;
-            if (d) ++cnt;
+// Stage 9 of the finish-time mapping, the Scheduler's P2P_TIME algorithm
+// (Task::constructMappingByFinishTime, merge/LevelTask.cpp:1647-1910). Level 0 is split by cost as
+// in the four-rule mapping, and each thread accumulates its busy time. On every later level the
+// nthread_per_level[l] threads that finish first are chosen (std::nth_element), every group's
+// earliest start is the latest finish among its parents (held in an int, as the reference
+// holds it), the groups are sorted by that start (std::sort) and each goes, in that order, to
+// the chosen thread that finishes first (std::min_element), which advances that thread's time.
+// The same standard-library calls on the same sequences give the reference's order also among
+// ties.
+void finish_time_map(HostSchedule &s, const Csx &dag_csr) {
+    const int nl = s.nlevels, nt = s.nthread, nodes = s.ngroups;
+    const int *lp = s.level_ptr.data();
+    const int *p2o = s.perm_to_orig.data();
+    std::vector<int> by_level_thread(nodes);
+    std::vector<std::pair<int, int>> task_rows((size_t)nl * nt);
+    std::vector<int> level_single(nl, -1);
+    std::vector<double> finish(nodes, 0.0), ttime(nt, 0.0);
+    {
+        const int et = s.nthread_per_level[0];
+        const int lb = lp[0], le = lp[1];
+        std::vector<double> pre(le - lb + 1);
+        double load = 0.0;
+        for (int i = lb; i < le; i++) {
+            pre[i - lb] = load;
+            load += s.cost[p2o[i]];
         }
-        rows_before[t + 1] = sum;
-        s.thread_boundaries[t + 1] = cnt;
+        const double per = (load + et - 1) / et;
+        int prev_end = lb, r = lb;
+        if (et == 1) level_single[0] = 0;
+        for (int t = 0; t < et; t++) {
+            int nr = r;
+            if (r < le) nr = lb + (int)(std::lower_bound(pre.begin() + (r - lb), pre.begin() + (le - lb), (t + 1) * per) - pre.begin());
+            r = nr;
+            const int b = prev_end, e = std::min(r, le);
+            prev_end = e;
+            task_rows[(size_t)t * nl + 0] = {b, e};
+            for (int k = b; k < e; k++) {
+                const int node = p2o[k];
+                by_level_thread[k] = node;
+                ttime[t] += s.cost[node];
+                finish[node] = ttime[t];
+            }
+            ++r;
+        }
+        for (int t = et; t < nt; t++) task_rows[(size_t)t * nl + 0] = {le, le};
     }
-    for (int t = 0; t < nt; t++) {
-        rows_before[t + 1] += rows_before[t];
-        s.thread_boundaries[t + 1] += s.thread_boundaries[t];
-    }
-    s.ntasks = s.thread_boundaries[nt];
-    s.task_boundaries.assign(s.ntasks + 1, 0);
-    s.orig_to_thread_cont.assign(nodes, 0);
-    s.thread_cont_to_orig.assign(nodes, 0);
-    for (int t = 0; t < nt; t++) {
-        int row = rows_before[t], task = s.thread_boundaries[t];
-        for (int l = 0; l < nl; l++) {
-            const auto &tr = task_rows[(size_t)t * nl + l];
-            if (tr.second > tr.first) {
-                s.task_boundaries[task++] = row;
-                for (int j = tr.first; j < tr.second; j++) {
-                    s.orig_to_thread_cont[by_level_thread[j]] = row;
-                    s.thread_cont_to_orig[row] = by_level_thread[j];
-                    row++;
-                }
+    std::vector<int> tidx(nt), order;
+    std::vector<std::vector<int>> tnodes(nt);
+    std::vector<uint8_t> chosen(nt);
+    for (int lvl = 1; lvl < nl; lvl++) {
+        const int lb = lp[lvl], le = lp[lvl + 1];
+        const int et = s.nthread_per_level[lvl];
+        for (auto &v : tnodes) v.clear();
+        std::iota(tidx.begin(), tidx.end(), 0);
+        std::nth_element(tidx.begin(), tidx.begin() + et, tidx.end(), [&](int a, int b) { return ttime[a] < ttime[b]; });
+        if (et == 1) level_single[lvl] = tidx[0];
+        for (int i = lb; i < le; i++) {
+            const int node = p2o[i];
+            int start = 0;
+            for (int q = dag_csr.ptr[node]; q < dag_csr.ptr[node + 1] - 1; q++) {
+                const int par = dag_csr.idx[q];
+                start = start < finish[par] ? (int)finish[par] : start;
+            }
+            finish[node] = start;
+        }
+        order.assign(p2o + lb, p2o + le);
+        std::sort(order.begin(), order.end(), [&](int a, int b) { return finish[a] < finish[b]; });
+        for (int node : order) {
+            const int t = *std::min_element(tidx.begin(), tidx.begin() + et, [&](int a, int b) { return ttime[a] < ttime[b]; });
+            finish[node] = ttime[t] + s.cost[node];
+            ttime[t] = finish[node];
+            tnodes[t].push_back(node);
+        }
+        std::fill(chosen.begin(), chosen.end(), 0);
+        for (int q = 0; q < et; q++) chosen[tidx[q]] = 1;
+        int pos = lb;
+        for (int t = 0; t < nt; t++) {
+            auto &tr = task_rows[(size_t)t * nl + lvl];
+            if (chosen[t]) {
+                tr = {pos, pos + (int)tnodes[t].size()};
+                for (int v : tnodes[t]) by_level_thread[pos++] = v;
+            } else {
+                tr = {pos, pos};
             }
         }
     }
-    s.task_boundaries[s.ntasks] = nodes;
+    finish_mapping(s, task_rows, by_level_thread, level_single);
 }
 
 // Stage 10: for every task, the sorted set of tasks on other threads that own a parent group.
@@ -716,7 +815,7 @@ void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         }
 
     level_sets(fdag, s);  // stage 7
-    if (mapping == Mapping::FourRule)
+    if (mapping == Mapping::FourRule || mapping == Mapping::FinishTime)
         threads_per_level(s);  // stage 8
     else
         merge_levels_group(s);
@@ -725,6 +824,8 @@ void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
     Csx dag_csr = transpose(fdag);  // parents of each group, then the group itself
     if (mapping == Mapping::FourRule)
         four_rule_map(s, dag_csr);  // stage 9
+    else if (mapping == Mapping::FinishTime)
+        finish_time_map(s, dag_csr);
     else
         cost_split_map(s, mapping == Mapping::CostSplitBarrier);
     task_dags(s, dag_csr);          // stage 10

@@ -57,11 +57,11 @@ struct HostSchedule {
 // Returns an empty string when valid, else the reason.
 const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedKind kind);
 
-// How groups are mapped to virtual threads: the BAAS four-rule mapping (P2P_RULE), or the
+// How groups are mapped to virtual threads: the BAAS four-rule mapping (P2P_RULE); the
 // Scheduler's P2P algorithm -- level merge plus a cost-balanced contiguous split per level
 // (Task::constructTask), with one task per non-empty range or, in barrier mode, one per level
-// and thread.
-enum class Mapping { FourRule = 0, CostSplit = 1, CostSplitBarrier = 2 };
+// and thread; or P2P_TIME, earliest-finishing threads take the earliest-startable groups.
+enum class Mapping { FourRule = 0, CostSplit = 1, CostSplitBarrier = 2, FinishTime = 3 };
 
 // Runs stages 1-10. `rowptr`/`colidx` are host arrays of the analysed matrix.
 void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,

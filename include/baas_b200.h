@@ -109,7 +109,7 @@ typedef struct baas_options {
     int smem_budget;  /* bytes of shared memory per CTA for solution slots and the two plan
                          window buffers (0 = library default, 220 KiB; at most 224 KiB) */
     int mapping;      /* BAAS_MAPPING_FOUR_RULE (default) or, for BAAS_KERNEL_ICCG, one of the
-                         cost-split mappings; fixed by the analysis */
+                         Scheduler's other mappings; fixed by the analysis */
 } baas_options;
 
 /* How the analysis maps groups to the reference's virtual threads (Schedule::ALG_SCHEDULE,
@@ -117,10 +117,17 @@ typedef struct baas_options {
  * (merge/LevelTask.cpp:2295-2684). COST_SPLIT: P2P -- level merge (merge/LevelMerge.cpp:372-421)
  * and a cost-balanced contiguous split of every merged level (Task::constructTask,
  * merge/LevelTask.cpp:42-196), one task per non-empty range. COST_SPLIT_BARRIER: the same split
- * with the barrier-mode task layout (Task(ngroups, true): one task per level and thread). The
- * cost-split mappings are the Scheduler's (kind BAAS_KERNEL_ICCG only). The GPU plan does not
- * depend on the mapping except through BAAS_PARTITION_BAAS_THREADS. */
-enum { BAAS_MAPPING_FOUR_RULE = 0, BAAS_MAPPING_COST_SPLIT = 1, BAAS_MAPPING_COST_SPLIT_BARRIER = 2 };
+ * with the barrier-mode task layout (Task(ngroups, true): one task per level and thread).
+ * FINISH_TIME: P2P_TIME (Task::constructMappingByFinishTime, merge/LevelTask.cpp:1647-1910): on
+ * each level the threads that finish first take the groups that can start first. All but
+ * FOUR_RULE are the Scheduler's (kind BAAS_KERNEL_ICCG only). The GPU plan does not depend on the
+ * mapping except through BAAS_PARTITION_BAAS_THREADS. */
+enum {
+    BAAS_MAPPING_FOUR_RULE = 0,
+    BAAS_MAPPING_COST_SPLIT = 1,
+    BAAS_MAPPING_COST_SPLIT_BARRIER = 2,
+    BAAS_MAPPING_FINISH_TIME = 3
+};
 
 /* How rows are given to CTAs. RANGES: contiguous row-index ranges, so every cross-CTA
  * dependency of the lower sweep points to an earlier CTA. BAAS_THREADS: CTA t runs the groups the

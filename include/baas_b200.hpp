@@ -35,8 +35,9 @@
 
 namespace baas_b200 {
 
-// test/Schedule.hpp:31-37. P2P_RULE (the BAAS four-rule mapping) and P2P (level merge and a
-// cost-balanced split per level) are built; P2P_MAPPING and P2P_TIME are not.
+// test/Schedule.hpp:31-37. P2P_RULE (the BAAS four-rule mapping), P2P (level merge and a
+// cost-balanced split per level) and P2P_TIME (earliest-finishing threads first) are built;
+// P2P_MAPPING is not.
 enum ALG_SCHEDULE { P2P, P2P_MAPPING, P2P_TIME, P2P_RULE };
 
 namespace detail {
@@ -114,9 +115,8 @@ class Scheduler {
         : csrA_(csrA), num_thread_(num_thread) {
         if (!isSymmetric) throw std::runtime_error("Scheduler: only the symmetric (IC0/ICCG) schedule is built");
         if (isTRSVPerm) throw std::runtime_error("Scheduler: the permuted (isTRSVPerm) variant is not built");
-        if (alg != P2P_RULE && alg != P2P)
-            throw std::runtime_error("Scheduler: P2P_MAPPING and P2P_TIME are not built (P2P_RULE, P2P are)");
-        mapping_ = alg == P2P ? BAAS_MAPPING_COST_SPLIT : BAAS_MAPPING_FOUR_RULE;
+        if (alg == P2P_MAPPING) throw std::runtime_error("Scheduler: P2P_MAPPING is not built (P2P_RULE, P2P, P2P_TIME are)");
+        mapping_ = alg == P2P ? BAAS_MAPPING_COST_SPLIT : (alg == P2P_TIME ? BAAS_MAPPING_FINISH_TIME : BAAS_MAPPING_FOUR_RULE);
     }
     ~Scheduler() { baas_destroy(s_); }
     Scheduler(const Scheduler &) = delete;

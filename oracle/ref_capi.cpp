@@ -202,8 +202,9 @@ static int g_mapping = BAAS_MAPPING_FOUR_RULE;
 
 extern "C"
 {
-    /* BAAS_MAPPING_*: FOUR_RULE builds the Scheduler with P2P_RULE, COST_SPLIT with P2P, and
-     * COST_SPLIT_BARRIER with P2P followed by the barrier-mode task layout. */
+    /* BAAS_MAPPING_*: FOUR_RULE builds the Scheduler with P2P_RULE, COST_SPLIT with P2P,
+     * COST_SPLIT_BARRIER with P2P followed by the barrier-mode task layout, FINISH_TIME with
+     * P2P_TIME. */
     void ref_set_mapping(int mapping) { g_mapping = mapping; }
 
     /* kind: a baas_kernel value. The matrix is the lower triangle incl. diagonal (diagonal last
@@ -224,8 +225,10 @@ extern "C"
         auto t0 = std::chrono::steady_clock::now();
         if (kind == BAAS_KERNEL_ICCG)
         {
-            const Schedule::ALG_SCHEDULE alg = g_mapping == BAAS_MAPPING_FOUR_RULE ? Schedule::ALG_SCHEDULE::P2P_RULE
-                                                                                  : Schedule::ALG_SCHEDULE::P2P;
+            const Schedule::ALG_SCHEDULE alg =
+                g_mapping == BAAS_MAPPING_FOUR_RULE
+                    ? Schedule::ALG_SCHEDULE::P2P_RULE
+                    : (g_mapping == BAAS_MAPPING_FINISH_TIME ? Schedule::ALG_SCHEDULE::P2P_TIME : Schedule::ALG_SCHEDULE::P2P);
             h->scheduler = new OpenScheduler(h->A, nthread, alg);
             h->scheduler->preprocessing();
             if (g_mapping == BAAS_MAPPING_COST_SPLIT_BARRIER)

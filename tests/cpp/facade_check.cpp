@@ -103,8 +103,8 @@ int main(int argc, char **argv) {
     } catch (const std::runtime_error &) {
     }
     try {
-        baas_b200::Scheduler<CSR> bad(&A, true, false, baas_b200::P2P_TIME, 8);
-        return fail("P2P_TIME accepted");
+        baas_b200::Scheduler<CSR> bad(&A, true, false, baas_b200::P2P_MAPPING, 8);
+        return fail("P2P_MAPPING accepted");
     } catch (const std::runtime_error &) {
     }
     // the P2P algorithm (level merge + cost split): a different task layout on the same groups

@@ -39,6 +39,9 @@ SCHEDULE_CASES = [
     # the Scheduler's P2P algorithm: level merge + cost split, and its barrier-mode task layout
     ("lap3d_8_p2p", 1, lambda: gen.laplace3d(8, 1e-3), (3, 8), 1),
     ("knn_200_p2p_barrier", 1, lambda: gen.knn_stiffness(nodes=200, k=12, seed=3), (4,), 2),
+    # P2P_TIME: earliest-finishing threads take the earliest-startable groups
+    ("lap3d_8_p2p_time", 1, lambda: gen.laplace3d(8, 1e-3), (3, 8), 3),
+    ("vardiff_30_p2p_time", 1, lambda: gen.vardiff2d(30, seed=2), (6,), 3),
 ]
 
 

@@ -139,9 +139,10 @@ def test_custom_partition_checks():
     assert np.array_equal(s.emulate_sweep(Lo, b), Port.lower_solve(Lo, b))
 
 
-@pytest.mark.parametrize("mapping", [1, 2])
-def test_cost_split_mapping_thread_partition_plan(mapping):
-    """CTA t runs virtual thread t of the Scheduler's P2P mapping (cost split per merged level)."""
+@pytest.mark.parametrize("mapping", [1, 2, 3])
+def test_scheduler_mapping_thread_partition_plan(mapping):
+    """CTA t runs virtual thread t of the Scheduler's P2P (cost split per merged level, both task
+    layouts) or P2P_TIME mapping."""
     A = gen.laplace3d(10, 1e-3)
     Lo, Up = _ic_lu(A)
     s = Schedule(A, kind=KERNEL_ICCG, nthread=12, partition=PARTITION_BAAS_THREADS, mapping=mapping)
