@@ -19,7 +19,7 @@ import numpy as np
 
 from . import _native
 from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, MAPPING_COST_SPLIT,
-                      MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_FOUR_RULE, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
+                      MAPPING_AFFINITY, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_FOUR_RULE, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
                       PARTITION_RANGES,
                       PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
@@ -27,7 +27,7 @@ from .gen import CSR
 __all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV",
            "KERNEL_ICCG", "KERNEL_IC0", "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "PARTITION_RANGES",
            "PARTITION_BAAS_THREADS", "PARTITION_CUSTOM", "MAPPING_FOUR_RULE", "MAPPING_COST_SPLIT",
-           "MAPPING_COST_SPLIT_BARRIER", "MAPPING_FINISH_TIME", "version"]
+           "MAPPING_COST_SPLIT_BARRIER", "MAPPING_FINISH_TIME", "MAPPING_AFFINITY", "version"]
 
 
 def version() -> str:

@@ -26,7 +26,7 @@ STATUS_NAMES = {
 KERNEL_SPTRSV, KERNEL_ICCG, KERNEL_IC0, KERNEL_ILU0 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32_FACTORS = 0, 1
 PARTITION_RANGES, PARTITION_BAAS_THREADS, PARTITION_CUSTOM = 0, 1, 2
-MAPPING_FOUR_RULE, MAPPING_COST_SPLIT, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME = 0, 1, 2, 3
+MAPPING_FOUR_RULE, MAPPING_COST_SPLIT, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_AFFINITY = 0, 1, 2, 3, 4
 
 FIELDS = {
     "ngroups": 0, "nlevels": 1, "ntasks": 2, "group_ptr": 3, "group_set": 4, "level_ptr": 5,

@@ -884,10 +884,10 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     if (o.parts < 0) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 0");
     if (o.smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
-    if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_FINISH_TIME)
+    if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_AFFINITY)
         return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
     if (o.mapping != BAAS_MAPPING_FOUR_RULE && kind != BAAS_KERNEL_ICCG)
-        return fail(BAAS_ERR_BAD_ARG, "the P2P, barrier and P2P_TIME mappings are the Scheduler's (kind BAAS_KERNEL_ICCG)");
+        return fail(BAAS_ERR_BAD_ARG, "the P2P, barrier, P2P_TIME and P2P_MAPPING mappings are the Scheduler's (kind BAAS_KERNEL_ICCG)");
     if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
     if (A->rowptr[A->n] != A->nnz) return fail(BAAS_ERR_BAD_ARG, "nnz != rowptr[n]");
     // value-source codes of the sweep plan address positions below 2^30
@@ -898,7 +898,10 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     baas_schedule *s = new baas_schedule();
     s->opt = o;
     s->nnz_a = A->nnz;
-    baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping);
+    if (!baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping)) {
+        delete s;
+        return fail(BAAS_ERR_BAD_ARG, "the P2P_MAPPING scan left a group on a thread that does not execute");
+    }
     s->nnz_l = (int)s->hs.l_colidx.size();
     if (sk != baas::SchedKind::SpTRSV && s->nnz_a != 2 * s->nnz_l - A->n) {
         delete s;

@@ -12,6 +12,7 @@
 #include <cstdint>
 #include <limits>
 #include <numeric>
+#include <unordered_set>
 
 namespace baas {
 namespace {
@@ -704,6 +705,189 @@ void finish_time_map(HostSchedule &s, const Csx &dag_csr) {
     finish_mapping(s, task_rows, by_level_thread, level_single);
 }
 
+// Stage 9 of the affinity mapping, the Scheduler's P2P_MAPPING algorithm
+// (Task::constructMappingMergeSerial, merge/LevelTask.cpp:1206-1645). Level 0 is split by cost.
+// On every later level each group scores the threads of its parents within the level window
+// (`< LEVEL_WINDOW_SIZE` here, unlike the four-rule mapping's `<=`) and keeps its top
+// ceil(sqrt(min(exec, nthread))) threads; the threads with the highest total share execute.
+// Groups go to their top thread when it executes (costs summed as ints, as the reference sums
+// them there). Overloaded threads give back groups from their end. The given-back and
+// unplaced groups then try their next-best threads, and finally fill the threads still under
+// the average. The reference iterates two std::unordered_set<int>, so the same containers and the
+// same sequence of reserve / clear / insert / erase calls are used here: under the same standard
+// library they iterate in the same order. False if the reference's scan would drop a group (its
+// leftover loop falls back to thread 0 when no executing thread is still filling).
+bool affinity_map(HostSchedule &s, const Csx &dag_csr) {
+    struct NodeScore {
+        int node;
+        int thread;
+        double score;
+    };
+    const int nl = s.nlevels, nt = s.nthread, nodes = s.ngroups;
+    const int *lp = s.level_ptr.data();
+    const int *p2o = s.perm_to_orig.data();
+    const int *o2p = s.perm.data();
+    const int *n2l = s.node_to_level.data();
+    std::vector<int> by_level_thread(nodes, -1), node_thread(nodes, -1);
+    std::vector<std::pair<int, int>> task_rows((size_t)nl * nt);
+    std::vector<int> level_single(nl, -1);
+    {
+        const int et = s.nthread_per_level[0];
+        const int lb = lp[0], le = lp[1];
+        std::vector<double> pre(le - lb + 1);
+        double load = 0.0;
+        for (int i = lb; i < le; i++) {
+            pre[i - lb] = load;
+            load += s.cost[p2o[i]];
+        }
+        const double per = (load + et - 1) / et;
+        int prev_end = lb, r = lb;
+        if (et == 1) level_single[0] = 0;
+        for (int t = 0; t < et; t++) {
+            int nr = r;
+            if (r < le) nr = lb + (int)(std::lower_bound(pre.begin() + (r - lb), pre.begin() + (le - lb), (t + 1) * per) - pre.begin());
+            r = nr;
+            const int b = prev_end, e = std::min(r, le);
+            prev_end = e;
+            task_rows[(size_t)t * nl + 0] = {b, e};
+            for (int k = b; k < e; k++) {
+                by_level_thread[k] = p2o[k];
+                node_thread[p2o[k]] = t;
+            }
+            ++r;
+        }
+        for (int t = et; t < nt; t++) task_rows[(size_t)t * nl + 0] = {le, le};
+    }
+    std::vector<double> node_score(nt), thread_load(nt), thread_score(nt);
+    std::vector<int> tidx(nt), thread_order(nt), disperse;
+    std::vector<std::vector<int>> tnodes(nt);
+    std::unordered_set<int> allocating;
+    std::unordered_set<int> chosen;
+    chosen.reserve(nt);
+    allocating.reserve(nt);
+    disperse.reserve(nodes);
+    const double alpha = 1.2;
+    for (int lvl = 1; lvl < nl; lvl++) {
+        const int lb = lp[lvl], le = lp[lvl + 1];
+        const int et = s.nthread_per_level[lvl];
+        const int width = le - lb;
+        chosen.clear();
+        disperse.clear();
+        allocating.clear();
+        std::fill(thread_load.begin(), thread_load.end(), 0.0);
+        std::fill(thread_score.begin(), thread_score.end(), 0.0);
+        std::iota(thread_order.begin(), thread_order.end(), 0);
+        for (auto &v : tnodes) v.clear();
+        const int sw = (int)std::ceil(std::sqrt((double)std::min(et, nt)));
+        std::vector<NodeScore> table((size_t)sw * width);
+        for (int i = lb; i < le; i++) {
+            std::fill(node_score.begin(), node_score.end(), 0.0);
+            const int node = p2o[i];
+            const int nlev = n2l[node];
+            for (int q = dag_csr.ptr[node]; q < dag_csr.ptr[node + 1] - 1; q++) {
+                const int par = dag_csr.idx[q];
+                const int diff = nlev - n2l[par];
+                if (diff < kLevelWindow)
+                    node_score[node_thread[par]] +=
+                        kAmplify * std::log2(1.0 * (s.group_ptr[par + 1] - s.group_ptr[par] + 1)) / std::log2(1.0 * (diff + 1));
+            }
+            std::iota(tidx.begin(), tidx.end(), 0);
+            std::partial_sort(tidx.begin(), tidx.begin() + sw, tidx.end(), [&](int a, int b) { return node_score[a] > node_score[b]; });
+            double total = 0.0;
+            for (int m = 0; m < sw; m++) {
+                const int t = tidx[m];
+                auto &en = table[(size_t)(i - lb) + (size_t)m * width];
+                en.node = node;
+                en.thread = t;
+                en.score = node_score[t];
+                total += node_score[t] * std::exp(-alpha * (m + 1));
+            }
+            for (int m = 0; m < sw; m++) {
+                const int t = tidx[m];
+                thread_score[t] += node_score[t] * std::exp(-alpha * (m + 1)) / total;
+            }
+        }
+        std::sort(table.begin(), table.begin() + width, [](NodeScore &a, NodeScore &b) {
+            if (a.thread != b.thread) return a.thread < b.thread;
+            return a.score > b.score;
+        });
+        std::sort(thread_order.begin(), thread_order.end(), [&](int a, int b) { return thread_score[a] > thread_score[b]; });
+        chosen.insert(thread_order.begin(), thread_order.begin() + et);
+        if (et == 1) level_single[lvl] = thread_order[0];
+        double level_load = 0;
+        for (int i = 0; i < width; i++) {
+            const NodeScore &it = table[i];
+            const int c = (int)s.cost[it.node];
+            level_load += c;
+            if (chosen.find(it.thread) != chosen.end()) {
+                tnodes[it.thread].push_back(it.node);
+                thread_load[it.thread] += c;
+            } else {
+                disperse.push_back(it.node);
+            }
+        }
+        const double avg = (level_load + et - 1) / et;
+        for (auto &t : chosen) {
+            if (thread_load[t] >= avg) {
+                int node = tnodes[t].back();
+                while (thread_load[t] - s.cost[node] >= avg) {
+                    disperse.push_back(node);
+                    tnodes[t].pop_back();
+                    thread_load[t] -= s.cost[node];
+                    node = tnodes[t].back();
+                }
+            } else {
+                allocating.insert(t);
+            }
+        }
+        int ndisp = 0;
+        for (size_t i = 0; i < disperse.size(); i++) {
+            const int node = disperse[i];
+            bool placed = false;
+            for (int w = 1; w < sw; w++) {
+                const int p = table[(size_t)w * width + (size_t)(o2p[node] - lb)].thread;
+                if (allocating.find(p) != allocating.end()) {
+                    thread_load[p] += s.cost[node];
+                    tnodes[p].push_back(node);
+                    if (thread_load[p] >= avg) allocating.erase(p);
+                    placed = true;
+                    break;
+                }
+            }
+            if (!placed) disperse[ndisp++] = node;
+        }
+        auto iter = allocating.begin();
+        int ai = 0, t = 0;
+        while (ai < ndisp && iter != allocating.end()) {
+            t = *iter;
+            while (thread_load[t] <= avg && ai < ndisp) {
+                const int node = disperse[ai++];
+                thread_load[t] += s.cost[node];
+                tnodes[t].push_back(node);
+            }
+            iter++;
+        }
+        while (ai < ndisp) tnodes[t].push_back(disperse[ai++]);
+        int pos = lb;
+        for (int th = 0; th < nt; th++) {
+            auto &tr = task_rows[(size_t)th * nl + lvl];
+            if (chosen.find(th) != chosen.end()) {
+                tr = {pos, pos + (int)tnodes[th].size()};
+                for (int v : tnodes[th]) {
+                    if (pos >= le) return false;
+                    by_level_thread[pos++] = v;
+                    node_thread[v] = th;
+                }
+            } else {
+                tr = {pos, pos};
+            }
+        }
+        if (pos != le) return false;  // a group was left on a thread that does not execute
+    }
+    finish_mapping(s, task_rows, by_level_thread, level_single);
+    return true;
+}
+
 // Stage 10: for every task, the sorted set of tasks on other threads that own a parent group.
 void task_dags(HostSchedule &s, const Csx &dag_csr) {
     const int nt = s.nthread, ntask = s.ntasks;
@@ -757,7 +941,7 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
     return "";
 }
 
-void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
+bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
                     Mapping mapping) {
     auto t0 = std::chrono::steady_clock::now();
     s = HostSchedule();
@@ -815,7 +999,7 @@ void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         }
 
     level_sets(fdag, s);  // stage 7
-    if (mapping == Mapping::FourRule || mapping == Mapping::FinishTime)
+    if (mapping == Mapping::FourRule || mapping == Mapping::FinishTime || mapping == Mapping::Affinity)
         threads_per_level(s);  // stage 8
     else
         merge_levels_group(s);
@@ -826,6 +1010,9 @@ void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         four_rule_map(s, dag_csr);  // stage 9
     else if (mapping == Mapping::FinishTime)
         finish_time_map(s, dag_csr);
+    else if (mapping == Mapping::Affinity) {
+        if (!affinity_map(s, dag_csr)) return false;
+    }
     else
         cost_split_map(s, mapping == Mapping::CostSplitBarrier);
     task_dags(s, dag_csr);          // stage 10
@@ -833,6 +1020,7 @@ void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
     s.fdag_set = std::move(fdag.idx);
     auto t1 = std::chrono::steady_clock::now();
     s.analysis_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return true;
 }
 
 }  // namespace baas

@@ -60,11 +60,13 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
 // How groups are mapped to virtual threads: the BAAS four-rule mapping (P2P_RULE); the
 // Scheduler's P2P algorithm -- level merge plus a cost-balanced contiguous split per level
 // (Task::constructTask), with one task per non-empty range or, in barrier mode, one per level
-// and thread; or P2P_TIME, earliest-finishing threads take the earliest-startable groups.
-enum class Mapping { FourRule = 0, CostSplit = 1, CostSplitBarrier = 2, FinishTime = 3 };
+// and thread; P2P_TIME, earliest-finishing threads take the earliest-startable groups; or
+// P2P_MAPPING, parent-thread affinity scores with load rebalancing.
+enum class Mapping { FourRule = 0, CostSplit = 1, CostSplitBarrier = 2, FinishTime = 3, Affinity = 4 };
 
-// Runs stages 1-10. `rowptr`/`colidx` are host arrays of the analysed matrix.
-void build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
+// Runs stages 1-10. `rowptr`/`colidx` are host arrays of the analysed matrix. False when the
+// affinity mapping would leave a group unmapped (the reference's P2P_MAPPING scan can).
+bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
                     Mapping mapping = Mapping::FourRule);
 
 }  // namespace baas

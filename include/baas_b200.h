@@ -119,14 +119,17 @@ typedef struct baas_options {
  * merge/LevelTask.cpp:42-196), one task per non-empty range. COST_SPLIT_BARRIER: the same split
  * with the barrier-mode task layout (Task(ngroups, true): one task per level and thread).
  * FINISH_TIME: P2P_TIME (Task::constructMappingByFinishTime, merge/LevelTask.cpp:1647-1910): on
- * each level the threads that finish first take the groups that can start first. All but
+ * each level the threads that finish first take the groups that can start first. AFFINITY:
+ * P2P_MAPPING (Task::constructMappingMergeSerial, merge/LevelTask.cpp:1206-1645): groups score
+ * their parents' threads, the best-scoring threads execute, loads are rebalanced. All but
  * FOUR_RULE are the Scheduler's (kind BAAS_KERNEL_ICCG only). The GPU plan does not depend on the
  * mapping except through BAAS_PARTITION_BAAS_THREADS. */
 enum {
     BAAS_MAPPING_FOUR_RULE = 0,
     BAAS_MAPPING_COST_SPLIT = 1,
     BAAS_MAPPING_COST_SPLIT_BARRIER = 2,
-    BAAS_MAPPING_FINISH_TIME = 3
+    BAAS_MAPPING_FINISH_TIME = 3,
+    BAAS_MAPPING_AFFINITY = 4
 };
 
 /* How rows are given to CTAs. RANGES: contiguous row-index ranges, so every cross-CTA

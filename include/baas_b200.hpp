@@ -35,9 +35,9 @@
 
 namespace baas_b200 {
 
-// test/Schedule.hpp:31-37. P2P_RULE (the BAAS four-rule mapping), P2P (level merge and a
-// cost-balanced split per level) and P2P_TIME (earliest-finishing threads first) are built;
-// P2P_MAPPING is not.
+// test/Schedule.hpp:31-37. All four are built: P2P_RULE (the BAAS four-rule mapping), P2P
+// (level merge and a cost-balanced split per level), P2P_MAPPING (parent-thread affinity with
+// load rebalancing) and P2P_TIME (earliest-finishing threads first).
 enum ALG_SCHEDULE { P2P, P2P_MAPPING, P2P_TIME, P2P_RULE };
 
 namespace detail {
@@ -115,8 +115,10 @@ class Scheduler {
         : csrA_(csrA), num_thread_(num_thread) {
         if (!isSymmetric) throw std::runtime_error("Scheduler: only the symmetric (IC0/ICCG) schedule is built");
         if (isTRSVPerm) throw std::runtime_error("Scheduler: the permuted (isTRSVPerm) variant is not built");
-        if (alg == P2P_MAPPING) throw std::runtime_error("Scheduler: P2P_MAPPING is not built (P2P_RULE, P2P, P2P_TIME are)");
-        mapping_ = alg == P2P ? BAAS_MAPPING_COST_SPLIT : (alg == P2P_TIME ? BAAS_MAPPING_FINISH_TIME : BAAS_MAPPING_FOUR_RULE);
+        mapping_ = alg == P2P           ? BAAS_MAPPING_COST_SPLIT
+                   : alg == P2P_TIME    ? BAAS_MAPPING_FINISH_TIME
+                   : alg == P2P_MAPPING ? BAAS_MAPPING_AFFINITY
+                                        : BAAS_MAPPING_FOUR_RULE;
     }
     ~Scheduler() { baas_destroy(s_); }
     Scheduler(const Scheduler &) = delete;

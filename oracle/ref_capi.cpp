@@ -204,7 +204,7 @@ extern "C"
 {
     /* BAAS_MAPPING_*: FOUR_RULE builds the Scheduler with P2P_RULE, COST_SPLIT with P2P,
      * COST_SPLIT_BARRIER with P2P followed by the barrier-mode task layout, FINISH_TIME with
-     * P2P_TIME. */
+     * P2P_TIME, AFFINITY with P2P_MAPPING. */
     void ref_set_mapping(int mapping) { g_mapping = mapping; }
 
     /* kind: a baas_kernel value. The matrix is the lower triangle incl. diagonal (diagonal last
@@ -228,7 +228,9 @@ extern "C"
             const Schedule::ALG_SCHEDULE alg =
                 g_mapping == BAAS_MAPPING_FOUR_RULE
                     ? Schedule::ALG_SCHEDULE::P2P_RULE
-                    : (g_mapping == BAAS_MAPPING_FINISH_TIME ? Schedule::ALG_SCHEDULE::P2P_TIME : Schedule::ALG_SCHEDULE::P2P);
+                    : (g_mapping == BAAS_MAPPING_FINISH_TIME ? Schedule::ALG_SCHEDULE::P2P_TIME
+                       : g_mapping == BAAS_MAPPING_AFFINITY  ? Schedule::ALG_SCHEDULE::P2P_MAPPING
+                                                             : Schedule::ALG_SCHEDULE::P2P);
             h->scheduler = new OpenScheduler(h->A, nthread, alg);
             h->scheduler->preprocessing();
             if (g_mapping == BAAS_MAPPING_COST_SPLIT_BARRIER)

@@ -102,11 +102,6 @@ int main(int argc, char **argv) {
         return fail("isTRSVPerm accepted");
     } catch (const std::runtime_error &) {
     }
-    try {
-        baas_b200::Scheduler<CSR> bad(&A, true, false, baas_b200::P2P_MAPPING, 8);
-        return fail("P2P_MAPPING accepted");
-    } catch (const std::runtime_error &) {
-    }
     // the P2P algorithm (level merge + cost split): a different task layout on the same groups
     baas_b200::Scheduler<CSR> p2p(&A, true, false, baas_b200::P2P, 8);
     p2p.preprocessing();

@@ -42,6 +42,9 @@ SCHEDULE_CASES = [
     # P2P_TIME: earliest-finishing threads take the earliest-startable groups
     ("lap3d_8_p2p_time", 1, lambda: gen.laplace3d(8, 1e-3), (3, 8), 3),
     ("vardiff_30_p2p_time", 1, lambda: gen.vardiff2d(30, seed=2), (6,), 3),
+    # P2P_MAPPING: parent-thread affinity with load rebalancing
+    ("lap3d_8_p2p_mapping", 1, lambda: gen.laplace3d(8, 1e-3), (3, 8), 4),
+    ("knn_200_p2p_mapping", 1, lambda: gen.knn_stiffness(nodes=200, k=12, seed=3), (5,), 4),
 ]
 
 

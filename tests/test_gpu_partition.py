@@ -57,10 +57,10 @@ def test_custom_partition_sweeps_ic0_iccg(blocks):
     assert np.array_equal(lu.cpu().numpy(), lu_o)
 
 
-@pytest.mark.parametrize("mapping", [1, 2, 3])
+@pytest.mark.parametrize("mapping", [1, 2, 3, 4])
 def test_scheduler_mapping_on_gpu(mapping):
-    """ICCG and the sweeps with CTA t running virtual thread t of the Scheduler's P2P or P2P_TIME
-    mapping."""
+    """ICCG and the sweeps with CTA t running virtual thread t of the Scheduler's P2P, P2P_TIME or
+    P2P_MAPPING mapping."""
     import torch
 
     from baas_b200 import PARTITION_BAAS_THREADS

@@ -139,10 +139,10 @@ def test_custom_partition_checks():
     assert np.array_equal(s.emulate_sweep(Lo, b), Port.lower_solve(Lo, b))
 
 
-@pytest.mark.parametrize("mapping", [1, 2, 3])
+@pytest.mark.parametrize("mapping", [1, 2, 3, 4])
 def test_scheduler_mapping_thread_partition_plan(mapping):
     """CTA t runs virtual thread t of the Scheduler's P2P (cost split per merged level, both task
-    layouts) or P2P_TIME mapping."""
+    layouts), P2P_TIME or P2P_MAPPING mapping."""
     A = gen.laplace3d(10, 1e-3)
     Lo, Up = _ic_lu(A)
     s = Schedule(A, kind=KERNEL_ICCG, nthread=12, partition=PARTITION_BAAS_THREADS, mapping=mapping)

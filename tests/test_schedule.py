@@ -90,12 +90,12 @@ MAPPED = [
 ]
 
 
-@pytest.mark.parametrize("mapping", [1, 2, 3])
+@pytest.mark.parametrize("mapping", [1, 2, 3, 4])
 @pytest.mark.parametrize("case", range(len(MAPPED)))
 def test_scheduler_mappings_match_live_reference(case, mapping, ref_lib):
     """The Scheduler's P2P algorithm (level merge + Task::constructTask), its barrier-mode task
-    layout and P2P_TIME (Task::constructMappingByFinishTime), every exported array against the
-    reference's."""
+    layout, P2P_TIME (Task::constructMappingByFinishTime) and P2P_MAPPING
+    (Task::constructMappingMergeSerial), every exported array against the reference's."""
     A = MAPPED[case]()
     for nt in (3, 8, 16):
         ours = Schedule(A, kind=KERNEL_ICCG, nthread=nt, mapping=mapping).arrays()
@@ -110,7 +110,7 @@ def test_mapping_checks():
     with pytest.raises(BaasError):
         Schedule(gen.laplace2d(8).lower(), kind=KERNEL_SPTRSV, mapping=1)  # the Scheduler's (ICCG) only
     with pytest.raises(BaasError):
-        Schedule(gen.laplace3d(4, 1e-3), kind=KERNEL_ICCG, mapping=4)
+        Schedule(gen.laplace3d(4, 1e-3), kind=KERNEL_ICCG, mapping=5)
     s = Schedule(gen.laplace3d(4, 1e-3), kind=KERNEL_ICCG, mapping=1)
     s.replan(parts=2)  # keeps the analysed mapping
 
