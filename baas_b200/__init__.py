@@ -275,6 +275,7 @@ class BatchSchedule(Schedule):
         self.nnz = A.nnz
         self.kind = KERNEL_ICCG
         self.nthread = nthread
+        self.mapping = MAPPING_FOUR_RULE  # batched analyses use the four-rule mapping
 
     def iccg_batched(self, A: DeviceCSR, B, X, tol: float = 1e-10, maxiter: int = 2000,
                      precision: int = PREC_FP64, stream=None, raise_on_nonconvergence: bool = True):

@@ -149,3 +149,12 @@ def test_scheduler_mapping_thread_partition_plan(mapping):
     r = gen.uniform_rhs(A.n, 1)
     assert np.array_equal(s.emulate_sweep(Lo, r), Port.lower_solve(Lo, r))
     assert np.array_equal(s.emulate_sweep(Up, r, upper=True), Port.upper_solve(Up, r, descending=True))
+
+
+def test_batch_schedule_replan_keeps_analysis():
+    """BatchSchedule.replan (the autotuner's call) rebuilds only the device plan."""
+    from baas_b200 import BatchSchedule
+
+    bs = BatchSchedule([gen.laplace2d(8), gen.vardiff2d(10, seed=1)], parts=3)
+    bs.replan(parts=2, smem_budget=64 * 1024)
+    bs.replan(parts=3)
