@@ -255,7 +255,8 @@ __device__ __forceinline__ double div_fast(double a, double b, double y, bool &s
     return q2;
 }
 
-// div_fast with its fall-back: always RN(a/b).
+// div_fast with its fall-back: always RN(a/b). The sweeps do not use it (they repeat a flagged
+// launch instead); baas_test_divide does, to check div_fast quotient by quotient.
 __device__ __forceinline__ double div_rcp(double a, double b, double y) {
     bool slow = false;
     const double q = div_fast(a, b, y, slow);

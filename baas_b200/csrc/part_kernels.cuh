@@ -1,22 +1,20 @@
-// Partitioned, level-synchronous kernels: the production execution of the BAAS hot path.
+// Partitioned, level-synchronous factorisation kernels (IC0, ILU0): the factor step of the BAAS
+// hot path. (The triangular sweeps run from the chunked plan of staged.cuh.)
 //
-// Rows are owned by P CTAs (contiguous row ranges by default; one 512-thread CTA per SM). The
-// schedule's coarsened groups are the work items, and each CTA walks the schedule's global
-// group levels in order: at level l it runs its own groups of level l (one group per thread,
-// the group's rows in ascending order, exactly as one reference thread runs a group,
-// merge/SpTRSV.cpp:458-471), then a CTA barrier. So
+// Rows are owned by P CTAs (contiguous row ranges by default; one CTA per SM). The schedule's
+// coarsened groups are the work items, and each CTA walks the group DAG's dependency levels in
+// order: at level l it runs its own groups of level l (one group per thread, the group's rows in
+// ascending order, exactly as one reference thread runs a group, merge/SpTRSV.cpp:458-471),
+// then a CTA barrier. So
 //   - a dependency on a row of the same CTA needs no wait at all: the barrier (or program
-//     order, inside a group) already made it visible, and its value is read from shared memory;
-//   - a dependency on a row of another CTA is a point-to-point wait on that row's global slot
-//     (the value itself is the ready flag for the sweeps; a release/acquire row flag for the
-//     factorisations), the analogue of the reference's taskFinsished waits
+//     order, inside a group) already made it visible;
+//   - a dependency on a row of another CTA is a point-to-point wait on that row's epoch-stamped
+//     release/acquire flag, the analogue of the reference's taskFinsished waits
 //     (merge/include/SpTRSV.hpp:16-35).
 // A group of level l depends only on groups of levels < l and every CTA walks the levels in
 // the same increasing order, so by induction on l every CTA finishes every level: no deadlock
 // while all CTAs are resident (cooperative launch). With contiguous row ranges every cross-CTA
-// dependency of the lower sweep points to a later CTA, so a downstream CTA settles at a fixed
-// lag behind its upstream neighbour: the L2 hop (~360 ns one way on B200) is paid once per
-// range boundary on the critical path, not once per level.
+// dependency points to an earlier CTA.
 //
 // Dependency encoding per factor entry: dep >= 0 is a global row index (remote), dep < 0 is
 // -(slot + 1) with slot the CTA-local index of a row computed earlier by this CTA.

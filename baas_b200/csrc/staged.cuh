@@ -12,7 +12,7 @@
 //               padded to 8 ints
 //   value block [diag (nl) | 1/diag (nl) | val (nl*E)], padded to 4 values
 // with E the widest row of the CTA (one stride for all of a CTA's chunks, so the walk is
-// specialised on it once per window), and row `pos` finds its entries at pos*E + j.
+// specialised on it once per direction), and row `pos` finds its entries at pos*E + j.
 // nl_next is the next chunk's row count (what the pipelined walk needs to address it early).
 // dep >= 0 is a CTA-local solution slot (final after the barrier that ended the producing
 // step); dep < 0 is -(row+1) of a row owned by another CTA (a value-as-flag wait on its global
