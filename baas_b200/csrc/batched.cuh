@@ -140,6 +140,93 @@ __device__ __forceinline__ void batch_totals(const BatchArgs &A, int buf, const 
     __syncthreads();
 }
 
+// Element-wise row loops of the vector phases. Each thread issues the loads of several rows
+// before the stores of any of them (a row loop that stores between its loads keeps one row's
+// loads in flight at a time), and adds its rows to its sums in the order of a row-at-a-time loop,
+// so every sum keeps its bits. The arrays a loop reads are written by other phases of the launch,
+// so they are read through plain pointers (never the read-only path).
+constexpr int kVecRows = 4;  // rows in flight per thread
+
+// Right-hand side r on rows [a, b): x += alpha p, r -= alpha Ap (act), acc += r.r, z sentinel.
+template <typename T>
+__device__ __forceinline__ double batch_update_rows(double *__restrict__ x, double *__restrict__ rr,
+                                                    const double *p, const double *Ap, T *__restrict__ zg, int a,
+                                                    int b, bool act, double alpha, double acc) {
+    const int bd = blockDim.x;
+    for (int i0 = a + (int)threadIdx.x; i0 < b; i0 += kVecRows * bd) {
+        double xv[kVecRows], rv[kVecRows], pv[kVecRows], av[kVecRows];
+#pragma unroll
+        for (int u = 0; u < kVecRows; u++) {
+            const int i = i0 + u * bd;
+            if (i < b) {
+                rv[u] = rr[i];
+                if (act) {
+                    xv[u] = x[i];
+                    pv[u] = p[i];
+                    av[u] = Ap[i];
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kVecRows; u++) {
+            const int i = i0 + u * bd;
+            if (i < b) {
+                if (act) {
+                    x[i] = __dadd_rn(xv[u], __dmul_rn(alpha, pv[u]));
+                    rv[u] = __dadd_rn(rv[u], __dmul_rn(-alpha, av[u]));
+                    rr[i] = rv[u];
+                }
+                acc = __dadd_rn(acc, __dmul_rn(rv[u], rv[u]));
+                zg[i] = Sent<T>::value();
+            }
+        }
+    }
+    return acc;
+}
+
+// Right-hand side r on rows [a, b): acc += r.z.
+template <typename T>
+__device__ __forceinline__ double batch_rz_rows(const double *rr, const T *zg, int a, int b, double acc) {
+    const int bd = blockDim.x;
+    for (int i0 = a + (int)threadIdx.x; i0 < b; i0 += kVecRows * bd) {
+        double rv[kVecRows], zv[kVecRows];
+#pragma unroll
+        for (int u = 0; u < kVecRows; u++) {
+            const int i = i0 + u * bd;
+            if (i < b) {
+                rv[u] = rr[i];
+                zv[u] = (double)Sent<T>::load(zg + i);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kVecRows; u++)
+            if (i0 + u * bd < b) acc = __dadd_rn(acc, __dmul_rn(rv[u], zv[u]));
+    }
+    return acc;
+}
+
+// Right-hand side r on rows [a, b): p = z + beta p.
+template <typename T>
+__device__ __forceinline__ void batch_p_rows(double *__restrict__ p, const T *zg, int a, int b, double beta) {
+    const int bd = blockDim.x;
+    for (int i0 = a + (int)threadIdx.x; i0 < b; i0 += kVecRows * bd) {
+        double pv[kVecRows], zv[kVecRows];
+#pragma unroll
+        for (int u = 0; u < kVecRows; u++) {
+            const int i = i0 + u * bd;
+            if (i < b) {
+                pv[u] = p[i];
+                zv[u] = (double)Sent<T>::load(zg + i);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kVecRows; u++) {
+            const int i = i0 + u * bd;
+            if (i < b) p[i] = __dadd_rn(zv[u], __dmul_rn(beta, pv[u]));
+        }
+    }
+}
+
 template <typename T, bool MR, bool IEEE>
 __device__ __forceinline__ bool batch_precond(const BatchArgs &A, WinStream<T> &ws, unsigned char *smem, Waiter &w) {
     T *yg = sizeof(T) == 8 ? (T *)A.y : (T *)A.y32;
@@ -284,20 +371,13 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_batched(BatchArgs A) {
                 act[r] = r < R ? sc.act[ls * kMaxRhs + r] : 0;
                 alpha[r] = act[r] ? sc.rz[ls * kMaxRhs + r] / sc.t[ls * kMaxRhs + r] : 0.0;
             }
-            for (int i = a + (int)threadIdx.x; i < b; i += blockDim.x)
 #pragma unroll
-                for (int r = 0; r < kMaxRhs; r++)
-                    if (r < R) {
-                        const size_t q = (size_t)r * n + i;
-                        double ri = A.r[q];
-                        if (act[r]) {
-                            A.X[(size_t)r * A.ldb + i] = __dadd_rn(A.X[(size_t)r * A.ldb + i], __dmul_rn(alpha[r], A.p[q]));
-                            ri = __dadd_rn(ri, __dmul_rn(-alpha[r], A.Ap[q]));
-                            A.r[q] = ri;
-                        }
-                        acc[r] = __dadd_rn(acc[r], __dmul_rn(ri, ri));
-                        zg[q] = Sent<T>::value();
-                    }
+            for (int r = 0; r < kMaxRhs; r++)
+                if (r < R) {
+                    const size_t o = (size_t)r * n;
+                    acc[r] = batch_update_rows<T>(A.X + (size_t)r * A.ldb, A.r + o, A.p + o, A.Ap + o, zg + o, a, b,
+                                                  act[r] != 0, alpha[r], acc[r]);
+                }
         });
         BAAS_BARRIER();
         batch_totals(A, red++ & 1, sc);
@@ -325,13 +405,9 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_batched(BatchArgs A) {
         }
         BAAS_BARRIER();
         batch_partials(A, red & 1, [&](int a, int b, int, double (&acc)[kMaxRhs]) {
-            for (int i = a + (int)threadIdx.x; i < b; i += blockDim.x)
 #pragma unroll
-                for (int r = 0; r < kMaxRhs; r++)
-                    if (r < R) {
-                        const size_t q = (size_t)r * n + i;
-                        acc[r] = __dadd_rn(acc[r], __dmul_rn(A.r[q], (double)Sent<T>::load(zg + q)));
-                    }
+            for (int r = 0; r < kMaxRhs; r++)
+                if (r < R) acc[r] = batch_rz_rows<T>(A.r + (size_t)r * n, zg + (size_t)r * n, a, b, acc[r]);
         });
         BAAS_BARRIER();
         // every CTA reads the same count after this barrier
@@ -349,13 +425,9 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_batched(BatchArgs A) {
                 act[r] = r < R ? sc.act[ls * kMaxRhs + r] : 0;
                 beta[r] = act[r] ? sc.t[ls * kMaxRhs + r] / sc.rz[ls * kMaxRhs + r] : 0.0;
             }
-            for (int i = a + (int)threadIdx.x; i < b; i += blockDim.x)
 #pragma unroll
-                for (int r = 0; r < kMaxRhs; r++)
-                    if (r < R && act[r]) {
-                        const size_t q = (size_t)r * n + i;
-                        A.p[q] = __dadd_rn((double)Sent<T>::load(zg + q), __dmul_rn(beta[r], A.p[q]));
-                    }
+            for (int r = 0; r < kMaxRhs; r++)
+                if (r < R && act[r]) batch_p_rows<T>(A.p + (size_t)r * n, zg + (size_t)r * n, a, b, beta[r]);
         }
         __syncthreads();
         for (int q = threadIdx.x; q < nls * kMaxRhs; q += blockDim.x)
