@@ -227,7 +227,7 @@ __device__ __forceinline__ void batch_p_rows(double *__restrict__ p, const T *zg
     }
 }
 
-template <typename T, bool MR, bool IEEE>
+template <typename T, bool MR, bool IEEE, int RW>
 __device__ __forceinline__ bool batch_precond(const BatchArgs &A, WinStream<T> &ws, unsigned char *smem, Waiter &w) {
     T *yg = sizeof(T) == 8 ? (T *)A.y : (T *)A.y32;
     T *zg = sizeof(T) == 8 ? (T *)A.z : (T *)A.z32;
@@ -235,15 +235,16 @@ __device__ __forceinline__ bool batch_precond(const BatchArgs &A, WinStream<T> &
     const int n0 = ws.ctl->n0;
     {
         const WalkIO<T, double, MR, false> lo{xs, yg, A.r, nullptr, A.n, A.n, A.bp.R};
-        if (!walk_dir<T, double, false, MR, false, kDiv<T, IEEE>>(ws, 0, n0, lo, w, A.spin_limit, A.st)) return false;
+        if (!walk_dir<T, double, false, MR, false, kDiv<T, IEEE>, RW>(ws, 0, n0, lo, w, A.spin_limit, A.st)) return false;
     }
     const WalkIO<T, T, MR, false> up{xs, zg, yg, nullptr, A.n, A.n, A.bp.R};
-    return walk_dir<T, T, true, MR, false, kDiv<T, IEEE>>(ws, n0, ws.total(), up, w, A.spin_limit, A.st);
+    return walk_dir<T, T, true, MR, false, kDiv<T, IEEE>, RW>(ws, n0, ws.total(), up, w, A.spin_limit, A.st);
 }
 
 // IEEE (FP64 factors only): sweep divisions by __ddiv_rn, for the repeat of a launch whose
-// div_fast divisions left their range.
-template <typename T, bool MR, bool IEEE>
+// div_fast divisions left their range. RW = 4 (FP32 factors, 4 right-hand sides): the sweeps
+// take the row-wide walk.
+template <typename T, bool MR, bool IEEE, int RW>
 __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_batched(BatchArgs A) {
     constexpr bool kMixed = sizeof(T) == 4;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_batched(BatchArgs A) {
     }
     __syncthreads();
 
-    if (!batch_precond<T, MR, IEEE>(A, ws, smem, w)) {
+    if (!batch_precond<T, MR, IEEE, RW>(A, ws, smem, w)) {
         ws.drain(A.spin_limit);
         return;
     }
@@ -399,7 +400,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_batched(BatchArgs A) {
         }
         __syncthreads();
 
-        if (!batch_precond<T, MR, IEEE>(A, ws, smem, w)) {
+        if (!batch_precond<T, MR, IEEE, RW>(A, ws, smem, w)) {
             ws.drain(A.spin_limit);
             return;
         }

@@ -452,6 +452,173 @@ __device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsig
     return alive;
 }
 
+// ---------------------------------------------------------------------------------------
+// Row-wide multi-right-hand-side walk (FP32 factors, RW = 4 right-hand sides, not staged):
+// thread t takes rows t, t + blockDim, ... of every chunk with all RW right-hand sides. A row's
+// plan is then read once instead of once per right-hand side, its RW solves are independent
+// chains, and a chunk of up to blockDim rows is one pass instead of RW. The slot layout
+// (xs[slot * RW + r]), the operations and so every result are those of the MR walk, which gives
+// each (row, right-hand side) pair a thread of its own.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void sh_ld4(unsigned int a, float (&v)[4]) {
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "r"(a));
+}
+__device__ __forceinline__ void sh_st4(unsigned int a, const float (&v)[4]) {
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]));
+}
+
+template <typename RT, bool RL2, int RW>
+__device__ __forceinline__ void load_rhs_rw(int row, const WalkIO<float, RT, true, false> &io, float (&rh)[RW]) {
+#pragma unroll
+    for (int r = 0; r < RW; r++) {
+        const RT *src = io.rhs + (size_t)r * io.ldr + row;
+        if constexpr (RL2)
+            rh[r] = (float)Sent<RT>::load(src);
+        else
+            rh[r] = (float)*src;
+    }
+}
+
+template <typename RT, int RW, int EK>
+__device__ __forceinline__ void load_remote_rw(const RowDeps<EK> &p, const WalkIO<float, RT, true, false> &io,
+                                               float (&pf)[RW][EK]) {
+    bool rem = false;
+#pragma unroll
+    for (int j = 0; j < EK; j++) rem |= j < p.ne && p.d[j] < 0;
+    if (rem) {
+#pragma unroll
+        for (int r = 0; r < RW; r++)
+#pragma unroll
+            for (int j = 0; j < EK; j++)
+                pf[r][j] = Sent<float>::load(io.xg + (size_t)r * io.ldx + ((j < p.ne && p.d[j] < 0) ? -p.d[j] - 1 : p.row));
+    }
+}
+
+// row_compute for all RW right-hand sides of one row (DIV == 0: multiply by the stored 1/diag).
+template <typename RT, int RW, int EK>
+__device__ __forceinline__ bool row_compute_rw(const RowDeps<EK> &p, const RowVals<float, EK> &v, const float (&rh)[RW],
+                                               const float (&pf)[RW][EK], const WalkIO<float, RT, true, false> &io,
+                                               Waiter &w) {
+    static_assert(RW == 4, "the row-wide walk moves slots as 4-float vectors");
+    float xv[EK][RW];
+    bool miss = false;
+#pragma unroll
+    for (int j = 0; j < EK; j++) {
+        const int dj = p.d[j];
+        float loc[RW];
+        sh_ld4(io.xs_at((dj >= 0 ? dj : 0) * RW), loc);
+#pragma unroll
+        for (int r = 0; r < RW; r++) {
+            xv[j][r] = dj >= 0 ? loc[r] : pf[r][j];
+            miss |= j < p.ne && dj < 0 && Sent<float>::is(pf[r][j]);
+        }
+    }
+    if (miss) {
+#pragma unroll
+        for (int r = 0; r < RW; r++)
+#pragma unroll
+            for (int j = 0; j < EK; j++)
+                if (j < p.ne && p.d[j] < 0 && Sent<float>::is(xv[j][r]) &&
+                    !wait_value<float>(io.xg + (size_t)r * io.ldx + (-p.d[j] - 1), xv[j][r], w, -p.d[j] - 1))
+                    return false;
+    }
+    float o[RW];
+#pragma unroll
+    for (int r = 0; r < RW; r++) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int j = 0; j < EK; j++)
+            if (j < p.ne) sum = fmaf(xv[j][r], v.a[j], sum);
+        o[r] = (rh[r] - sum) * v.diag;  // FP32 value blocks hold 1/diag
+    }
+    if (v.sl >= 0) sh_st4(io.xs_at(v.sl * RW), o);
+#pragma unroll
+    for (int r = 0; r < RW; r++) Sent<float>::store(io.xg + (size_t)r * io.ldx + p.row, o[r]);
+    return true;
+}
+
+// walk_run_e with the row-wide mapping: the same window crossing and step pipeline, the
+// step-s+1 row's remote values and right-hand sides loaded before the barrier ending step s.
+template <typename RT, bool RL2, int RW, int EK>
+__device__ __forceinline__ bool walk_run_rw(WinStream<float> &ws, int &i, const unsigned char *buf, int nint,
+                                            const WalkIO<float, RT, true, false> &io, Waiter &w, unsigned int spin,
+                                            DevStatus *st) {
+    constexpr unsigned int S = sizeof(float);
+    const int lr = (int)threadIdx.x, stp = (int)blockDim.x;
+    unsigned int I0 = smem_u32(buf);
+    unsigned int Iend = I0 + 4u * (unsigned int)nint;
+    unsigned int V0 = Iend;
+    bool alive = true;
+    int nl0 = Sh<int>::ldu(I0);
+    RowDeps<EK> q0, q1;
+    float pf0[RW][EK];
+    float rh0[RW], rh1[RW];
+    bool m0 = lr < nl0;
+    if (m0) {
+        load_deps<EK>(I0, nl0, lr, q0);
+        load_remote_rw<RT, RW, EK>(q0, io, pf0);
+        load_rhs_rw<RT, RL2, RW>(q0.row, io, rh0);
+    }
+    for (;;) {
+        const int nl1 = Sh<int>::ldu(I0 + 8u);
+        unsigned int I1 = I0 + 4u * (unsigned int)chunk_nint(nl0, EK);
+        unsigned int V1 = V0 + S * (unsigned int)chunk_nval(nl0, EK);
+        unsigned int Iend1 = Iend;
+        const bool cross = nl1 != 0 && I1 == Iend;
+        bool okw = true;
+        if (cross) {
+            const unsigned char *nb;
+            int nn;
+            okw = ws.peek(i, spin, nb, nn);
+            I1 = smem_u32(nb);
+            Iend1 = I1 + 4u * (unsigned int)nn;
+            V1 = Iend1;
+        }
+        const bool m1 = okw && lr < nl1;
+        if (m1) load_deps<EK>(I1, nl1, lr, q1);
+        if (alive && m0) {
+            RowVals<float, EK> v;
+            load_vals<float, RT, RL2, true, false, EK>(I0, V0, nl0, lr, q0, io, v);
+            if (!row_compute_rw<RT, RW, EK>(q0, v, rh0, pf0, io, w)) alive = false;
+        }
+        for (int pos = lr + stp; alive && pos < nl0; pos += stp) {
+            RowDeps<EK> q;
+            RowVals<float, EK> v;
+            float qf[RW][EK], rh[RW];
+            load_deps<EK>(I0, nl0, pos, q);
+            load_vals<float, RT, RL2, true, false, EK>(I0, V0, nl0, pos, q, io, v);
+            load_rhs_rw<RT, RL2, RW>(q.row, io, rh);
+#pragma unroll
+            for (int r = 0; r < RW; r++)
+#pragma unroll
+                for (int j = 0; j < EK; j++) qf[r][j] = Sent<float>::value();
+            if (!row_compute_rw<RT, RW, EK>(q, v, rh, qf, io, w)) alive = false;
+        }
+        if (m1 && alive) {
+            load_remote_rw<RT, RW, EK>(q1, io, pf0);
+            load_rhs_rw<RT, RL2, RW>(q1.row, io, rh1);
+        }
+        if (cross) {
+            if (!okw && atomicCAS(&st->code, kOk, kTimeout) == kOk) st->where = -1000000 - i - 1;
+            if (__syncthreads_or(!okw || !alive)) return false;
+            ws.release(i);
+            i++;
+            Iend = Iend1;
+        } else {
+            __syncthreads();
+        }
+        if (nl1 == 0) break;
+        I0 = I1;
+        V0 = V1;
+        nl0 = nl1;
+        m0 = m1;
+        q0 = q1;
+#pragma unroll
+        for (int r = 0; r < RW; r++) rh0[r] = rh1[r];
+    }
+    return alive;
+}
+
 // Any entry stride (the CTA's widest row has more than 3 entries): plain loop, waits in place.
 template <typename T, typename RT, bool RL2, bool MR, bool STG, int DIV>
 __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, const T *V,
@@ -510,17 +677,31 @@ __device__ __forceinline__ bool walk_window_any(const int *I, const int *Iend, c
 // Walk the windows [i, iend) of one direction (all of a CTA's chunks in a direction share one
 // entry stride). Every thread passes every barrier, also after a failed wait, so the CTA never
 // splits; the result is uniform. Each window is released after its walk.
-template <typename T, typename RT, bool RL2, bool MR, bool STG, int DIV>
+// RW > 1: the row-wide walk (FP32 factors, MR, not staged, io.R_ == RW) for entry strides up to
+// 2; wider strides keep the MR walk (a stride-3 row-wide walk pushed the batched kernel to 255
+// registers with spills, and its 64-system batch ran 13% slower than with strides up to 2).
+template <typename T, typename RT, bool RL2, bool MR, bool STG, int DIV, int RW = 1>
 __device__ __forceinline__ bool walk_dir(WinStream<T> &ws, int i, int iend, const WalkIO<T, RT, MR, STG> &io,
                                          Waiter &w, unsigned int spin, DevStatus *st) {
+    static_assert(RW == 1 || (sizeof(T) == 4 && MR && !STG && DIV == 0), "row-wide walk: FP32, MR, not staged");
     const unsigned char *b;
     int nint;
     if (i >= iend) return true;
     if (!ws.acquire(i, spin, st, b, nint)) return false;
     bool alive = true;
     switch (Sh<int>::ld(reinterpret_cast<const int *>(b) + 1)) {
-        case 1: alive = walk_run_e<T, RT, RL2, MR, STG, DIV, 1>(ws, i, b, nint, io, w, spin, st); break;
-        case 2: alive = walk_run_e<T, RT, RL2, MR, STG, DIV, 2>(ws, i, b, nint, io, w, spin, st); break;
+        case 1:
+            if constexpr (RW > 1)
+                alive = walk_run_rw<RT, RL2, RW, 1>(ws, i, b, nint, io, w, spin, st);
+            else
+                alive = walk_run_e<T, RT, RL2, MR, STG, DIV, 1>(ws, i, b, nint, io, w, spin, st);
+            break;
+        case 2:
+            if constexpr (RW > 1)
+                alive = walk_run_rw<RT, RL2, RW, 2>(ws, i, b, nint, io, w, spin, st);
+            else
+                alive = walk_run_e<T, RT, RL2, MR, STG, DIV, 2>(ws, i, b, nint, io, w, spin, st);
+            break;
         case 3: alive = walk_run_e<T, RT, RL2, MR, STG, DIV, 3>(ws, i, b, nint, io, w, spin, st); break;
         default:
             for (;;) {
