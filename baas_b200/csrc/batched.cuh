@@ -242,8 +242,8 @@ __device__ __forceinline__ bool batch_precond(const BatchArgs &A, WinStream<T> &
 }
 
 // IEEE (FP64 factors only): sweep divisions by __ddiv_rn, for the repeat of a launch whose
-// div_fast divisions left their range. RW = 4 (FP32 factors, 4 right-hand sides): the sweeps
-// take the row-wide walk.
+// div_fast divisions left their range. RW = 2 or 4 (FP32 factors, that many right-hand sides):
+// the sweeps take the row-wide walk.
 template <typename T, bool MR, bool IEEE, int RW>
 __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_batched(BatchArgs A) {
     constexpr bool kMixed = sizeof(T) == 4;

@@ -682,10 +682,12 @@ void *iccg_kernel(bool mixed, bool stg, bool ieee) {
     if (ieee) return stg ? (void *)baas::k_iccg_chunked<double, true, true> : (void *)baas::k_iccg_chunked<double, false, true>;
     return stg ? (void *)baas::k_iccg_chunked<double, true, false> : (void *)baas::k_iccg_chunked<double, false, false>;
 }
-// rw4: FP32 factors with exactly 4 right-hand sides take the row-wide sweeps (one thread per row
-// for all four); BAAS_BATCH_PAIRS=1 keeps the one-pair-per-thread sweeps (same results).
-void *batched_kernel(bool mixed, bool mr, bool ieee, bool rw4 = false) {
-    if (mixed && mr && rw4) return (void *)baas::k_iccg_batched<float, true, false, 4>;
+// rw: FP32 factors with exactly 2 or 4 right-hand sides take the row-wide sweeps (one thread per
+// row for all of them; rw = that count, else 1); BAAS_BATCH_PAIRS=1 keeps the
+// one-pair-per-thread sweeps (same results).
+void *batched_kernel(bool mixed, bool mr, bool ieee, int rw = 1) {
+    if (mixed && mr && rw == 4) return (void *)baas::k_iccg_batched<float, true, false, 4>;
+    if (mixed && mr && rw == 2) return (void *)baas::k_iccg_batched<float, true, false, 2>;
     if (mixed) return mr ? (void *)baas::k_iccg_batched<float, true, false, 1> : (void *)baas::k_iccg_batched<float, false, false, 1>;
     if (ieee) return mr ? (void *)baas::k_iccg_batched<double, true, true, 1> : (void *)baas::k_iccg_batched<double, false, true, 1>;
     return mr ? (void *)baas::k_iccg_batched<double, true, false, 1> : (void *)baas::k_iccg_batched<double, false, false, 1>;
@@ -756,7 +758,7 @@ baas_status ensure_device(baas_schedule *s) {
         for (int v = 0; v < 8; v++) {
             const bool a = v & 1, b = v & 2, c = v & 4;
             const void *kerns[] = {sweep_kernel(a, b, c), iccg_kernel(a, b, c), batched_kernel(a, b, c),
-                                   batched_kernel(true, true, false, true)};
+                                   batched_kernel(true, true, false, 4), batched_kernel(true, true, false, 2)};
             for (const void *k : kerns)
                 BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
         }
@@ -1494,7 +1496,8 @@ baas_status baas_iccg_batched(baas_schedule *s, const baas_csr *A, const double 
     if (smem > (size_t)kMaxDynSmem) return fail(BAAS_ERR_BAD_ARG, "batched solve: shared memory over budget");
     void *args[] = {(void *)&a};
     const bool mr = nrhs > 1;
-    const bool rw4 = mixed && nrhs == 4 && !(getenv("BAAS_BATCH_PAIRS") && atoi(getenv("BAAS_BATCH_PAIRS")) > 0);
+    const bool pairs = getenv("BAAS_BATCH_PAIRS") && atoi(getenv("BAAS_BATCH_PAIRS")) > 0;
+    const int rw = mixed && (nrhs == 2 || nrhs == 4) && !pairs ? nrhs : 1;
     for (int ieee = 0; ieee < 2; ieee++) {
         if (ieee) BAAS_CUDA(cudaMemcpyAsync(X, s->d_x0, sizeof(double) * xcount, cudaMemcpyDeviceToDevice, stream));
         BAAS_TRY(next_epoch(s, stream));
@@ -1502,7 +1505,7 @@ baas_status baas_iccg_batched(baas_schedule *s, const baas_csr *A, const double 
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
         BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
         BAAS_CUDA(cudaMemcpyAsync(s->d_active, &active, sizeof(active), cudaMemcpyHostToDevice, stream));
-        BAAS_CUDA(cudaLaunchCooperativeKernel(batched_kernel(mixed, mr, ieee != 0, rw4), P, baas::kStageBlock, args, smem,
+        BAAS_CUDA(cudaLaunchCooperativeKernel(batched_kernel(mixed, mr, ieee != 0, rw), P, baas::kStageBlock, args, smem,
                                               stream));
         BAAS_CUDA(cudaMemcpyAsync(iters, s->d_biters, sizeof(int) * (size_t)s->nsys * nrhs, cudaMemcpyDeviceToHost, stream));
         BAAS_CUDA(cudaMemcpyAsync(relres, s->d_brelres, sizeof(double) * (size_t)s->nsys * nrhs, cudaMemcpyDeviceToHost,

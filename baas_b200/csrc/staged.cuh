@@ -453,18 +453,24 @@ __device__ __forceinline__ bool walk_run_e(WinStream<T> &ws, int &i, const unsig
 }
 
 // ---------------------------------------------------------------------------------------
-// Row-wide multi-right-hand-side walk (FP32 factors, RW = 4 right-hand sides, not staged):
+// Row-wide multi-right-hand-side walk (FP32 factors, RW = 2 or 4 right-hand sides, not staged):
 // thread t takes rows t, t + blockDim, ... of every chunk with all RW right-hand sides. A row's
 // plan is then read once instead of once per right-hand side, its RW solves are independent
 // chains, and a chunk of up to blockDim rows is one pass instead of RW. The slot layout
 // (xs[slot * RW + r]), the operations and so every result are those of the MR walk, which gives
 // each (row, right-hand side) pair a thread of its own.
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ void sh_ld4(unsigned int a, float (&v)[4]) {
+__device__ __forceinline__ void sh_ldv(unsigned int a, float (&v)[4]) {
     asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "r"(a));
 }
-__device__ __forceinline__ void sh_st4(unsigned int a, const float (&v)[4]) {
+__device__ __forceinline__ void sh_stv(unsigned int a, const float (&v)[4]) {
     asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]));
+}
+__device__ __forceinline__ void sh_ldv(unsigned int a, float (&v)[2]) {
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v[0]), "=f"(v[1]) : "r"(a));
+}
+__device__ __forceinline__ void sh_stv(unsigned int a, const float (&v)[2]) {
+    asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v[0]), "f"(v[1]));
 }
 
 template <typename RT, bool RL2, int RW>
@@ -499,14 +505,14 @@ template <typename RT, int RW, int EK>
 __device__ __forceinline__ bool row_compute_rw(const RowDeps<EK> &p, const RowVals<float, EK> &v, const float (&rh)[RW],
                                                const float (&pf)[RW][EK], const WalkIO<float, RT, true, false> &io,
                                                Waiter &w) {
-    static_assert(RW == 4, "the row-wide walk moves slots as 4-float vectors");
+    static_assert(RW == 2 || RW == 4, "the row-wide walk moves slots as 2- or 4-float vectors");
     float xv[EK][RW];
     bool miss = false;
 #pragma unroll
     for (int j = 0; j < EK; j++) {
         const int dj = p.d[j];
         float loc[RW];
-        sh_ld4(io.xs_at((dj >= 0 ? dj : 0) * RW), loc);
+        sh_ldv(io.xs_at((dj >= 0 ? dj : 0) * RW), loc);
 #pragma unroll
         for (int r = 0; r < RW; r++) {
             xv[j][r] = dj >= 0 ? loc[r] : pf[r][j];
@@ -531,7 +537,7 @@ __device__ __forceinline__ bool row_compute_rw(const RowDeps<EK> &p, const RowVa
             if (j < p.ne) sum = fmaf(xv[j][r], v.a[j], sum);
         o[r] = (rh[r] - sum) * v.diag;  // FP32 value blocks hold 1/diag
     }
-    if (v.sl >= 0) sh_st4(io.xs_at(v.sl * RW), o);
+    if (v.sl >= 0) sh_stv(io.xs_at(v.sl * RW), o);
 #pragma unroll
     for (int r = 0; r < RW; r++) Sent<float>::store(io.xg + (size_t)r * io.ldx + p.row, o[r]);
     return true;

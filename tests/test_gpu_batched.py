@@ -80,15 +80,16 @@ def test_batched_full_configuration():
         assert np.linalg.norm(x - xw) / np.linalg.norm(xw) < 1e-6
 
 
-def test_row_wide_sweeps_match_pair_sweeps(monkeypatch):
-    """FP32 factors with 4 right-hand sides sweep one row per thread for all four; the
+@pytest.mark.parametrize("nrhs", [2, 4])
+def test_row_wide_sweeps_match_pair_sweeps(monkeypatch, nrhs):
+    """FP32 factors with 2 or 4 right-hand sides sweep one row per thread for all of them; the
     one-pair-per-thread sweeps (BAAS_BATCH_PAIRS=1) must give the same bits, iterations and
     residuals, on systems wide enough that a level spans several passes of the pair mapping."""
     systems = [gen.vardiff2d(int(k), seed=30 + j) for j, k in enumerate((90, 40, 120, 7))]
     out = []
     for pairs in ("1", "0"):
         monkeypatch.setenv("BAAS_BATCH_PAIRS", pairs)
-        s, B, X, it, rel = _solve(systems, 4, PREC_FP32_FACTORS, parts=6)
+        s, B, X, it, rel = _solve(systems, nrhs, PREC_FP32_FACTORS, parts=6)
         out.append((X, it, rel))
     assert np.array_equal(out[0][0].view(np.int64), out[1][0].view(np.int64))
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
