@@ -229,8 +229,8 @@ baas_status baas_ic0(baas_schedule *s, const baas_csr *A, double *lu, void *stre
 
 /* IC0 that allocates no memory, for callers that cannot call cudaMalloc at the moment they
  * factor: a hot loop of a real-time or latency-bound application that reserved all of its
- * memory up front, code that runs while a CUDA graph is being captured (where cudaMalloc is
- * not allowed), or a host framework whose device memory belongs to its own allocator.
+ * memory up front, a plug-in whose host application forbids device allocation after start-up,
+ * or a host framework whose device memory belongs to its own allocator.
  * No counterpart in the reference (its CPU routines malloc freely).
  *
  * Same arguments, arithmetic and result as baas_ic0 (bit-identical factor). Its scratch -- one

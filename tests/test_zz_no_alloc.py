@@ -1,6 +1,6 @@
 """baas_ic0_noalloc: the IC0 entry point that allocates nothing, for callers that cannot call
-cudaMalloc when they factor (pre-reserved real-time loops, code running during CUDA graph
-capture, hosts whose device memory belongs to another allocator). Its scratch is a static
+cudaMalloc when they factor (pre-reserved real-time loops, plug-ins whose host forbids device
+allocation after start-up, hosts whose device memory belongs to another allocator). Its scratch is a static
 device array inside the library, shared by every call.
 
 This file is collected last on purpose: if it fails, a run that stops at the first failure has
