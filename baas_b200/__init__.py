@@ -200,14 +200,16 @@ class Schedule:
         _native.check(_native.lib().baas_ilu0(self._h, C.byref(c), _ptr(lu), _stream_ptr(stream)), "baas_ilu0")
 
     def iccg(self, A: DeviceCSR, b, x, tol: float = 1e-10, maxiter: int = 2000, precision: int = PREC_FP64,
-             stream=None, raise_on_nonconvergence: bool = True):
-        """IC0-PCG solve; x holds the initial guess. Returns (iterations, relative residual)."""
+             stream=None, raise_on_nonconvergence: bool = True, raise_on_zero_pivot: bool = True):
+        """IC0-PCG solve; x holds the initial guess. Returns (iterations, relative residual).
+        raise_on_zero_pivot=False accepts a factor with non-positive pivots, which IC0 leaves
+        unchanged as the reference does (merge/IC.cpp:371-378), and returns the solve's result."""
         c = A.c()
         it = C.c_int(0)
         rr = C.c_double(0.0)
         st = _native.lib().baas_iccg(self._h, C.byref(c), _ptr(b), _ptr(x), tol, maxiter, precision,
                                      C.byref(it), C.byref(rr), _stream_ptr(stream))
-        if st == 5 and not raise_on_nonconvergence:
+        if (st == 5 and not raise_on_nonconvergence) or (st == 4 and not raise_on_zero_pivot):
             return it.value, rr.value
         _native.check(st, "baas_iccg")
         return it.value, rr.value

@@ -104,6 +104,20 @@ def random_symmetric_permutation(n: int, seed: int) -> np.ndarray:
     return np.random.default_rng(seed).permutation(n).astype(np.int32)
 
 
+# Configuration 2: the 64^3 7-point Laplacian with diagonal shift 1e-3, in natural order and under
+# a seeded random symmetric permutation; right-hand side b ~ U(-1, 1) with seed 1.
+C2_GRID = 64
+C2_SHIFT = 1e-3
+C2_PERMUTATION_SEED = 1
+C2_RHS_SEED = 1
+
+
+def c2_system(permuted: bool = False, k: int = C2_GRID) -> CSR:
+    """The configuration-2 matrix, natural order or P A P^T with the seeded permutation."""
+    A = laplace3d(k, C2_SHIFT)
+    return A.permuted(random_symmetric_permutation(A.n, C2_PERMUTATION_SEED)) if permuted else A
+
+
 def convdiff3d(k: int, velocity=(1.0, 0.5, 0.25), peclet: float = 10.0) -> CSR:
     """Nonsymmetric 7-point convection-diffusion on a k^3 grid (Dirichlet boundary).
 

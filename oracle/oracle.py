@@ -257,3 +257,27 @@ class Port:
         it = Port.lib().orc_pcg(A.n, _p(A.rowptr), _p(A.colidx), _p(A.values), _p(bc), _p(x),
                                 maxiter, tol, C.addressof(rel), None)
         return x, it, rel.value
+
+
+def _pcg_job(job):
+    """One oracle PCG solve in a worker process (top level, so a spawned worker can import it)."""
+    from baas_b200.gen import CSR as _CSR
+
+    n, rowptr, colidx, values, b, tol, maxiter = job
+    return Port.pcg(_CSR(n, rowptr, colidx, values), b, tol=tol, maxiter=maxiter)
+
+
+def pcg_many(jobs, workers=None):
+    """Port.pcg over many (A, b, tol, maxiter) jobs in a pool of spawned worker processes (spawned,
+    not forked, so a caller that already holds a CUDA context can use it). Returns the
+    (x, iterations, relres) triples in job order."""
+    import multiprocessing as mp
+    import os
+
+    packed = [(A.n, A.rowptr, A.colidx, A.values, np.ascontiguousarray(b, dtype=np.float64), tol, maxiter)
+              for A, b, tol, maxiter in jobs]
+    workers = max(1, min(len(packed), workers or os.cpu_count() or 1))
+    if workers == 1:
+        return [_pcg_job(j) for j in packed]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(_pcg_job, packed, chunksize=1)

@@ -1,6 +1,7 @@
 """Batched ICCG (baas_analyze_batch + baas_iccg_batched): many independent SPD systems with several
 right-hand sides each, in one persistent launch, checked per instance against the oracle's PCG
-(iterations within +-1 for FP64 factors, solutions within 1e-8) and by independent residuals."""
+(iterations within +-1 for FP64 factors, solutions within 1e-12 relative for FP64 factors and
+1e-9 for FP32 factors) and by independent residuals."""
 import numpy as np
 import pytest
 
@@ -41,7 +42,7 @@ def test_batched_small_matches_oracle(precision, nrhs):
             b = B[r, off[q]:off[q + 1]]
             xw, itw, _ = Port.pcg(m, b, tol=1e-10, maxiter=5000)
             x = X[r, off[q]:off[q + 1]]
-            assert np.linalg.norm(x - xw) / np.linalg.norm(xw) < 1e-8
+            assert np.linalg.norm(x - xw) / np.linalg.norm(xw) <= (1e-12 if precision == PREC_FP64 else 1e-9)
             if precision == PREC_FP64:
                 assert abs(int(it[q, r]) - itw) <= 1
 
@@ -63,7 +64,10 @@ def test_batched_zero_rhs_and_one_system():
 
 def test_batched_full_configuration():
     """64 systems, k ~ U[64, 512], 4 right-hand sides, FP32 factors; residuals recomputed on the
-    CPU, and three systems against the oracle in FP64."""
+    CPU, and every system against the FP64 oracle's PCG at the same tolerance (system q with
+    right-hand side q % 4; the oracle solves run in a pool of spawned processes)."""
+    from oracle.oracle import pcg_many
+
     systems = gen.batch_vardiff2d()
     s, B, X, it, rel = _solve(systems, 4, PREC_FP32_FACTORS)
     assert np.all(rel < 1e-10)
@@ -74,10 +78,14 @@ def test_batched_full_configuration():
         for q in range(len(systems)):
             sl = slice(off[q], off[q + 1])
             assert np.linalg.norm(res[sl]) / np.linalg.norm(B[r, sl]) < 1e-9
-    for q in (0, 17, 40):
-        xw, _, _ = Port.pcg(systems[q], B[0, off[q]:off[q + 1]], tol=1e-12, maxiter=20000)
-        x = X[0, off[q]:off[q + 1]]
-        assert np.linalg.norm(x - xw) / np.linalg.norm(xw) < 1e-6
+    jobs = [(m, B[q % 4, off[q]:off[q + 1]], 1e-10, 20000) for q, m in enumerate(systems)]
+    errs = []
+    for q, (xw, itw, relw) in enumerate(pcg_many(jobs)):
+        assert relw < 1e-10
+        x = X[q % 4, off[q]:off[q + 1]]
+        errs.append(np.linalg.norm(x - xw) / np.linalg.norm(xw))
+    print(f"FP32-factor batch vs FP64 oracle: max {max(errs):.3e}, median {np.median(errs):.3e}")
+    assert max(errs) <= 1e-8
 
 
 @pytest.mark.parametrize("nrhs", [2, 4])

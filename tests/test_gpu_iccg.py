@@ -26,7 +26,7 @@ def test_iccg_matches_oracle(k):
     assert rel < 1e-10
     xg = x.cpu().numpy()
     # both iterates converge to the same solution; the dot products differ only in summation order
-    assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) < 1e-8
+    assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) <= 1e-12
     res = np.linalg.norm(b - A.to_scipy() @ xg) / np.linalg.norm(b)
     assert res < 1e-9
 
@@ -41,7 +41,7 @@ def test_iccg_fp32_factors():
     assert rel < 1e-10
     assert it <= ito + max(3, ito // 10)
     xg = x.cpu().numpy()
-    assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) < 1e-7
+    assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) <= 1e-9  # FP32 factors vs the FP64 oracle
 
 
 def test_iccg_knn_stiffness():
@@ -52,7 +52,7 @@ def test_iccg_knn_stiffness():
     it, rel = s.iccg(DeviceCSR.from_host(A), _t(b), x, tol=1e-10, maxiter=2000, precision=PREC_FP64)
     xo, ito, _ = Port.pcg(A, b, tol=1e-10)
     assert abs(it - ito) <= 1
-    assert np.linalg.norm(x.cpu().numpy() - xo) / np.linalg.norm(xo) < 1e-8
+    assert np.linalg.norm(x.cpu().numpy() - xo) / np.linalg.norm(xo) <= 1e-12
 
 
 def test_iccg_repeat_and_permuted():

@@ -1,6 +1,10 @@
 """A matrix that arrives as a MatrixMarket file (baas_csr_read_mtx) through the GPU path: a k-NN
 stiffness-like SPD system written to a symmetric .mtx, read back, then IC0 bit-exact against the
-oracle and ICCG within +-1 iteration of the oracle's PCG."""
+oracle and ICCG within +-1 iteration of the oracle's PCG; and, where BAAS_MTX_DIR names a directory
+holding them, the reference's two SuiteSparse stiffness matrices through the same path."""
+import os
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -30,4 +34,61 @@ def test_mtx_file_to_gpu_solve(tmp_path):
     it, rel = s.iccg(dA, torch.from_numpy(b).cuda(), x, tol=1e-10, maxiter=5000)
     xo, ito, _ = Port.pcg(A, b, tol=1e-10, maxiter=5000)
     assert abs(it - ito) <= 1 and rel < 1e-10
-    assert np.linalg.norm(x.cpu().numpy() - xo) / np.linalg.norm(xo) < 1e-8
+    assert np.linalg.norm(x.cpu().numpy() - xo) / np.linalg.norm(xo) <= 1e-12
+
+
+# The reference's two SuiteSparse fixtures (its data/bcsstk18.mtx and data/bcsstk38.mtx) on the
+# GPU. They are not part of this repository: point BAAS_MTX_DIR at a directory holding them (for
+# example the reference's data/ directory); without it the test is skipped.
+MTX_DIR = os.environ.get("BAAS_MTX_DIR", "")
+
+
+@pytest.mark.parametrize("name", ["bcsstk18", "bcsstk38"])
+def test_reference_fixtures_on_gpu(name):
+    import torch
+
+    from baas_b200 import BaasError
+
+    path = Path(MTX_DIR) / f"{name}.mtx"
+    if not MTX_DIR or not path.exists():
+        pytest.skip("BAAS_MTX_DIR does not hold the reference's SuiteSparse fixtures")
+    A = gen.read_mtx(path)
+    dA = DeviceCSR.from_host(A)
+    want, bad = Port.ic0(A)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    lu = dA.values.clone()
+    if bad:
+        # non-positive pivots stay unchanged, as in the reference (merge/IC.cpp:371-378)
+        with pytest.raises(BaasError) as e:
+            s.ic0(dA, lu)
+        assert e.value.status == 4
+    else:
+        s.ic0(dA, lu)
+    assert np.array_equal(lu.cpu().numpy(), want)
+
+    Lo = gen.CSR(A.n, A.rowptr, A.colidx, want).lower()
+    Up = Lo.transpose()
+    b = gen.uniform_rhs(A.n, 1)
+    y = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    z = torch.zeros_like(y)
+    s.forward(DeviceCSR.from_host(Lo), torch.from_numpy(b).cuda(), y)
+    s.backward(DeviceCSR.from_host(Up), y, z)
+    yw = Port.lower_solve(Lo, b)
+    assert np.array_equal(y.cpu().numpy(), yw)
+    assert np.array_equal(z.cpu().numpy(), Port.upper_solve(Up, yw, descending=True))
+
+    x = torch.zeros_like(y)
+    it, rel = s.iccg(dA, torch.from_numpy(b).cuda(), x, tol=1e-10, maxiter=20000, raise_on_zero_pivot=False)
+    xo, ito, relo = Port.pcg(A, b, tol=1e-10, maxiter=20000)
+    xg = x.cpu().numpy()
+    err = float(np.linalg.norm(xg - xo) / np.linalg.norm(xo))
+    res = float(np.linalg.norm(b - A.to_scipy() @ xg) / np.linalg.norm(b))
+    print(f"{name}: n={A.n} nnz={A.nnz} zero pivots {bad}; iterations {it} (oracle {ito}), relres {rel:.3e}, "
+          f"x rel err vs oracle {err:.3e}, true residual {res:.3e}")
+    assert rel < 1e-10 and relo < 1e-10
+    # Ill-conditioned stiffness matrices (zero pivots skipped, thousands of iterations): the dot
+    # products' summation order moves the iteration count by a few percent (measured on a B200:
+    # 959 vs 992 on bcsstk18, 8,533 vs 9,145 on bcsstk38), while the solutions agree to 5e-15 and
+    # 7.5e-13 relative.
+    assert it <= ito + max(2, ito // 10)
+    assert err <= 1e-10

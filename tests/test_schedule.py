@@ -134,3 +134,24 @@ def test_schedule_invariants():
     for t in range(int(a["ntasks"][0])):
         for q in ts[tp[t]:tp[t + 1]]:
             assert owner[q] != owner[t]
+
+
+# The schedules the benchmark runs, at full size: configuration 2 (64^3, natural and permuted,
+# and the k-NN stiffness matrix at n = 12,000) and configuration 3 (96^3 ILU0).
+FULL = [
+    ("c2_natural", KERNEL_ICCG, lambda: gen.c2_system(False), (8, 16)),
+    ("c2_permuted", KERNEL_ICCG, lambda: gen.c2_system(True), (8,)),
+    ("c2_knn_12000", KERNEL_ICCG, lambda: gen.knn_stiffness(nodes=4000), (8,)),
+    ("c3_ilu0_96", KERNEL_ILU0, lambda: gen.convdiff3d(96), (8,)),
+]
+
+
+@pytest.mark.parametrize("case", [c[0] for c in FULL])
+def test_full_size_schedules_match_live_reference(case, ref_lib):
+    _, kind, mk, threads = next(c for c in FULL if c[0] == case)
+    A = mk()
+    for nt in threads:
+        ours = Schedule(A, kind=kind, nthread=nt).arrays()
+        ref = ref_lib.Schedule(kind, A, nt).arrays()
+        for f in FIELDS:
+            assert np.array_equal(ours[f], ref[f]), f"{case} nthread={nt} field {f}"
