@@ -20,14 +20,15 @@ import numpy as np
 from . import _native
 from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, MAPPING_COST_SPLIT,
                       MAPPING_AFFINITY, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_FOUR_RULE, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
-                      PARTITION_RANGES,
+                      PARTITION_RANGES, PARTITION_BLOCKS, PARTITION_AUTO, WALK_AUTO, WALK_CHUNKED, WALK_FETCH,
                       PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
 
 __all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV",
            "KERNEL_ICCG", "KERNEL_IC0", "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "PARTITION_RANGES",
            "PARTITION_BAAS_THREADS", "PARTITION_CUSTOM", "MAPPING_FOUR_RULE", "MAPPING_COST_SPLIT",
-           "MAPPING_COST_SPLIT_BARRIER", "MAPPING_FINISH_TIME", "MAPPING_AFFINITY", "version"]
+           "MAPPING_COST_SPLIT_BARRIER", "MAPPING_FINISH_TIME", "MAPPING_AFFINITY", "WALK_AUTO", "WALK_CHUNKED",
+           "WALK_FETCH", "PARTITION_BLOCKS", "PARTITION_AUTO", "version"]
 
 
 def version() -> str:
@@ -80,7 +81,8 @@ class Schedule:
     """
 
     def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
-                 parts: int = 0, partition: int = 0, smem_budget: int = 0, mapping: int = 0):
+                 parts: int = 0, partition: int = PARTITION_AUTO, smem_budget: int = 0, mapping: int = 0,
+                 walk: int = 0):
         L = _native.lib()
         self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
         self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
@@ -93,6 +95,7 @@ class Schedule:
         opt.partition = partition
         opt.smem_budget = smem_budget
         opt.mapping = mapping
+        opt.walk = walk
         h = C.c_void_p()
         _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
         self._h = h
@@ -125,11 +128,26 @@ class Schedule:
     def arrays(self) -> dict:
         return {k: self.export(k) for k in _native.FIELDS}
 
+    def plan_parts(self):
+        """(CTAs of the current device plan, grid box shape, boxes per axis); shapes are None
+        unless the plan uses grid boxes, and the count is 0 before a plan exists."""
+        box = np.zeros(6, dtype=np.int32)
+        P = int(_native.lib().baas_plan_parts(self._h, box.ctypes.data))
+        if box[0] == 0:
+            return P, None, None
+        return P, tuple(int(v) for v in box[:3]), tuple(int(v) for v in box[3:])
+
+    @property
+    def last_walk(self) -> int:
+        """WALK_CHUNKED or WALK_FETCH: the sweep kernel of the last sweep / ICCG call (0 before)."""
+        return int(_native.lib().baas_schedule_last_walk(self._h))
+
     def inject_unsatisfiable_wait(self, row: int) -> None:
         """Test hook: the next forward sweep waits on a value nothing writes (BAAS_ERR_TIMEOUT)."""
         _native.check(_native.lib().baas_test_inject_unsatisfiable_wait(self._h, row), "inject")
 
-    def replan(self, parts: int = 0, smem_budget: int = 0, partition: int = 0, spin_limit: int = 0) -> None:
+    def replan(self, parts: int = 0, smem_budget: int = 0, partition: int = PARTITION_AUTO, spin_limit: int = 0,
+               walk: int = 0) -> None:
         """Rebuild the device plan with other execution options (baas_replan), keeping the analysis."""
         opt = _native.BaasOptions()
         _native.lib().baas_options_default(C.byref(opt))
@@ -139,6 +157,7 @@ class Schedule:
         opt.smem_budget = smem_budget
         opt.partition = partition
         opt.spin_limit = spin_limit
+        opt.walk = walk
         _native.check(_native.lib().baas_replan(self._h, C.byref(opt)), "baas_replan")
 
     def replan_custom(self, row_part, parts: int | None = None, smem_budget: int = 0) -> None:
@@ -160,6 +179,15 @@ class Schedule:
         x = np.zeros(self.n)
         _native.check(_native.lib().baas_test_emulate_sweep(self._h, parts, smem_budget, int(upper), _ptr(tv),
                                                              _ptr(bb), _ptr(x)), "emulate_sweep")
+        return x
+
+    def emulate_fetch(self, T: CSR, b: np.ndarray, upper: bool = False, parts: int = 0) -> np.ndarray:
+        """Test hook: run the fetch-walk plan on the host (no GPU) and return x."""
+        tv = np.ascontiguousarray(T.values, dtype=np.float64)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        _native.check(_native.lib().baas_test_emulate_fetch(self._h, parts, int(upper), _ptr(tv), _ptr(bb), _ptr(x)),
+                      "emulate_fetch")
         return x
 
     @property

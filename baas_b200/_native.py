@@ -25,7 +25,8 @@ STATUS_NAMES = {
 
 KERNEL_SPTRSV, KERNEL_ICCG, KERNEL_IC0, KERNEL_ILU0 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32_FACTORS = 0, 1
-PARTITION_RANGES, PARTITION_BAAS_THREADS, PARTITION_CUSTOM = 0, 1, 2
+PARTITION_RANGES, PARTITION_BAAS_THREADS, PARTITION_CUSTOM, PARTITION_BLOCKS, PARTITION_AUTO = 0, 1, 2, 3, 4
+WALK_AUTO, WALK_CHUNKED, WALK_FETCH = 0, 1, 2
 MAPPING_FOUR_RULE, MAPPING_COST_SPLIT, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_AFFINITY = 0, 1, 2, 3, 4
 
 FIELDS = {
@@ -40,6 +41,7 @@ EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
     "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan", "baas_test_divide", "baas_replan_custom", "baas_csr_read_mtx", "baas_csr_free",
+    "baas_schedule_last_walk", "baas_test_emulate_fetch", "baas_plan_parts",
 ]
 
 
@@ -50,7 +52,7 @@ class BaasCsr(C.Structure):
 
 class BaasOptions(C.Structure):
     _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("parts", C.c_int),
-                ("partition", C.c_int), ("smem_budget", C.c_int), ("mapping", C.c_int)]
+                ("partition", C.c_int), ("smem_budget", C.c_int), ("mapping", C.c_int), ("walk", C.c_int)]
 
 
 class BaasError(RuntimeError):
@@ -81,6 +83,10 @@ def lib():
     L.baas_schedule_export.restype = i
     L.baas_schedule_analysis_ms.argtypes = [vp]
     L.baas_schedule_analysis_ms.restype = d
+    L.baas_schedule_last_walk.argtypes = [vp]
+    L.baas_schedule_last_walk.restype = i
+    L.baas_plan_parts.argtypes = [vp, vp]
+    L.baas_plan_parts.restype = i
     L.baas_destroy.argtypes = [vp]
     L.baas_destroy.restype = None
     L.baas_sptrsv.argtypes = [vp, C.POINTER(BaasCsr), i, vp, vp, i, i, vp]
@@ -112,6 +118,8 @@ def lib():
     L.baas_iccg_batched.restype = i
     L.baas_test_emulate_sweep.argtypes = [vp, i, i, i, vp, vp, vp]
     L.baas_test_emulate_sweep.restype = i
+    L.baas_test_emulate_fetch.argtypes = [vp, i, i, vp, vp, vp]
+    L.baas_test_emulate_fetch.restype = i
     L.baas_test_divide.argtypes = [vp, vp, vp, C.c_longlong, i, vp]
     L.baas_test_divide.restype = i
     L.baas_replan_custom.argtypes = [vp, vp, i, i]

@@ -170,6 +170,52 @@ struct WinCfg {
     }
 };
 
+// Fetch-walk plan (fetch.cuh): per direction and CTA an int block [step table | records], the
+// value-source codes of its records and the CTA's fetch list.
+struct FetchHostDir {
+    std::vector<int4> ints;        // int blocks, CTA by CTA
+    std::vector<int4> cblk;        // P + 1: {first int4, int4 count, steps, first record}
+    std::vector<int> code, codeT;  // 4 per record: {diag, a0, a1, a2} positions in A / in the caller's T
+    std::vector<int> cfetch, frow; // P + 1 and the fetch lists
+    int ints_max = 0;              // most int4 of one CTA's block
+};
+struct FetchHost {
+    bool ok = false;  // every row has at most 3 off-diagonal entries and every step fits the compute warps
+    FetchHostDir dir[2];
+    int ncomp = 32;     // compute threads: the widest step, rounded up to a warp
+    int rows_max = 0;   // most rows of one CTA
+    int nslot_max = 0;  // most slots of one CTA: rows + 1 + staging of both directions
+};
+struct FetchDevDir {
+    int4 *ints = nullptr, *cblk = nullptr;
+    int *code = nullptr, *codeT = nullptr, *cfetch = nullptr, *frow = nullptr;
+};
+struct FetchDev {
+    FetchDevDir dir[2];
+    void release() {
+        for (auto &D : dir) {
+            void *ptrs[] = {D.ints, D.cblk, D.code, D.codeT, D.cfetch, D.frow};
+            for (void *p : ptrs)
+                if (p) cudaFree(p);
+        }
+        *this = FetchDev();
+    }
+};
+
+baas_status upload_fetch(FetchDev &d, const FetchHost &h) {
+    for (int k = 0; k < 2; k++) {
+        const FetchHostDir &H = h.dir[k];
+        FetchDevDir &D = d.dir[k];
+        BAAS_TRY(upload(D.ints, H.ints));
+        BAAS_TRY(upload(D.cblk, H.cblk));
+        BAAS_TRY(upload(D.code, H.code));
+        BAAS_TRY(upload(D.codeT, H.codeT));
+        BAAS_TRY(upload(D.cfetch, H.cfetch));
+        BAAS_TRY(upload(D.frow, H.frow));
+    }
+    return BAAS_OK;
+}
+
 baas_status upload_chunks(ChunkDev &d, const ChunkHost &h) {
     for (int k = 0; k < 2; k++) {
         const ChunkHostDir &H = h.dir[k];
@@ -199,8 +245,11 @@ struct baas_schedule {
     int P = 0;
     std::vector<int> group_cta, row_cta;
     std::vector<int> custom_part;  // BAAS_PARTITION_CUSTOM: the caller's row -> CTA map
+    bool use_boxes = false;        // grid-box partition (choose_partition)
+    int grid[3] = {1, 1, 1}, box[3] = {1, 1, 1}, nbox[3] = {1, 1, 1};
     PartHost fwd, bwd;
     ChunkHost chk;
+    FetchHost fch;
     int fault_row = -1;  // test hook: forward row made to wait on its own output
 
     // device
@@ -209,6 +258,11 @@ struct baas_schedule {
     int num_sms = 0;
     PartDev d_fwd, d_bwd;
     ChunkDev d_chk;
+    FetchDev d_fch;
+    double *d_gf64[2] = {nullptr, nullptr};  // fetch-walk record values: ICCG factors, FP64
+    float *d_gf32[2] = {nullptr, nullptr};   // the same, FP32
+    double *d_gfT[2] = {nullptr, nullptr};   // record values of the caller's factor (sweeps)
+    int last_walk = 0;                       // walk of the last sweep / ICCG launch (BAAS_WALK_*)
     std::map<int, WinCfg> wins;  // key: value bytes * 16 + right-hand sides
     int smem_budget = 0;
     int rmax64 = 1;  // most FP64 right-hand sides one sweep walks together
@@ -280,8 +334,108 @@ void build_order(baas_schedule *s) {
         }
 }
 
+// Structured-grid detection: the off-diagonal offsets r - c of L's rows are {1}, {1, n1} or
+// {1, n1, n1 n2} (a 1-, 2- or 3-D stencil in natural ordering, x fastest), with n a multiple of
+// the grid's plane size. Only a hint for the partition: any partition gives the same results.
+bool detect_grid(const baas::HostSchedule &h, int dims[3]) {
+    const int n = h.n;
+    int off[4], no = 0;
+    for (int r = 0; r < n; r++)
+        for (int e = h.l_rowptr[r]; e < h.l_rowptr[r + 1] - 1; e++) {
+            const int o = r - h.l_colidx[e];
+            int t = 0;
+            while (t < no && off[t] != o) t++;
+            if (t == no) {
+                if (no == 3) return false;
+                off[no++] = o;
+            }
+        }
+    std::sort(off, off + no);
+    if (no == 0 || off[0] != 1) return false;
+    dims[0] = n, dims[1] = 1, dims[2] = 1;
+    if (no >= 2) {
+        if (n % off[1]) return false;
+        dims[0] = off[1];
+        dims[1] = n / off[1];
+    }
+    if (no == 3) {
+        if (off[2] % off[1] || n % off[2]) return false;
+        dims[1] = off[2] / off[1];
+        dims[2] = n / off[2];
+    }
+    return dims[0] >= 2 || n == 1;
+}
+
+// Box shape for the BLOCKS partition of an n1 x n2 x n3 grid: boxes of at most vmax rows, at
+// most max_boxes of them, whose widest level (anti-diagonal) fits the fetch walk's compute warps.
+// The shape minimises a model of the fetch walk's sweep time: one step per level of the grid
+// (~0.15 us, 10% more per extra compute warp) plus ~1.8 us for every box boundary the
+// critical path crosses -- the constants measured on B200 for 64^3 with 2,048-row boxes.
+bool choose_boxes(const int dims[3], int max_boxes, int vmax, int box[3], int nbox[3]) {
+    auto cand = [](int m) {
+        std::vector<int> v;
+        for (int b = 1; b < m; b *= 2) v.push_back(b);
+        v.push_back(m);
+        return v;
+    };
+    double best = 1e30;
+    bool found = false;
+    for (int b1 : cand(dims[0]))
+        for (int b2 : cand(dims[1]))
+            for (int b3 : cand(dims[2])) {
+                if ((long long)b1 * b2 * b3 > vmax) continue;
+                const int c1 = (dims[0] + b1 - 1) / b1, c2 = (dims[1] + b2 - 1) / b2, c3 = (dims[2] + b3 - 1) / b3;
+                if ((long long)c1 * c2 * c3 > max_boxes) continue;
+                std::vector<int> lev(b1 + b2 + b3, 0);
+                for (int i = 0; i < b1; i++)
+                    for (int j = 0; j < b2; j++)
+                        for (int k = 0; k < b3; k++) lev[i + j + k]++;
+                const int width = *std::max_element(lev.begin(), lev.end());
+                if (width > baas::kFetchMaxRows) continue;
+                const int warps = (width + 31) / 32;
+                const double est = (dims[0] + dims[1] + dims[2] - 2) * 0.15 * (1.0 + 0.1 * (warps - 1)) +
+                                   1.8 * (c1 - 1 + c2 - 1 + c3 - 1);
+                if (est < best - 1e-9 || (est < best + 1e-9 && found && b1 > box[0])) {
+                    best = est;
+                    box[0] = b1, box[1] = b2, box[2] = b3;
+                    nbox[0] = c1, nbox[1] = c2, nbox[2] = c3;
+                    found = true;
+                }
+            }
+    return found;
+}
+
+// The partition a plan uses and its CTA count. AUTO: grid boxes when the pattern is a
+// natural-order stencil whose rows (of L and of U = L^T) hold at most 3 off-diagonal entries and
+// the fetch walk is allowed (those are the plans the fetch walk runs fastest on), else RANGES.
+// BLOCKS: grid boxes whenever the pattern is a grid, else RANGES. RANGES: `parts`, or about one
+// CTA per 2,048 rows (at most 128, at most one per SM).
+int choose_partition(baas_schedule *s, int num_sms) {
+    const baas::HostSchedule &h = s->hs;
+    const int n = h.n;
+    s->use_boxes = false;
+    if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) return h.nthread;
+    if (s->opt.partition == BAAS_PARTITION_CUSTOM) return s->opt.parts;
+    const bool may_box = s->opt.parts == 0 && (s->opt.partition == BAAS_PARTITION_BLOCKS ||
+                                               (s->opt.partition == BAAS_PARTITION_AUTO && s->opt.walk != BAAS_WALK_CHUNKED));
+    if (may_box) {
+        bool narrow = true;
+        for (int r = 0; r < n && narrow; r++) narrow = h.l_rowptr[r + 1] - h.l_rowptr[r] - 1 <= 3 && s->cptr[r + 1] - s->cptr[r] - 1 <= 3;
+        int dims[3];
+        if ((narrow || s->opt.partition == BAAS_PARTITION_BLOCKS) && detect_grid(h, dims) &&
+            choose_boxes(dims, num_sms, 2048, s->box, s->nbox)) {
+            s->use_boxes = true;
+            s->grid[0] = dims[0], s->grid[1] = dims[1], s->grid[2] = dims[2];
+            return s->nbox[0] * s->nbox[1] * s->nbox[2];
+        }
+    }
+    if (s->opt.parts > 0) return std::min(s->opt.parts, n);
+    return std::max(1, std::min({(n + 2047) / 2048, 128, num_sms}));
+}
+
 // Groups -> CTAs. RANGES: the CTA whose row range holds the group's first row (P contiguous,
-// row-balanced ranges). BAAS_THREADS: the four-rule mapping's thread of the group.
+// row-balanced ranges). BAAS_THREADS: the four-rule mapping's thread of the group. Boxes
+// (use_boxes): the grid box that holds the group's first row.
 void build_partition(baas_schedule *s, int P) {
     const baas::HostSchedule &h = s->hs;
     const int n = h.n;
@@ -293,6 +447,12 @@ void build_partition(baas_schedule *s, int P) {
         for (int t = 0; t < h.nthread; t++)
             for (int task = h.thread_boundaries[t]; task < h.thread_boundaries[t + 1]; task++)
                 for (int q = h.task_boundaries[task]; q < h.task_boundaries[task + 1]; q++) s->group_cta[h.thread_cont_to_orig[q]] = t;
+    } else if (s->use_boxes) {
+        for (int g = 0; g < h.ngroups; g++) {
+            const int r0 = h.group_set[h.group_ptr[g]];
+            const int i = r0 % s->grid[0], j = (r0 / s->grid[0]) % s->grid[1], k = r0 / (s->grid[0] * s->grid[1]);
+            s->group_cta[g] = i / s->box[0] + s->nbox[0] * (j / s->box[1] + s->nbox[1] * (k / s->box[2]));
+        }
     } else {
         for (int g = 0; g < h.ngroups; g++) {
             const int r0 = h.group_set[h.group_ptr[g]];
@@ -548,6 +708,117 @@ void build_chunks(baas_schedule *s) {
     }
 }
 
+// Fetch-walk plan (fetch.cuh) from the same per-CTA steps as the chunk plan: a level segment
+// whose groups hold up to m rows is m steps, step j holding the j-th row of every group.
+// Records carry the row's own slot (its position in the CTA's row list, C.srow) and one slot
+// per off-diagonal entry, in the entry order of the position plan (ascending columns for L,
+// descending for U): the producer's own slot when it belongs to this CTA, the zero slot (rows)
+// for an absent entry, or the staging slot of the producer's fetch-list entry (rows + 1 + f in
+// the lower direction, rows + 1 + nf_lower + f in the upper). The plan is marked unusable (and
+// the chunked walk runs) when a row has more than 3 off-diagonal entries or a step more rows
+// than the compute warps hold.
+void build_fetch(baas_schedule *s) {
+    const int n = s->hs.n, P = s->P;
+    const ChunkHost &C = s->chk;
+    FetchHost &F = s->fch;
+    F = FetchHost();
+    std::vector<int> kpos_of(n, 0);
+    for (int c = 0; c < P; c++) {
+        for (int k = C.soff[c]; k < C.soff[c + 1]; k++) kpos_of[C.srow[k]] = k - C.soff[c];
+        F.rows_max = std::max(F.rows_max, C.soff[c + 1] - C.soff[c]);
+    }
+    std::vector<int> fidx(n, -1), nf0(P, 0), nslot(P, 0);
+    bool ok = true;
+    int widest = 1;
+    for (int d = 0; d < 2 && ok; d++) {
+        const PartHost &H = d == 0 ? s->fwd : s->bwd;
+        FetchHostDir &D = F.dir[d];
+        D.cfetch.assign(1, 0);
+        D.code.reserve(4 * (size_t)n);
+        D.codeT.reserve(4 * (size_t)n);
+        for (int c = 0; c < P && ok; c++) {
+            const int nrows = C.soff[c + 1] - C.soff[c];
+            const int sbase = nrows + 1 + (d ? nf0[c] : 0);
+            std::vector<int> order, step_end;
+            for (int sg = H.cta_seg[c]; sg < H.cta_seg[c + 1]; sg++) {
+                int m = 0;
+                for (int it = H.seg_item[sg]; it < H.seg_item[sg + 1]; it++) m = std::max(m, H.item_pos[it + 1] - H.item_pos[it]);
+                for (int j = 0; j < m; j++) {
+                    for (int it = H.seg_item[sg]; it < H.seg_item[sg + 1]; it++)
+                        if (H.item_pos[it] + j < H.item_pos[it + 1]) order.push_back(H.item_pos[it] + j);
+                    step_end.push_back((int)order.size());
+                }
+            }
+            const int ns = (int)step_end.size();
+            const int i0 = (int)D.ints.size();
+            // step table: {first record, rows, 0, 0}, then two copies of the last step
+            int kb = 0;
+            for (int t = 0; t < ns; t++) {
+                const int nl = step_end[t] - kb;
+                if (nl > baas::kFetchMaxRows) ok = false;
+                widest = std::max(widest, nl);
+                D.ints.push_back(make_int4(kb, nl, 0, 0));
+                kb = step_end[t];
+            }
+            const int4 last = ns > 0 ? D.ints.back() : make_int4(0, 1, 0, 0);
+            D.ints.push_back(last);
+            D.ints.push_back(last);
+            const int fb = (int)D.frow.size();
+            for (int pos : order) {
+                const int row = H.row[pos], ne = H.eptr[pos + 1] - H.eptr[pos];
+                if (ne > 3) {
+                    ok = false;
+                    break;
+                }
+                int sl[3] = {nrows, nrows, nrows}, ca[4] = {H.dsrcA[pos], -1, -1, -1}, ct[4] = {H.dsrcT[pos], -1, -1, -1};
+                for (int j = 0; j < ne; j++) {
+                    const int e = H.eptr[pos] + j, dd = H.dep[e];
+                    if (dd < 0) {
+                        sl[j] = kpos_of[H.row[H.cta_pos[c] + (-dd - 1)]];
+                    } else {
+                        if (fidx[dd] < 0) {
+                            fidx[dd] = (int)D.frow.size() - fb;
+                            D.frow.push_back(dd);
+                        }
+                        sl[j] = sbase + fidx[dd];
+                    }
+                    ca[j + 1] = H.srcA[e];
+                    ct[j + 1] = H.srcT[e];
+                }
+                D.ints.push_back(make_int4(kpos_of[row], sl[0], sl[1], sl[2]));
+                for (int j = 0; j < 4; j++) {
+                    D.code.push_back(ca[j]);
+                    D.codeT.push_back(ct[j]);
+                }
+            }
+            for (size_t f = fb; f < D.frow.size(); f++) fidx[D.frow[f]] = -1;
+            const int nf = (int)D.frow.size() - fb;
+            if (d == 0) nf0[c] = nf;
+            nslot[c] = std::max(nslot[c], nrows + 1 + nf0[c] + (d ? nf : 0));
+            D.cblk.push_back(make_int4(i0, (int)D.ints.size() - i0, ns, C.soff[c]));
+            D.cfetch.push_back((int)D.frow.size());
+            D.ints_max = std::max(D.ints_max, (int)D.ints.size() - i0);
+        }
+        D.cblk.push_back(make_int4((int)D.ints.size(), 0, 0, n));
+    }
+    for (int c = 0; c < P; c++) F.nslot_max = std::max(F.nslot_max, nslot[c]);
+    F.ncomp = (widest + 31) / 32 * 32;
+    F.ok = ok && F.ncomp <= baas::kFetchMaxRows;
+    if (!F.ok) F = FetchHost();
+}
+
+// Shared bytes of a fetch-walk launch: ICCG (both directions' int blocks resident; values: FP64
+// one direction at a time, FP32 both) or a standalone sweep (one direction).
+size_t fetch_smem(const FetchHost &F, int vbytes, bool iccg) {
+    const int slot_bytes = (F.nslot_max * vbytes + 15) / 16 * 16;
+    const int srow_bytes = (F.rows_max * 4 + 15) / 16 * 16;
+    const int ib0 = 16 * (iccg ? F.dir[0].ints_max : std::max(F.dir[0].ints_max, F.dir[1].ints_max));
+    const int ib1 = iccg ? 16 * F.dir[1].ints_max : 0;
+    const int rb = vbytes == 8 ? 8 * baas::kFetchVal64 : 4 * baas::kFetchVal32;
+    const int vb = rb * F.rows_max * (iccg && vbytes == 4 ? 2 : 1);
+    return (size_t)baas::fetch_smem_bytes(slot_bytes, srow_bytes, ib0, ib1, vb);
+}
+
 // Windows for values of `vbytes` bytes and R right-hand sides: each CTA's chunks grouped
 // greedily into blocks that fit one of the two buffers. False if a chunk does not fit.
 // Window buffers: at most kWindowTarget bytes each unless the budget was set explicitly (then
@@ -663,10 +934,60 @@ baas::ChunkPlan chunk_plan(const baas_schedule *s, const WinCfg &w) {
     return p;
 }
 
+// Device view of the fetch-walk plan for values of `vbytes` bytes, for an ICCG launch (both
+// directions resident) or a standalone sweep.
+baas::FetchPlan fetch_plan(const baas_schedule *s, int vbytes, bool iccg) {
+    const FetchHost &F = s->fch;
+    baas::FetchPlan p{};
+    p.P = s->P;
+    for (int d = 0; d < 2; d++) {
+        const FetchDevDir &D = s->d_fch.dir[d];
+        p.dir[d] = baas::FetchDir{D.ints, D.cblk, D.code, D.codeT, D.cfetch, D.frow};
+    }
+    p.soff = s->d_chk.soff;
+    p.srow = s->d_chk.srow;
+    p.nslot = F.nslot_max;
+    p.srow_bytes = (F.rows_max * 4 + 15) / 16 * 16;
+    p.ints_bytes[0] = 16 * (iccg ? F.dir[0].ints_max : std::max(F.dir[0].ints_max, F.dir[1].ints_max));
+    p.ints_bytes[1] = iccg ? 16 * F.dir[1].ints_max : 0;
+    const int rb = vbytes == 8 ? 8 * baas::kFetchVal64 : 4 * baas::kFetchVal32;
+    p.vals_bytes = rb * F.rows_max * (iccg && vbytes == 4 ? 2 : 1);
+    p.ncomp = F.ncomp;
+    return p;
+}
+
 constexpr int kMaxSmemBudget = 224 * 1024;
 // dynamic shared memory a kernel may request: B200's 227 KB per block less room for the
 // kernels' static shared memory
 constexpr int kMaxDynSmem = 227 * 1024 - 2048;
+
+// Builds every plan of the partition choose_partition picked. When AUTO picked grid boxes but
+// the fetch walk cannot run them (a step too wide, or the ICCG plan too large for shared memory),
+// the plans are rebuilt on RANGES, where the chunked walk is faster than on boxes.
+void build_plans(baas_schedule *s, int P, int num_sms) {
+    for (int pass = 0; pass < 2; pass++) {
+        build_partition(s, P);
+        build_dir(s, false, s->fwd);
+        build_dir(s, true, s->bwd);
+        build_chunks(s);
+        build_fetch(s);
+        const bool fits = s->fch.ok && fetch_smem(s->fch, 8, s->hs.kind != baas::SchedKind::SpTRSV) <= (size_t)kMaxDynSmem;
+        if (!s->use_boxes || s->opt.partition != BAAS_PARTITION_AUTO || fits) return;
+        s->use_boxes = false;
+        P = s->opt.parts > 0 ? std::min(s->opt.parts, s->hs.n) : std::max(1, std::min({(s->hs.n + 2047) / 2048, 128, num_sms}));
+    }
+}
+
+// Whether a launch takes the fetch walk (values of vbytes bytes; ICCG or a standalone sweep of
+// one right-hand side). BAAS_WALK_FETCH turns a plan that does not qualify into an error.
+baas_status pick_walk(const baas_schedule *s, int vbytes, bool iccg, bool &fw) {
+    const bool fits = s->fch.ok && fetch_smem(s->fch, vbytes, iccg) <= (size_t)kMaxDynSmem;
+    if (s->opt.walk == BAAS_WALK_FETCH && !fits)
+        return fail(BAAS_ERR_BAD_ARG, "the fetch walk needs rows of at most 3 off-diagonal entries, steps of at most " +
+                                          std::to_string(baas::kFetchMaxRows) + " rows and a plan that fits shared memory");
+    fw = fits && s->opt.walk != BAAS_WALK_CHUNKED;
+    return BAAS_OK;
+}
 
 // The launched variants. ieee: sweep divisions by __ddiv_rn, for the repeat of a launch whose
 // div_fast divisions left their range (DevStatus::slow_div); FP32 factors never divide.
@@ -677,10 +998,19 @@ void *sweep_kernel(bool mr, bool stg, bool ieee) {
     return mr ? (stg ? (void *)baas::k_sweep_chunked<true, true, false> : (void *)baas::k_sweep_chunked<true, false, false>)
               : (stg ? (void *)baas::k_sweep_chunked<false, true, false> : (void *)baas::k_sweep_chunked<false, false, false>);
 }
-void *iccg_kernel(bool mixed, bool stg, bool ieee) {
-    if (mixed) return stg ? (void *)baas::k_iccg_chunked<float, true, false> : (void *)baas::k_iccg_chunked<float, false, false>;
-    if (ieee) return stg ? (void *)baas::k_iccg_chunked<double, true, true> : (void *)baas::k_iccg_chunked<double, false, true>;
-    return stg ? (void *)baas::k_iccg_chunked<double, true, false> : (void *)baas::k_iccg_chunked<double, false, false>;
+void *iccg_kernel(bool mixed, bool stg, bool ieee, bool fw = false) {
+    if (fw) {
+        if (mixed) return (void *)baas::k_iccg_chunked<float, false, false, true>;
+        return ieee ? (void *)baas::k_iccg_chunked<double, false, true, true> : (void *)baas::k_iccg_chunked<double, false, false, true>;
+    }
+    if (mixed)
+        return stg ? (void *)baas::k_iccg_chunked<float, true, false, false> : (void *)baas::k_iccg_chunked<float, false, false, false>;
+    if (ieee)
+        return stg ? (void *)baas::k_iccg_chunked<double, true, true, false> : (void *)baas::k_iccg_chunked<double, false, true, false>;
+    return stg ? (void *)baas::k_iccg_chunked<double, true, false, false> : (void *)baas::k_iccg_chunked<double, false, false, false>;
+}
+void *sweep_fetch_kernel(bool ieee) {
+    return ieee ? (void *)baas::k_sweep_fetch<true> : (void *)baas::k_sweep_fetch<false>;
 }
 // rw: FP32 factors with exactly 2 or 4 right-hand sides take the row-wide sweeps (one thread per
 // row for all of them; rw = that count, else 1); BAAS_BATCH_PAIRS=1 keeps the
@@ -728,26 +1058,16 @@ baas_status ensure_device(baas_schedule *s) {
     // partition size: BAAS_THREADS: the schedule's threads; else `parts`, or about one CTA per
     // 2,048 rows (at most 128, at most one per SM)
     const int n = s->hs.n;
-    int P;
-    if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) {
-        P = s->hs.nthread;
-        if (s->opt.parts > 0 && s->opt.parts != P) return fail(BAAS_ERR_BAD_ARG, "BAAS_THREADS partition needs parts == nthread");
-    } else if (s->opt.partition == BAAS_PARTITION_CUSTOM) {
-        P = s->opt.parts;
-    } else if (s->opt.parts > 0) {
-        P = std::min(s->opt.parts, n);
-    } else {
-        P = std::max(1, std::min({(n + 2047) / 2048, 128, s->num_sms}));
-    }
+    if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS && s->opt.parts > 0 && s->opt.parts != s->hs.nthread)
+        return fail(BAAS_ERR_BAD_ARG, "BAAS_THREADS partition needs parts == nthread");
+    const int P = choose_partition(s, s->num_sms);
     if (P > s->num_sms) return fail(BAAS_ERR_BAD_ARG, "the partition needs more CTAs than the device has SMs");
-    build_partition(s, P);
-    build_dir(s, false, s->fwd);
-    build_dir(s, true, s->bwd);
-    build_chunks(s);
+    build_plans(s, P, s->num_sms);
 
     BAAS_TRY(upload_part(s->d_fwd, s->fwd));
     BAAS_TRY(upload_part(s->d_bwd, s->bwd));
     BAAS_TRY(upload_chunks(s->d_chk, s->chk));
+    if (s->fch.ok) BAAS_TRY(upload_fetch(s->d_fch, s->fch));
     BAAS_TRY(upload(s->d_a_diag, s->hs.a_diagptr));
     BAAS_TRY(dalloc(s->d_status, 1));
     BAAS_TRY(dalloc(s->d_flags, (size_t)n));
@@ -760,6 +1080,9 @@ baas_status ensure_device(baas_schedule *s) {
             const void *kerns[] = {sweep_kernel(a, b, c), iccg_kernel(a, b, c), batched_kernel(a, b, c),
                                    batched_kernel(true, true, false, 4), batched_kernel(true, true, false, 2)};
             for (const void *k : kerns)
+                BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+            const void *fk[] = {iccg_kernel(a, false, b, true), sweep_fetch_kernel(a)};
+            for (const void *k : fk)
                 BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
         }
     }
@@ -862,9 +1185,10 @@ void baas_options_default(baas_options *opt) {
     opt->nthread = 8;
     opt->spin_limit = 0;
     opt->parts = 0;
-    opt->partition = BAAS_PARTITION_RANGES;
+    opt->partition = BAAS_PARTITION_AUTO;
     opt->smem_budget = 0;
     opt->mapping = BAAS_MAPPING_FOUR_RULE;
+    opt->walk = BAAS_WALK_AUTO;
 }
 
 const char *baas_last_error_string(void) { return g_err.c_str(); }
@@ -886,10 +1210,12 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     baas_options_default(&o);
     if (opt) o = *opt;
     if (o.nthread < 1) return fail(BAAS_ERR_BAD_ARG, "nthread must be >= 1");
-    if (o.partition != BAAS_PARTITION_RANGES && o.partition != BAAS_PARTITION_BAAS_THREADS)
+    if (o.partition != BAAS_PARTITION_RANGES && o.partition != BAAS_PARTITION_BAAS_THREADS &&
+        o.partition != BAAS_PARTITION_BLOCKS && o.partition != BAAS_PARTITION_AUTO)
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     if (o.parts < 0) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 0");
     if (o.smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
+    if (o.walk < BAAS_WALK_AUTO || o.walk > BAAS_WALK_FETCH) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
     if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_AFFINITY)
         return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
     if (o.mapping != BAAS_MAPPING_FOUR_RULE && kind != BAAS_KERNEL_ICCG)
@@ -958,6 +1284,18 @@ int baas_schedule_export(const baas_schedule *s, int field, int *out) {
 
 double baas_schedule_analysis_ms(const baas_schedule *s) { return s ? s->hs.analysis_ms : 0.0; }
 
+int baas_schedule_last_walk(const baas_schedule *s) { return s ? s->last_walk : 0; }
+
+int baas_plan_parts(const baas_schedule *s, int *box) {
+    if (!s) return 0;
+    if (box)
+        for (int t = 0; t < 3; t++) {
+            box[t] = s->use_boxes ? s->box[t] : 0;
+            box[3 + t] = s->use_boxes ? s->nbox[t] : 0;
+        }
+    return s->P;
+}
+
 baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row) {
     if (!s || row < 0 || row >= s->hs.n) return fail(BAAS_ERR_BAD_ARG, "bad row");
     const int lb = s->hs.l_rowptr[row], le = s->hs.l_rowptr[row + 1];
@@ -999,13 +1337,12 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
     if (!s || !tval || !b || !x) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     if (s->uploaded) return fail(BAAS_ERR_STATE, "the schedule's plan is resident on a GPU");
     const int n = s->hs.n;
-    int P = parts > 0 ? std::min(parts, n) : std::max(1, std::min({(n + 2047) / 2048, 128, 148}));
-    if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS) P = s->hs.nthread;
-    if (s->opt.partition == BAAS_PARTITION_CUSTOM) P = s->opt.parts;
-    build_partition(s, P);
-    build_dir(s, false, s->fwd);
-    build_dir(s, true, s->bwd);
-    build_chunks(s);
+    const int saved_parts = s->opt.parts;
+    if (parts > 0 && s->opt.partition != BAAS_PARTITION_CUSTOM && s->opt.partition != BAAS_PARTITION_BAAS_THREADS)
+        s->opt.parts = parts;
+    build_plans(s, choose_partition(s, 148), 148);  // plans as for a 148-SM B200
+    s->opt.parts = saved_parts;
+    const int P = s->P;
     const int budget = smem_budget > 0 ? std::min(smem_budget, kMaxSmemBudget) : (int)kSmemBudget;
     std::vector<int4> rec[2];
     std::vector<int> swptr[2];
@@ -1148,6 +1485,138 @@ baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget
     return BAAS_OK;
 }
 
+baas_status baas_test_emulate_fetch(baas_schedule *s, int parts, int upper, const double *tval, const double *b,
+                                    double *x) {
+    if (!s || !tval || !b || !x) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    if (s->uploaded) return fail(BAAS_ERR_STATE, "the schedule's plan is resident on a GPU");
+    if (s->fault_row >= 0) return fail(BAAS_ERR_STATE, "emulate: the schedule carries an injected fault");
+    const int n = s->hs.n;
+    const int saved_parts = s->opt.parts;
+    if (parts > 0 && s->opt.partition != BAAS_PARTITION_CUSTOM && s->opt.partition != BAAS_PARTITION_BAAS_THREADS)
+        s->opt.parts = parts;
+    build_plans(s, choose_partition(s, 148), 148);  // plans as for a 148-SM B200
+    s->opt.parts = saved_parts;
+    const int P = s->P;
+    auto bad = [](const std::string &m) { return fail(BAAS_ERR_BAD_ARG, "emulate fetch: " + m); };
+    const FetchHost &F = s->fch;
+    if (!F.ok) return bad("the plan does not qualify for the fetch walk");
+    if (fetch_smem(F, 8, false) > (size_t)kMaxDynSmem) return bad("the sweep plan does not fit shared memory");
+    const int d = upper ? 1 : 0;
+    const FetchHostDir &D = F.dir[d];
+    const ChunkHost &C = s->chk;
+    const baas::HostSchedule &hs = s->hs;
+    // column of entry j of row r in the reference's order, and the caller's value position
+    auto column = [&](int r, int j) { return upper ? s->crow[s->cptr[r + 1] - 1 - j] : hs.l_colidx[hs.l_rowptr[r] + j]; };
+    // the caller's upper factor is U = L^T in CSR, i.e. L's columns: positions index crow
+    auto tpos = [&](int r, int j) { return upper ? s->cptr[r + 1] - 1 - j : hs.l_rowptr[r] + j; };
+    auto nent = [&](int r) { return upper ? s->cptr[r + 1] - s->cptr[r] - 1 : hs.l_rowptr[r + 1] - hs.l_rowptr[r] - 1; };
+    auto dpos = [&](int r) { return upper ? s->cptr[r] : hs.l_rowptr[r + 1] - 1; };
+    if ((int)D.cblk.size() != P + 1 || (int)D.cfetch.size() != P + 1 || (int)D.code.size() != 4 * n) return bad("table sizes");
+    std::vector<char> ready(n, 0);
+    struct Cta {
+        int step = 0, ns = 0, i0 = 0, nrows = 0, nf0 = 0;
+        std::vector<double> slot;
+        std::vector<int> owner;  // row whose value a slot holds (-1: none yet)
+    };
+    std::vector<Cta> cta(P);
+    for (int c = 0; c < P; c++) {
+        Cta &K = cta[c];
+        const int4 cb = D.cblk[c];
+        K.ns = cb.z;
+        K.i0 = cb.x;
+        K.nrows = C.soff[c + 1] - C.soff[c];
+        K.nf0 = F.dir[0].cfetch[c + 1] - F.dir[0].cfetch[c];
+        const int nf = D.cfetch[c + 1] - D.cfetch[c];
+        if (cb.w != C.soff[c]) return bad("a CTA's first record is not its first row");
+        if (cb.y != K.ns + 2 + K.nrows || cb.x + cb.y > (int)D.ints.size()) return bad("int block size");
+        if (16 * cb.y > 16 * D.ints_max) return bad("int block larger than its shared region");
+        if (K.nrows + 1 + K.nf0 + (d ? nf : 0) > F.nslot_max) return bad("slots beyond the shared slot region");
+        K.slot.assign((size_t)F.nslot_max, 0.0);
+        K.owner.assign((size_t)F.nslot_max, -1);
+        for (int k = 0; k < K.nrows; k++) {
+            K.slot[k] = b[C.srow[C.soff[c] + k]];
+            K.owner[k] = -2;  // staged right-hand side
+        }
+        K.slot[K.nrows] = -0.0;
+    }
+    int remaining = 0;
+    for (int c = 0; c < P; c++) remaining += cta[c].ns > 0;
+    while (remaining > 0) {
+        bool progress = false;
+        for (int c = 0; c < P; c++) {
+            Cta &K = cta[c];
+            if (K.step >= K.ns) continue;
+            const int4 st = D.ints[K.i0 + K.step];
+            const int nl = st.y, rb = K.i0 + K.ns + 2;
+            if (nl < 1 || nl > F.ncomp) return bad("step row count out of range");
+            if (st.x < 0 || st.x + nl > K.nrows) return bad("step records out of range");
+            const int fb = D.cfetch[c], sbase = K.nrows + 1 + (d ? K.nf0 : 0), nf = D.cfetch[c + 1] - fb;
+            // a step runs once every staged value it reads has been written by its producer
+            bool wait = false;
+            for (int q = 0; q < nl && !wait; q++) {
+                const int4 r = D.ints[rb + st.x + q];
+                const int sl[3] = {r.y, r.z, r.w};
+                for (int j = 0; j < 3; j++)
+                    if (sl[j] >= sbase) {
+                        if (sl[j] >= sbase + nf) return bad("staging slot beyond the fetch list");
+                        if (!ready[D.frow[fb + sl[j] - sbase]]) wait = true;
+                    }
+            }
+            if (wait) continue;
+            std::vector<double> outs(nl);
+            for (int q = 0; q < nl; q++) {
+                const int4 r = D.ints[rb + st.x + q];
+                if (r.x < 0 || r.x >= K.nrows) return bad("own slot out of range");
+                const int row = C.srow[C.soff[c] + r.x];
+                if (ready[row]) return bad("a row computed twice");
+                const int ne = nent(row);
+                const int *code = D.codeT.data() + 4 * (size_t)(C.soff[c] + st.x + q);
+                if (code[0] != dpos(row)) return bad("diagonal code does not name the row's diagonal");
+                const int sl[3] = {r.y, r.z, r.w};
+                double sum = 0.0;
+                for (int j = 0; j < 3; j++) {
+                    if (j >= ne) {
+                        if (sl[j] != K.nrows || code[j + 1] != -1) return bad("an absent entry does not read the zero slot");
+                        continue;
+                    }
+                    const int col = column(row, j);
+                    if (code[j + 1] != tpos(row, j)) return bad("entry code does not name the entry");
+                    double xv;
+                    if (sl[j] < K.nrows) {
+                        if (K.owner[sl[j]] != col) return bad("a local slot does not hold the column the row needs");
+                        xv = K.slot[sl[j]];
+                    } else if (sl[j] >= sbase) {
+                        if (D.frow[fb + sl[j] - sbase] != col) return bad("a staging slot names the wrong row");
+                        xv = x[col];
+                    } else {
+                        return bad("a slot between the zero slot and this direction's staging");
+                    }
+                    sum = sum + xv * tval[code[j + 1]];
+                }
+                outs[q] = (K.slot[r.x] - sum) / tval[code[0]];
+            }
+            for (int q = 0; q < nl; q++) {
+                const int4 r = D.ints[rb + st.x + q];
+                const int row = C.srow[C.soff[c] + r.x];
+                K.slot[r.x] = outs[q];
+                K.owner[r.x] = row;
+                x[row] = outs[q];
+                ready[row] = 1;
+            }
+            if (++K.step == K.ns) {
+                remaining--;
+                const int4 t0 = D.ints[K.i0 + K.ns], t1 = D.ints[K.i0 + K.ns + 1], tl = D.ints[K.i0 + K.ns - 1];
+                if (t0.x != tl.x || t0.y != tl.y || t1.x != tl.x || t1.y != tl.y) return bad("terminal step copies");
+            }
+            progress = true;
+        }
+        if (!progress) return bad("no CTA can make progress (the plan would deadlock)");
+    }
+    for (int i = 0; i < n; i++)
+        if (!ready[i]) return bad("a row was never computed");
+    return BAAS_OK;
+}
+
 // Frees the schedule's device state (plan, workspaces) on its device and returns the schedule to
 // its state right after analysis; the host schedule and the batch offsets stay.
 static void release_device(baas_schedule *s) {
@@ -1158,8 +1627,12 @@ static void release_device(baas_schedule *s) {
         s->d_fwd.release();
         s->d_bwd.release();
         s->d_chk.release();
+        s->d_fch.release();
         for (auto &kv : s->wins) kv.second.release();
         for (int d = 0; d < 2; d++) {
+            if (s->d_gf64[d]) cudaFree(s->d_gf64[d]);
+            if (s->d_gf32[d]) cudaFree(s->d_gf32[d]);
+            if (s->d_gfT[d]) cudaFree(s->d_gfT[d]);
             if (s->d_gv64[d]) cudaFree(s->d_gv64[d]);
             if (s->d_gv32[d]) cudaFree(s->d_gv32[d]);
             if (s->d_gvT[d]) cudaFree(s->d_gvT[d]);
@@ -1204,10 +1677,12 @@ baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
     if (opt->nthread != s->hs.nthread) return fail(BAAS_ERR_BAD_ARG, "nthread is fixed by the analysis");
     if (opt->mapping != s->opt.mapping) return fail(BAAS_ERR_BAD_ARG, "mapping is fixed by the analysis");
     if (opt->parts < 0 || opt->smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "parts and smem_budget must be >= 0");
+    if (opt->walk < BAAS_WALK_AUTO || opt->walk > BAAS_WALK_FETCH) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
     if (opt->partition == BAAS_PARTITION_CUSTOM) {
         if (s->custom_part.empty()) return fail(BAAS_ERR_BAD_ARG, "no custom partition: use baas_replan_custom");
         if (opt->parts != s->opt.parts) return fail(BAAS_ERR_BAD_ARG, "a custom partition fixes parts");
-    } else if (opt->partition != BAAS_PARTITION_RANGES && opt->partition != BAAS_PARTITION_BAAS_THREADS) {
+    } else if (opt->partition != BAAS_PARTITION_RANGES && opt->partition != BAAS_PARTITION_BAAS_THREADS &&
+               opt->partition != BAAS_PARTITION_BLOCKS && opt->partition != BAAS_PARTITION_AUTO) {
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     }
     release_device(s);
@@ -1240,6 +1715,31 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
     BAAS_TRY(ensure_device(s));
     cudaStream_t stream = (cudaStream_t)stream_;
     const int d = upper ? 1 : 0;
+    bool fw = false;
+    if (nrhs == 1) BAAS_TRY(pick_walk(s, 8, false, fw));
+    if (fw) {
+        if (!s->d_gfT[d]) BAAS_TRY(dalloc(s->d_gfT[d], (size_t)baas::kFetchVal64 * n));
+        baas::FetchPlan fp = fetch_plan(s, 8, false);
+        const size_t smem = fetch_smem(s->fch, 8, false);
+        unsigned int spin = s->spin();
+        double *gv = s->d_gfT[d];
+        void *args[] = {(void *)&fp, (void *)&d, (void *)&T->values, (void *)&gv, (void *)&b, (void *)&x,
+                        (void *)&s->d_status, (void *)&spin, (void *)&s->d_trace};
+        s->last_walk = BAAS_WALK_FETCH;
+        for (int ieee = 0; ieee < 2; ieee++) {
+            BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+            const int fill_blocks = (int)std::min<long long>(4LL * s->num_sms, ((long long)n + 255) / 256);
+            baas::k_fill_sentinel<double><<<std::max(fill_blocks, 1), 256, 0, stream>>>(x, n, 1, ldb);
+            BAAS_CUDA(cudaGetLastError());
+            BAAS_CUDA(cudaLaunchCooperativeKernel(sweep_fetch_kernel(ieee != 0), s->P, baas::kStageBlock, args, smem, stream));
+            dump_trace(s, upper ? "sptrsv-upper" : "sptrsv-lower", stream);
+            const baas_status st = read_status(s, stream);
+            if (!needs_ieee_repeat(s)) return st;
+        }
+        return fail(BAAS_ERR_CUDA, "IEEE sweep reported a fast-path division");
+    }
+    s->last_walk = BAAS_WALK_CHUNKED;
+    if (s->opt.walk == BAAS_WALK_FETCH) return fail(BAAS_ERR_BAD_ARG, "the fetch walk takes one right-hand side");
     // right-hand sides walked together: as many as the solution slots leave room for
     const int R = std::min(nrhs, s->rmax64);
     WinCfg *w = nullptr;
@@ -1550,6 +2050,14 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
         s->ws_ready = true;
     }
     const bool mixed = precision == BAAS_PREC_FP32_FACTORS;
+    bool fw = false;
+    BAAS_TRY(pick_walk(s, mixed ? 4 : 8, true, fw));
+    if (fw && !s->d_gf64[0]) {
+        for (int d = 0; d < 2; d++) {
+            BAAS_TRY(dalloc(s->d_gf64[d], (size_t)baas::kFetchVal64 * n));
+            BAAS_TRY(dalloc(s->d_gf32[d], (size_t)baas::kFetchVal32 * n));
+        }
+    }
     WinCfg *w = nullptr;
     BAAS_TRY(get_windows(s, mixed ? 4 : 8, 1, &w));
     if (!mixed) BAAS_TRY(save_x0(s, x, (size_t)n, stream));
@@ -1590,6 +2098,16 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
     a.reuse = reuse ? 1 : 0;
     a.xf = xf;
     a.grad_a = grad_a;
+    size_t smem = w->smem;
+    if (fw) {
+        a.fp = fetch_plan(s, mixed ? 4 : 8, true);
+        for (int d = 0; d < 2; d++) {
+            a.gf64[d] = s->d_gf64[d];
+            a.gf32[d] = s->d_gf32[d];
+        }
+        smem = fetch_smem(s->fch, mixed ? 4 : 8, true);
+    }
+    s->last_walk = fw ? BAAS_WALK_FETCH : BAAS_WALK_CHUNKED;
     void *args[] = {(void *)&a};
     const bool stg = w->rhs_bytes > 0;
     int it = 0;
@@ -1601,7 +2119,8 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
         a.epoch = s->epoch;
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
         BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
-        BAAS_CUDA(cudaLaunchCooperativeKernel(iccg_kernel(mixed, stg, ieee != 0), P, baas::kStageBlock, args, w->smem, stream));
+        BAAS_CUDA(cudaLaunchCooperativeKernel(iccg_kernel(mixed, fw ? false : stg, ieee != 0, fw), P, baas::kStageBlock, args,
+                                              smem, stream));
         BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));
         BAAS_CUDA(cudaMemcpyAsync(&rr, s->d_relres, sizeof(double), cudaMemcpyDeviceToHost, stream));
         dump_trace(s, "iccg", stream);

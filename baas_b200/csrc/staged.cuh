@@ -30,6 +30,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "fetch.cuh"
 #include "part_kernels.cuh"
 
 namespace baas {
@@ -37,6 +38,7 @@ namespace baas {
 // 256 threads: steps hold tens of rows per CTA, so more threads would only add idle warps to
 // every step barrier; and the pipelined walk gets up to 255 registers.
 constexpr int kStageBlock = 256;
+static_assert(kStageBlock == kFetchBlock, "the fetch walk runs in the chunked kernels' CTAs");
 constexpr int kChunkHdr = 4;
 constexpr int kIssuer = kStageBlock - 32;  // lane 0 of the last warp issues the bulk copies
 constexpr int kMaxRhs = 8;                 // right-hand sides walked together
@@ -816,6 +818,9 @@ struct IccgArgs {
     int reuse;         // 1: the value slots already hold the factors (adjoint solves)
     const double *xf;  // with grad_a: the forward solution x
     double *grad_a;    // if set: grad_a[e] = -x_i * xf_j for each entry e = (i, j) of A
+    FetchPlan fp;      // fetch-walk plan (kernels instantiated with FW)
+    double *gf64[2];   // fetch-walk record values per direction, FP64 factors
+    float *gf32[2];    // the same, FP32 factors
 };
 
 // Vector phases take L rows (or elements) per thread per pass: rows i, i + W, ..., i + (L-1) W
@@ -892,6 +897,124 @@ __device__ __forceinline__ bool chunk_precond(const IccgArgs &A, WinStream<T> &w
     return true;
 }
 
+// Shared-memory addresses of a fetch walk (fetch.cuh): slots, the int blocks (both directions
+// resident), the value buffer (FP64: one direction at a time; FP32: both), the control block.
+struct FetchSh {
+    unsigned int SL, RW, I[2], V[2];
+    FetchCtl *ctl;
+    int nrows, s0, nf0, nf1, ns[2];
+};
+template <typename T>
+__device__ __forceinline__ FetchSh fetch_layout(const FetchPlan &fp, unsigned char *smem, bool two_dirs) {
+    const int c = blockIdx.x;
+    FetchSh F;
+    const unsigned int slot_bytes = ((unsigned int)fp.nslot * (unsigned int)sizeof(T) + 15u) & ~15u;
+    F.s0 = __ldg(fp.soff + c);
+    F.nrows = __ldg(fp.soff + c + 1) - F.s0;
+    F.SL = smem_u32(smem);
+    F.RW = F.SL + slot_bytes;
+    F.I[0] = F.RW + (unsigned int)fp.srow_bytes;
+    F.I[1] = F.I[0] + (unsigned int)fp.ints_bytes[0];
+    const unsigned int vb = F.I[1] + (two_dirs ? (unsigned int)fp.ints_bytes[1] : 0u);
+    F.V[0] = vb;
+    F.V[1] = sizeof(T) == 4 && two_dirs ? vb + 16u * (unsigned int)F.nrows : vb;
+    F.ctl = reinterpret_cast<FetchCtl *>(smem + (vb - F.SL) + (unsigned int)fp.vals_bytes);
+    F.nf0 = __ldg(fp.dir[0].cfetch + c + 1) - __ldg(fp.dir[0].cfetch + c);
+    F.nf1 = __ldg(fp.dir[1].cfetch + c + 1) - __ldg(fp.dir[1].cfetch + c);
+    F.ns[0] = __ldg(fp.dir[0].cblk + c).z;
+    F.ns[1] = __ldg(fp.dir[1].cblk + c).z;
+    return F;
+}
+// Issues the copies of the int blocks (both directions when two_dirs, else direction d at I[0])
+// on mbar_ints. One thread.
+__device__ __forceinline__ void fetch_issue_ints(const FetchPlan &fp, const FetchSh &F, bool two_dirs, int d) {
+    const int4 c0 = __ldg(fp.dir[two_dirs ? 0 : d].cblk + blockIdx.x);
+    const int4 c1 = __ldg(fp.dir[1].cblk + blockIdx.x);
+    fence_async_shared();
+    mbar_expect_tx(&F.ctl->mbar_ints, 16u * (unsigned int)(c0.y + (two_dirs ? c1.y : 0)));
+    fetch_copy(F.I[0], fp.dir[two_dirs ? 0 : d].ints + c0.x, 16u * (unsigned int)c0.y, &F.ctl->mbar_ints);
+    if (two_dirs) fetch_copy(F.I[1], fp.dir[1].ints + c1.x, 16u * (unsigned int)c1.y, &F.ctl->mbar_ints);
+}
+// Issues the copy of this CTA's record values of direction d (both directions, FP32 only, when
+// both) into V[d] (V[0], V[1]) on mbar_vals. One thread.
+template <typename T>
+__device__ __forceinline__ void fetch_issue_vals(const FetchPlan &fp, const FetchSh &F, T *const gv[2], int d, bool both) {
+    constexpr unsigned int RB = sizeof(T) == 8 ? 8u * kFetchVal64 : 4u * kFetchVal32;
+    const unsigned int bytes = RB * (unsigned int)F.nrows;
+    fence_async_shared();
+    mbar_expect_tx(&F.ctl->mbar_vals, both ? 2u * bytes : bytes);  // 0 bytes (no rows): the phase completes here
+    for (int k = both ? 0 : d; bytes > 0 && k <= (both ? 1 : d); k++) {
+        const int rb = __ldg(fp.dir[k].cblk + blockIdx.x).w;
+        fetch_copy(F.V[k], reinterpret_cast<const unsigned char *>(gv[k]) + (size_t)RB * (size_t)rb, bytes, &F.ctl->mbar_vals);
+    }
+}
+
+// Fetch-walk preconditioner (fetch.cuh): z = U^-1 L^-1 r on this CTA's rows, p = z if set_p, and
+// this thread's share of r.z. r is staged in the row slots; the lower walk leaves y there, the
+// upper walk z. The compute warps walk both directions while the last warp fetches both
+// directions' remote values. FP64 values: the lower block was copied in before this call (by
+// the caller, or by the previous call's tail); the upper block is copied once the lower walk
+// is over, and this call's tail starts the copy of the next lower block. Thread 0 issues every
+// copy and keeps in vpend the mbarrier parity of the one in flight (-1: none), which it awaits
+// before the kernel exits. false (uniform) if a wait gave up.
+template <typename T, bool IEEE>
+__device__ __forceinline__ bool fetch_precond(const IccgArgs &A, const FetchSh &F, bool set_p, double &rz, int &vpend) {
+    constexpr unsigned int S = sizeof(T);
+    const FetchPlan &fp = A.fp;
+    const int tid = (int)threadIdx.x, c = blockIdx.x;
+    T *yg = sizeof(T) == 8 ? (T *)A.y : (T *)A.y32;
+    T *zg = sizeof(T) == 8 ? (T *)A.z : (T *)A.z32;
+    for (int k = tid; k < F.nrows; k += blockDim.x) Sh<T>::stu(F.SL + S * (unsigned int)k, (T)A.r[__ldg(fp.srow + F.s0 + k)]);
+    fetch_reset_slots<T>(F.SL, F.nrows, F.nf0 + F.nf1);
+    if constexpr (sizeof(T) == 8) {
+        if (!mbar_wait(&F.ctl->mbar_vals, 0u, A.spin_limit) && atomicCAS(&A.st->code, kOk, kTimeout) == kOk)
+            A.st->where = -3000000;
+        if (tid == 0) vpend = -1;
+    }
+    __syncthreads();
+    trace_mark(A.trace, 56);
+    bool slow = false;
+    if (tid >= kFetchWarp * 32) {
+        const int *f0 = fp.dir[0].frow + __ldg(fp.dir[0].cfetch + c);
+        const int *f1 = fp.dir[1].frow + __ldg(fp.dir[1].cfetch + c);
+        fetch_run<T>(f0, F.nf0, yg, F.SL + S * (unsigned int)(F.nrows + 1), A.spin_limit, A.st, F.ctl);
+        fetch_run<T>(f1, F.nf1, zg, F.SL + S * (unsigned int)(F.nrows + 1 + F.nf0), A.spin_limit, A.st, F.ctl);
+    } else if (tid < fp.ncomp) {
+        walk_fetch<T, kDiv<T, IEEE>>(F.I[0], F.V[0], F.SL, F.RW, F.ns[0], fp.ncomp, yg, A.spin_limit, A.st, F.ctl, slow);
+        if constexpr (sizeof(T) == 8) {
+            // the lower walk's last step barrier has passed: every compute thread is done with
+            // the lower values
+            if (tid == 0) {
+                fetch_issue_vals<T>(fp, F, reinterpret_cast<T *const *>(A.gf64), 1, false);
+                vpend = 1;
+            }
+            if (!mbar_wait(&F.ctl->mbar_vals, 1u, A.spin_limit)) {
+                F.ctl->err = 1;
+            } else if (tid == 0) {
+                vpend = -1;
+            }
+        }
+        walk_fetch<T, kDiv<T, IEEE>>(F.I[1], F.V[1], F.SL, F.RW, F.ns[1], fp.ncomp, zg, A.spin_limit, A.st, F.ctl, slow);
+    }
+    if (kDiv<T, IEEE> == 1 && slow) A.st->slow_div = 1;
+    trace_mark(A.trace, 57);
+    if (__syncthreads_or(F.ctl->err)) return false;
+    if constexpr (sizeof(T) == 8) {
+        if (tid == 0) {
+            fetch_issue_vals<T>(fp, F, reinterpret_cast<T *const *>(A.gf64), 0, false);
+            vpend = 0;
+        }
+    }
+    for (int k = tid; k < F.nrows; k += blockDim.x) {
+        const int row = __ldg(fp.srow + F.s0 + k);
+        const double zd = (double)Sh<T>::ldu(F.SL + S * (unsigned int)k);
+        rz = __dadd_rn(rz, __dmul_rn(A.r[row], zd));
+        if (set_p) A.p[row] = zd;
+    }
+    trace_mark(A.trace, 59);
+    return true;
+}
+
 // This CTA's value slots of one direction from the IC0 factor lu (FP32: the diagonal as its
 // reciprocal).
 template <typename T>
@@ -913,7 +1036,7 @@ __device__ __forceinline__ void pack_factor(const ChunkDir &D, const double *lu,
 // staged in shared memory (when they fit). One instantiation per combination keeps each one's
 // register budget to what it uses. IEEE (FP64 factors only): sweep divisions by __ddiv_rn, for the
 // repeat of a launch whose div_fast divisions left their range.
-template <typename T, bool STG, bool IEEE>
+template <typename T, bool STG, bool IEEE, bool FW>
 __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     constexpr bool kMixed = sizeof(T) == 4;
     constexpr int kLanes = kMixed ? 1 : 4;
@@ -924,12 +1047,40 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     unsigned int nb = 0;
     Waiter w(A.spin_limit, A.st);
     WinStream<T> ws;
-    ws.init(A.pl, 0, true, kMixed ? (const T *)A.gv32[0] : (const T *)A.gv64[0],
-            kMixed ? (const T *)A.gv32[1] : (const T *)A.gv64[1], smem, 0xFFFFFFFFu);
+    FetchSh F;
+    int vpend = -1;           // thread 0: parity of the value copy in flight (fetch walk)
+    bool ints_pending = FW;   // the int blocks' copy has not been awaited yet
+    if constexpr (FW) {
+        F = fetch_layout<T>(A.fp, smem, true);
+        if (threadIdx.x == 0) {
+            F.ctl->err = 0;
+            mbar_init(&F.ctl->mbar_ints, 1);
+            mbar_init(&F.ctl->mbar_vals, 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) fetch_issue_ints(A.fp, F, true, 0);
+        for (int k = threadIdx.x; k < F.nrows; k += blockDim.x) Sh<int>::stu(F.RW + 4u * (unsigned int)k, __ldg(A.fp.srow + F.s0 + k));
+    } else {
+        ws.init(A.pl, 0, true, kMixed ? (const T *)A.gv32[0] : (const T *)A.gv64[0],
+                kMixed ? (const T *)A.gv32[1] : (const T *)A.gv64[1], smem, 0xFFFFFFFFu);
+    }
+    // waits (bounded) for this CTA's bulk copies still in flight before it exits
+    auto drain = [&]() {
+        if constexpr (FW) {
+            if (threadIdx.x == 0) {
+                if (ints_pending) mbar_wait(&F.ctl->mbar_ints, 0u, A.spin_limit);
+                if (vpend >= 0) mbar_wait(&F.ctl->mbar_vals, (unsigned int)vpend, A.spin_limit);
+            }
+            __syncthreads();
+        } else {
+            ws.drain(A.spin_limit);
+        }
+    };
 #define BAAS_BARRIER()                                            \
     do {                                                          \
         if (!grid_barrier(A.bar, nb, A.st, A.spin_limit)) {       \
-            ws.drain(A.spin_limit);                               \
+            drain();                                              \
             return;                                               \
         }                                                         \
     } while (0)
@@ -947,9 +1098,27 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
 
         // pack this CTA's value slots of L and U = L^T (IC0_preconditioner split,
         // test/iccg_level_merge.cpp:874-891)
-        pack_factor<T>(A.pl.dir[0], A.lu, A.gv64[0], A.gv32[0]);
-        pack_factor<T>(A.pl.dir[1], A.lu, A.gv64[1], A.gv32[1]);
+        if constexpr (FW) {
+            for (int d = 0; d < 2; d++)
+                fetch_pack<T>(A.fp.dir[d], A.fp.dir[d].code, A.lu, kMixed ? (T *)A.gf32[d] : (T *)A.gf64[d]);
+        } else {
+            pack_factor<T>(A.pl.dir[0], A.lu, A.gv64[0], A.gv32[0]);
+            pack_factor<T>(A.pl.dir[1], A.lu, A.gv64[1], A.gv32[1]);
+        }
         fence_async_global();
+    }
+    if constexpr (FW) {
+        // the record values this CTA walks first: FP32 both directions (they stay), FP64 the
+        // lower block (the upper one follows each lower walk)
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if constexpr (kMixed) {
+                fetch_issue_vals<T>(A.fp, F, reinterpret_cast<T *const *>(A.gf32), 0, true);
+            } else {
+                fetch_issue_vals<T>(A.fp, F, reinterpret_cast<T *const *>(A.gf64), 0, false);
+            }
+            vpend = 0;
+        }
     }
     // r = b - A x; sentinels
     double acc = 0.0;
@@ -972,8 +1141,19 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     trace_mark(A.trace, 3);
 
     double rzl = 0.0;
-    if (!chunk_precond<T, STG, IEEE>(A, ws, smem, true, rzl, w)) {
-        ws.drain(A.spin_limit);
+    if constexpr (FW) {
+        bool ok = mbar_wait(&F.ctl->mbar_ints, 0u, A.spin_limit);
+        if (kMixed) ok = mbar_wait(&F.ctl->mbar_vals, 0u, A.spin_limit) && ok;
+        if (!ok && atomicCAS(&A.st->code, kOk, kTimeout) == kOk) A.st->where = -3000001;
+        if (__syncthreads_or(!ok)) {
+            drain();
+            return;
+        }
+        ints_pending = false;
+        if (kMixed && threadIdx.x == 0) vpend = -1;
+    }
+    if (!(FW ? fetch_precond<T, IEEE>(A, F, true, rzl, vpend) : chunk_precond<T, STG, IEEE>(A, ws, smem, true, rzl, w))) {
+        drain();
         return;
     }
     trace_mark(A.trace, 4);
@@ -1037,8 +1217,8 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
         if (rel < A.tol) break;
 
         rzl = 0.0;
-        if (!chunk_precond<T, STG, IEEE>(A, ws, smem, false, rzl, w)) {
-            ws.drain(A.spin_limit);
+        if (!(FW ? fetch_precond<T, IEEE>(A, F, false, rzl, vpend) : chunk_precond<T, STG, IEEE>(A, ws, smem, false, rzl, w))) {
+            drain();
             return;
         }
         if (k <= 8) trace_mark(A.trace, 8 + 5 * (k - 1));
@@ -1077,12 +1257,68 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
                 A.grad_a[e] = __dmul_rn(li, __ldg(A.xf + __ldg(A.a_colidx + e)));
         }
     }
-    ws.drain(A.spin_limit);
+    drain();
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *A.out_iters = iters;
         *A.out_relres = rel;
     }
 #undef BAAS_BARRIER
+}
+
+// Standalone sweep of the caller's triangular CSR by the fetch walk (fetch.cuh): one right-hand
+// side, direction d (0: L, 1: U = L^T). gv: this direction's record values, gathered from tval
+// here; x must hold the sentinel on entry (its entries are the rows' ready flags). IEEE: divide
+// with __ddiv_rn (the repeat of a launch whose div_fast divisions left their range).
+template <bool IEEE>
+__global__ void __launch_bounds__(kStageBlock, 1) k_sweep_fetch(FetchPlan fp, int d, const double *__restrict__ tval,
+                                                               double *gv, const double *__restrict__ b, double *x,
+                                                               DevStatus *st, unsigned int spin, unsigned long long *trace) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr unsigned int S = sizeof(double);
+    const int tid = (int)threadIdx.x, c = blockIdx.x;
+    trace_mark(trace, 0);
+    const FetchSh F = fetch_layout<double>(fp, smem, false);
+    if (tid == 0) {
+        F.ctl->err = 0;
+        mbar_init(&F.ctl->mbar_ints, 1);
+        mbar_init(&F.ctl->mbar_vals, 1);
+        fence_mbar_init();
+    }
+    fetch_pack<double>(fp.dir[d], fp.dir[d].codeT, tval, gv);
+    fence_async_global();
+    __syncthreads();
+    if (tid == 0) {
+        fetch_issue_ints(fp, F, false, d);
+        double *const gvs[2] = {gv, gv};
+        fetch_issue_vals<double>(fp, F, gvs, d, false);
+    }
+    for (int k = tid; k < F.nrows; k += blockDim.x) {
+        const int row = __ldg(fp.srow + F.s0 + k);
+        Sh<double>::stu(F.SL + S * (unsigned int)k, b[row]);
+        Sh<int>::stu(F.RW + 4u * (unsigned int)k, row);
+    }
+    fetch_reset_slots<double>(F.SL, F.nrows, F.nf0 + F.nf1);
+    bool ok = mbar_wait(&F.ctl->mbar_ints, 0u, spin);
+    ok = mbar_wait(&F.ctl->mbar_vals, 0u, spin) && ok;
+    if (!ok && atomicCAS(&st->code, kOk, kTimeout) == kOk) st->where = -3000002;
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) {  // both copies were issued: let them land before the CTA exits
+            mbar_wait(&F.ctl->mbar_ints, 0u, spin);
+            mbar_wait(&F.ctl->mbar_vals, 0u, spin);
+        }
+        return;
+    }
+    trace_mark(trace, 1);
+    bool slow = false;
+    if (tid >= kFetchWarp * 32) {
+        const int *f = fp.dir[d].frow + __ldg(fp.dir[d].cfetch + c);
+        fetch_run<double>(f, d ? F.nf1 : F.nf0, x, F.SL + S * (unsigned int)(F.nrows + 1 + (d ? F.nf0 : 0)), spin, st, F.ctl);
+    } else if (tid < fp.ncomp) {
+        walk_fetch<double, IEEE ? 2 : 1>(F.I[0], F.V[d], F.SL, F.RW, F.ns[d], fp.ncomp, x, spin, st, F.ctl, slow);
+    }
+    if (!IEEE && slow) st->slow_div = 1;
+    __syncthreads();
+    trace_mark(trace, 2);
 }
 
 }  // namespace baas

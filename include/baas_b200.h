@@ -104,13 +104,23 @@ typedef struct baas_options {
     int spin_limit;   /* polls before a device wait gives up (0 = library default) */
     int parts;        /* CTAs that own rows in the partitioned kernels (0 = automatic: about one
                          per 2,048 rows, at most 128 and at most one per SM) */
-    int partition;    /* BAAS_PARTITION_RANGES (default), BAAS_PARTITION_BAAS_THREADS, or
-                         BAAS_PARTITION_CUSTOM (set by baas_replan_custom only) */
+    int partition;    /* BAAS_PARTITION_AUTO (default), BAAS_PARTITION_RANGES, BAAS_PARTITION_BLOCKS,
+                         BAAS_PARTITION_BAAS_THREADS, or BAAS_PARTITION_CUSTOM (set by
+                         baas_replan_custom only) */
     int smem_budget;  /* bytes of shared memory per CTA for solution slots and the two plan
                          window buffers (0 = library default, 220 KiB; at most 224 KiB) */
     int mapping;      /* BAAS_MAPPING_FOUR_RULE (default) or, for BAAS_KERNEL_ICCG, one of the
                          Scheduler's other mappings; fixed by the analysis */
+    int walk;         /* BAAS_WALK_AUTO (default) or BAAS_WALK_CHUNKED: which triangular-sweep
+                         kernel the single-right-hand-side sweeps and ICCG use */
 } baas_options;
+
+/* Triangular-sweep kernels. CHUNKED: the plan streamed through shared memory in windows, any row
+ * width, up to 8 right-hand sides walked together. FETCH: rows of at most 3 off-diagonal entries
+ * (stencil matrices) and one right-hand side; the compute warps read every dependency from shared
+ * memory while the CTA's last warp brings other CTAs' results in. AUTO: FETCH wherever the plan
+ * qualifies and fits shared memory, else CHUNKED. Results are bit-identical between the two. */
+enum { BAAS_WALK_AUTO = 0, BAAS_WALK_CHUNKED = 1, BAAS_WALK_FETCH = 2 };
 
 /* How the analysis maps groups to the reference's virtual threads (Schedule::ALG_SCHEDULE,
  * test/Schedule.hpp:31-37, 263-281). FOUR_RULE: P2P_RULE, the BAAS four-rule mapping
@@ -135,9 +145,22 @@ enum {
 /* How rows are given to CTAs. RANGES: contiguous row-index ranges, so every cross-CTA
  * dependency of the lower sweep points to an earlier CTA. BAAS_THREADS: CTA t runs the groups the
  * four-rule mapping gives virtual thread t (requires parts == nthread or parts == 0). CUSTOM: a
- * caller's row-to-CTA map (baas_replan_custom). Any partition is deadlock-free: every CTA walks
- * its rows in level order and a row only waits on rows of lower levels. */
-enum { BAAS_PARTITION_RANGES = 0, BAAS_PARTITION_BAAS_THREADS = 1, BAAS_PARTITION_CUSTOM = 2 };
+ * caller's row-to-CTA map (baas_replan_custom). BLOCKS: when the pattern is a 1-, 2- or 3-D
+ * stencil in natural ordering (the off-diagonal offsets of L are {1, n1, n1*n2}), boxes of the
+ * grid of at most 2,048 rows, shaped to keep the sweeps' critical path inside few boxes; other
+ * patterns get RANGES. AUTO (the default): BLOCKS when the pattern is such a grid, its rows hold
+ * at most 3 off-diagonal entries, parts == 0 and the fetch walk may run (the combination it is
+ * fastest on), else RANGES. Any partition is deadlock-free (every CTA walks its rows in level
+ * order and a row only waits on rows of lower levels) and gives bit-identical sweeps and factors;
+ * the ICCG sums its dot products CTA by CTA, so its iterates differ between partitions in the
+ * last bits. */
+enum {
+    BAAS_PARTITION_RANGES = 0,
+    BAAS_PARTITION_BAAS_THREADS = 1,
+    BAAS_PARTITION_CUSTOM = 2,
+    BAAS_PARTITION_BLOCKS = 3,
+    BAAS_PARTITION_AUTO = 4
+};
 
 typedef struct baas_schedule baas_schedule;
 
@@ -158,6 +181,15 @@ int baas_schedule_export(const baas_schedule *s, int field, int *out);
 /* Wall time of baas_analyze in milliseconds (the reference's Scheduling_Time,
  * test/SpTRSV_level_merge.cpp:70). */
 double baas_schedule_analysis_ms(const baas_schedule *s);
+
+/* The sweep kernel (BAAS_WALK_CHUNKED or BAAS_WALK_FETCH) of the schedule's last baas_sptrsv or
+ * baas_iccg call; 0 before the first. No counterpart in the reference. */
+int baas_schedule_last_walk(const baas_schedule *s);
+
+/* CTAs of the schedule's current device plan (0 before one is built: at the first GPU call, or by
+ * a plan test hook). With box != NULL, writes the grid box shape and the box counts per axis
+ * (6 ints; zeros unless the plan uses grid boxes). No counterpart in the reference. */
+int baas_plan_parts(const baas_schedule *s, int *box);
 
 /* Frees the schedule and its device memory. */
 void baas_destroy(baas_schedule *s);
@@ -202,6 +234,15 @@ baas_status baas_test_inject_unsatisfiable_wait(baas_schedule *s, int row);
  * BAAS_ERR_STATE once the schedule's plan is resident on a GPU. */
 baas_status baas_test_emulate_sweep(baas_schedule *s, int parts, int smem_budget, int upper, const double *tval,
                                     const double *b, double *x);
+
+/* Plan test hook (no counterpart in the reference): builds the fetch-walk plan (BAAS_WALK_FETCH)
+ * for `parts` CTAs (0 = automatic, assuming 148 SMs) and runs it on the host, step by step and
+ * each step only once its staged values' producers are written, checking every record, slot,
+ * fetch-list entry and value code against the pattern, and writes x (host arrays; tval as for
+ * baas_test_emulate_sweep). BAAS_ERR_BAD_ARG names the first violation, or that the pattern does
+ * not qualify. Must run before the schedule's first GPU call. */
+baas_status baas_test_emulate_fetch(baas_schedule *s, int parts, int upper, const double *tval, const double *b,
+                                    double *x);
 
 /* Division test hook (no counterpart in the reference), on device arrays a, b, q of n doubles.
  * mode 0: q[i] = a[i] / b[i] as the FP64 sweeps compute it -- Markstein's correction on the stored
