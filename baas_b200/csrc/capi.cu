@@ -811,7 +811,7 @@ void build_fetch(baas_schedule *s) {
 // one direction at a time, FP32 both) or a standalone sweep (one direction).
 size_t fetch_smem(const FetchHost &F, int vbytes, bool iccg) {
     const int slot_bytes = (F.nslot_max * vbytes + 15) / 16 * 16;
-    const int srow_bytes = (F.rows_max * 4 + 15) / 16 * 16;
+    const int srow_bytes = (F.nslot_max * 4 + 15) / 16 * 16;
     const int ib0 = 16 * (iccg ? F.dir[0].ints_max : std::max(F.dir[0].ints_max, F.dir[1].ints_max));
     const int ib1 = iccg ? 16 * F.dir[1].ints_max : 0;
     const int rb = vbytes == 8 ? 8 * baas::kFetchVal64 : 4 * baas::kFetchVal32;
@@ -947,7 +947,7 @@ baas::FetchPlan fetch_plan(const baas_schedule *s, int vbytes, bool iccg) {
     p.soff = s->d_chk.soff;
     p.srow = s->d_chk.srow;
     p.nslot = F.nslot_max;
-    p.srow_bytes = (F.rows_max * 4 + 15) / 16 * 16;
+    p.srow_bytes = (F.nslot_max * 4 + 15) / 16 * 16;  // the row list and both fetch lists
     p.ints_bytes[0] = 16 * (iccg ? F.dir[0].ints_max : std::max(F.dir[0].ints_max, F.dir[1].ints_max));
     p.ints_bytes[1] = iccg ? 16 * F.dir[1].ints_max : 0;
     const int rb = vbytes == 8 ? 8 * baas::kFetchVal64 : 4 * baas::kFetchVal32;

@@ -13,10 +13,12 @@
 //     bit for bit, in the FP64 add as in the FP32 fused multiply-add), or a STAGING slot that
 //     the fetcher warp fills with another CTA's result;
 //   - the compute warps run the step without branches: lanes beyond the step's row count repeat
-//     its last row (the same value to the same places), all loads are unconditional, and a
-//     staged value that has not arrived yet is awaited behind one warp-wide vote;
+//     its last row (within a warp they read before any of them stores, so they store the same
+//     value to the same places; a warp wholly past the row count stores nothing), all loads are
+//     unconditional, and a staged value that has not arrived yet is awaited behind one
+//     warp-wide vote;
 //   - the fetcher warp (the CTA's last warp) walks the CTA's fetch list -- the remote rows in
-//     order of first use -- with two polls in flight per lane, and stores each value into its
+//     order of first use, kept in shared memory -- with four polls in flight per lane, and stores each value into its
 //     staging slot as soon as it is no longer the sentinel. It never joins the compute warps'
 //     step barrier (a named barrier), so its polls never delay a step.
 // Row operations are the reference's (merge/SpTRSV.cpp:421-478 forward, :601-660 backward):
@@ -63,14 +65,15 @@ struct FetchPlan {
     FetchDir dir[2];
     const int *soff, *srow;  // rows of each CTA (its row list: position -> row)
     int nslot;               // slots per CTA: rows + 1 + staging of both directions (the most of any CTA)
-    int srow_bytes;          // shared bytes reserved for the CTA's row list
+    int srow_bytes;          // shared bytes reserved for the CTA's row list and both fetch lists
     int ints_bytes[2];       // shared bytes reserved for each direction's int block
     int vals_bytes;          // shared bytes of the value buffer
     int ncomp;               // compute threads (a multiple of 32, at most kFetchMaxRows)
 };
 
-// Shared-memory layout of a fetch walk: [slots | row list | int block lower | int block upper |
-// values | control]; the row list and both int blocks stay resident for the launch.
+// Shared-memory layout of a fetch walk: [slots | row list | fetch lists (lower, upper) | int block
+// lower | int block upper | values | control]; all but the slots and values stay resident for the
+// launch.
 struct FetchCtl {
     unsigned long long mbar_ints, mbar_vals;
     int err;
@@ -97,37 +100,47 @@ struct FetchWait {
     }
 };
 
-// Fetcher: lane l stages entries l, l + 64, ... together with l + 32, l + 96, ...: two polls in
-// flight per lane. Entry f goes to staging slot `stage + f`.
+// Fetcher: lane l stages entries l, l + 32, l + 64, l + 96, then l + 128, ...: four polls in
+// flight per lane. The CTA's fetch list sits in shared memory (FL: its shared address); entry f
+// goes to staging slot `stage + f`.
 template <typename T>
-__device__ __forceinline__ void fetch_run(const int *__restrict__ frow, int nf, const T *xg, unsigned int stage,
-                                          unsigned int limit, DevStatus *st, FetchCtl *ctl) {
+__device__ __forceinline__ void fetch_run(unsigned int FL, int nf, const T *xg, unsigned int stage, unsigned int limit,
+                                          DevStatus *st, FetchCtl *ctl) {
     constexpr unsigned int S = sizeof(T);
+    constexpr int U = 4;
     const int l = (int)(threadIdx.x & 31);
     volatile int *cerr = &ctl->err;
-    for (int k = l; k < nf; k += 64) {
-        const int k2 = k + 32;
-        const bool two = k2 < nf;
-        const int ra = __ldg(frow + k), rb = two ? __ldg(frow + k2) : ra;
-        T va = Sent<T>::load(xg + ra), vb = Sent<T>::load(xg + rb);
-        bool da = false, db = !two;
+    for (int k0 = l; k0 < nf; k0 += 32 * U) {
+        int r[U];
+        T v[U];
+        bool done[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = k0 + 32 * u;
+            done[u] = k >= nf;
+            r[u] = Sh<int>::ldu(FL + 4u * (unsigned int)(done[u] ? k0 : k));
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = Sent<T>::load(xg + r[u]);
         FetchWait w{0u, limit};
         for (;;) {
-            if (!da && !Sent<T>::is(va)) {
-                Sh<T>::stu(stage + S * (unsigned int)k, va);
-                da = true;
+            bool all = true;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (!done[u] && !Sent<T>::is(v[u])) {
+                    Sh<T>::stu(stage + S * (unsigned int)(k0 + 32 * u), v[u]);
+                    done[u] = true;
+                }
+                all &= done[u];
             }
-            if (!db && !Sent<T>::is(vb)) {
-                Sh<T>::stu(stage + S * (unsigned int)k2, vb);
-                db = true;
-            }
-            if (da && db) break;
-            if (!w.tick(st, cerr, da ? rb : ra)) {
+            if (all) break;
+            if (!w.tick(st, cerr, r[0])) {
                 *cerr = 1;
                 return;
             }
-            if (!da) va = Sent<T>::load(xg + ra);
-            if (!db) vb = Sent<T>::load(xg + rb);
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (!done[u]) v[u] = Sent<T>::load(xg + r[u]);
         }
     }
 }
@@ -183,7 +196,7 @@ __device__ __forceinline__ void walk_fetch(unsigned int I, unsigned int V, unsig
         T x2 = Sh<T>::ldu(SL + S * (unsigned int)rec.w);
         const T rhs = Sh<T>::ldu(ko);
         const int4 recn = ldsh4(R0 + 16u * (unsigned int)(stn.x + min(tid, stn.y - 1)));
-        if ((tid & ~31) < nl) {  // warp-uniform: warps past the step's rows only join the barrier
+        {
             T o;
             if constexpr (sizeof(T) == 8) {
                 const double2 dr = ldsh_d2(va), a01 = ldsh_d2(va + 16u), a2 = ldsh_d2(va + 32u);
@@ -223,8 +236,12 @@ __device__ __forceinline__ void walk_fetch(unsigned int I, unsigned int V, unsig
                 sum = fmaf(x2, v.w, sum);
                 o = (rhs - sum) * v.x;
             }
-            Sh<T>::stu(ko, o);
-            Sent<T>::store(xg + row, o);
+            // a warp past the step's rows computed a copy of the last row and stores nothing:
+            // another warp may already have replaced that row's right-hand side by its result
+            if ((tid & ~31) < nl) {
+                Sh<T>::stu(ko, o);
+                Sent<T>::store(xg + row, o);
+            }
         }
         row = Sh<int>::ldu(RW + 4u * (unsigned int)recn.x);
         rec = recn;

@@ -900,7 +900,7 @@ __device__ __forceinline__ bool chunk_precond(const IccgArgs &A, WinStream<T> &w
 // Shared-memory addresses of a fetch walk (fetch.cuh): slots, the int blocks (both directions
 // resident), the value buffer (FP64: one direction at a time; FP32: both), the control block.
 struct FetchSh {
-    unsigned int SL, RW, I[2], V[2];
+    unsigned int SL, RW, FL[2], I[2], V[2];
     FetchCtl *ctl;
     int nrows, s0, nf0, nf1, ns[2];
 };
@@ -923,7 +923,18 @@ __device__ __forceinline__ FetchSh fetch_layout(const FetchPlan &fp, unsigned ch
     F.nf1 = __ldg(fp.dir[1].cfetch + c + 1) - __ldg(fp.dir[1].cfetch + c);
     F.ns[0] = __ldg(fp.dir[0].cblk + c).z;
     F.ns[1] = __ldg(fp.dir[1].cblk + c).z;
+    F.FL[0] = F.RW + 4u * (unsigned int)F.nrows;
+    F.FL[1] = F.FL[0] + 4u * (unsigned int)F.nf0;
     return F;
+}
+// The CTA's row list and both directions' fetch lists into shared memory (all threads; the
+// caller's next barrier publishes them).
+__device__ __forceinline__ void fetch_stage_lists(const FetchPlan &fp, const FetchSh &F) {
+    const int c = blockIdx.x;
+    const int *f0 = fp.dir[0].frow + __ldg(fp.dir[0].cfetch + c), *f1 = fp.dir[1].frow + __ldg(fp.dir[1].cfetch + c);
+    for (int k = threadIdx.x; k < F.nrows; k += blockDim.x) Sh<int>::stu(F.RW + 4u * (unsigned int)k, __ldg(fp.srow + F.s0 + k));
+    for (int k = threadIdx.x; k < F.nf0; k += blockDim.x) Sh<int>::stu(F.FL[0] + 4u * (unsigned int)k, __ldg(f0 + k));
+    for (int k = threadIdx.x; k < F.nf1; k += blockDim.x) Sh<int>::stu(F.FL[1] + 4u * (unsigned int)k, __ldg(f1 + k));
 }
 // Issues the copies of the int blocks (both directions when two_dirs, else direction d at I[0])
 // on mbar_ints. One thread.
@@ -975,12 +986,11 @@ __device__ __forceinline__ bool fetch_precond(const IccgArgs &A, const FetchSh &
     trace_mark(A.trace, 56);
     bool slow = false;
     if (tid >= kFetchWarp * 32) {
-        const int *f0 = fp.dir[0].frow + __ldg(fp.dir[0].cfetch + c);
-        const int *f1 = fp.dir[1].frow + __ldg(fp.dir[1].cfetch + c);
-        fetch_run<T>(f0, F.nf0, yg, F.SL + S * (unsigned int)(F.nrows + 1), A.spin_limit, A.st, F.ctl);
-        fetch_run<T>(f1, F.nf1, zg, F.SL + S * (unsigned int)(F.nrows + 1 + F.nf0), A.spin_limit, A.st, F.ctl);
+        fetch_run<T>(F.FL[0], F.nf0, yg, F.SL + S * (unsigned int)(F.nrows + 1), A.spin_limit, A.st, F.ctl);
+        fetch_run<T>(F.FL[1], F.nf1, zg, F.SL + S * (unsigned int)(F.nrows + 1 + F.nf0), A.spin_limit, A.st, F.ctl);
     } else if (tid < fp.ncomp) {
         walk_fetch<T, kDiv<T, IEEE>>(F.I[0], F.V[0], F.SL, F.RW, F.ns[0], fp.ncomp, yg, A.spin_limit, A.st, F.ctl, slow);
+        trace_mark(A.trace, 60);
         if constexpr (sizeof(T) == 8) {
             // the lower walk's last step barrier has passed: every compute thread is done with
             // the lower values
@@ -994,6 +1004,7 @@ __device__ __forceinline__ bool fetch_precond(const IccgArgs &A, const FetchSh &
                 vpend = -1;
             }
         }
+        trace_mark(A.trace, 61);
         walk_fetch<T, kDiv<T, IEEE>>(F.I[1], F.V[1], F.SL, F.RW, F.ns[1], fp.ncomp, zg, A.spin_limit, A.st, F.ctl, slow);
     }
     if (kDiv<T, IEEE> == 1 && slow) A.st->slow_div = 1;
@@ -1060,7 +1071,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
         }
         __syncthreads();
         if (threadIdx.x == 0) fetch_issue_ints(A.fp, F, true, 0);
-        for (int k = threadIdx.x; k < F.nrows; k += blockDim.x) Sh<int>::stu(F.RW + 4u * (unsigned int)k, __ldg(A.fp.srow + F.s0 + k));
+        fetch_stage_lists(A.fp, F);
     } else {
         ws.init(A.pl, 0, true, kMixed ? (const T *)A.gv32[0] : (const T *)A.gv64[0],
                 kMixed ? (const T *)A.gv32[1] : (const T *)A.gv64[1], smem, 0xFFFFFFFFu);
@@ -1292,11 +1303,8 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_fetch(FetchPlan fp, in
         double *const gvs[2] = {gv, gv};
         fetch_issue_vals<double>(fp, F, gvs, d, false);
     }
-    for (int k = tid; k < F.nrows; k += blockDim.x) {
-        const int row = __ldg(fp.srow + F.s0 + k);
-        Sh<double>::stu(F.SL + S * (unsigned int)k, b[row]);
-        Sh<int>::stu(F.RW + 4u * (unsigned int)k, row);
-    }
+    fetch_stage_lists(fp, F);
+    for (int k = tid; k < F.nrows; k += blockDim.x) Sh<double>::stu(F.SL + S * (unsigned int)k, b[__ldg(fp.srow + F.s0 + k)]);
     fetch_reset_slots<double>(F.SL, F.nrows, F.nf0 + F.nf1);
     bool ok = mbar_wait(&F.ctl->mbar_ints, 0u, spin);
     ok = mbar_wait(&F.ctl->mbar_vals, 0u, spin) && ok;
@@ -1311,8 +1319,8 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_fetch(FetchPlan fp, in
     trace_mark(trace, 1);
     bool slow = false;
     if (tid >= kFetchWarp * 32) {
-        const int *f = fp.dir[d].frow + __ldg(fp.dir[d].cfetch + c);
-        fetch_run<double>(f, d ? F.nf1 : F.nf0, x, F.SL + S * (unsigned int)(F.nrows + 1 + (d ? F.nf0 : 0)), spin, st, F.ctl);
+        fetch_run<double>(F.FL[d], d ? F.nf1 : F.nf0, x, F.SL + S * (unsigned int)(F.nrows + 1 + (d ? F.nf0 : 0)), spin, st,
+                          F.ctl);
     } else if (tid < fp.ncomp) {
         walk_fetch<double, IEEE ? 2 : 1>(F.I[0], F.V[d], F.SL, F.RW, F.ns[d], fp.ncomp, x, spin, st, F.ctl, slow);
     }
