@@ -8,6 +8,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstdint>
 #include <limits>
@@ -944,6 +946,15 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
                     Mapping mapping) {
     auto t0 = std::chrono::steady_clock::now();
+    // BAAS_ANALYSIS_TRACE=1: stage times of the analysis on stderr
+    const bool trace = getenv("BAAS_ANALYSIS_TRACE") && atoi(getenv("BAAS_ANALYSIS_TRACE")) > 0;
+    auto tl = t0;
+    auto stage = [&](const char *name) {
+        if (!trace) return;
+        const auto t = std::chrono::steady_clock::now();
+        fprintf(stderr, "[baas analysis] %s %.2f ms\n", name, std::chrono::duration<double, std::milli>(t - tl).count());
+        tl = t;
+    };
     s = HostSchedule();
     s.kind = kind;
     s.n = n;
@@ -970,11 +981,14 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         }
     Csx lower{s.l_rowptr, s.l_colidx};
     Csx dag0 = transpose(lower);  // column j: j itself, then the rows that depend on j
+    stage("lower triangle + CSC");
 
     Csx dag = two_hop_reduce(dag0);                   // stage 2
+    stage("two-hop reduction");
     Grouping rev = tree_coarsen(dag, true);           // stage 3
     Csx gdag = group_dag(n, rev, dag);                // stage 4
     Grouping fwd = tree_coarsen(gdag, false);         // stage 5
+    stage("tree coarsening + group DAGs");
     // remap forward groups (of reverse groups) onto rows (merge/Coarsen.cpp:896-928)
     s.ngroups = fwd.ngroups;
     s.group_ptr.assign(1, 0);
@@ -998,7 +1012,9 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
             s.cost[g] += 1 * (s.l_rowptr[r + 1] - s.l_rowptr[r]);
         }
 
+    stage("remap + group DAG + cost");
     level_sets(fdag, s);  // stage 7
+    stage("level sets");
     if (mapping == Mapping::FourRule || mapping == Mapping::FinishTime || mapping == Mapping::Affinity)
         threads_per_level(s);  // stage 8
     else
@@ -1006,6 +1022,7 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
     for (int g = 0; g < s.ngroups; g++)  // test/Schedule.hpp:72-79
         std::sort(s.group_set.begin() + s.group_ptr[g], s.group_set.begin() + s.group_ptr[g + 1]);
     Csx dag_csr = transpose(fdag);  // parents of each group, then the group itself
+    stage("threads per level + group sort + inverse DAG");
     if (mapping == Mapping::FourRule)
         four_rule_map(s, dag_csr);  // stage 9
     else if (mapping == Mapping::FinishTime)
@@ -1015,7 +1032,9 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
     }
     else
         cost_split_map(s, mapping == Mapping::CostSplitBarrier);
+    stage("mapping");
     task_dags(s, dag_csr);          // stage 10
+    stage("task DAGs");
     s.fdag_ptr = std::move(fdag.ptr);
     s.fdag_set = std::move(fdag.idx);
     auto t1 = std::chrono::steady_clock::now();
