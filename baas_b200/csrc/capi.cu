@@ -263,6 +263,7 @@ struct baas_schedule {
     float *d_gf32[2] = {nullptr, nullptr};   // the same, FP32
     double *d_gfT[2] = {nullptr, nullptr};   // record values of the caller's factor (sweeps)
     int last_walk = 0;                       // walk of the last sweep / ICCG launch (BAAS_WALK_*)
+    double *d_dg = nullptr;                  // fetch-walk IC0: each row's diagonal (its ready flag)
     std::map<int, WinCfg> wins;  // key: value bytes * 16 + right-hand sides
     int smem_budget = 0;
     int rmax64 = 1;  // most FP64 right-hand sides one sweep walks together
@@ -810,12 +811,14 @@ void build_fetch(baas_schedule *s) {
 // Shared bytes of a fetch-walk launch: ICCG (both directions' int blocks resident; values: FP64
 // one direction at a time, FP32 both) or a standalone sweep (one direction).
 size_t fetch_smem(const FetchHost &F, int vbytes, bool iccg) {
-    const int slot_bytes = (F.nslot_max * vbytes + 15) / 16 * 16;
+    // an ICCG launch reserves 8-byte slots in both precisions (its IC0 walk passes FP64 diagonals)
+    const int slot_bytes = (F.nslot_max * (iccg ? 8 : vbytes) + 15) / 16 * 16;
     const int srow_bytes = (F.nslot_max * 4 + 15) / 16 * 16;
     const int ib0 = 16 * (iccg ? F.dir[0].ints_max : std::max(F.dir[0].ints_max, F.dir[1].ints_max));
     const int ib1 = iccg ? 16 * F.dir[1].ints_max : 0;
     const int rb = vbytes == 8 ? 8 * baas::kFetchVal64 : 4 * baas::kFetchVal32;
-    const int vb = rb * F.rows_max * (iccg && vbytes == 4 ? 2 : 1);
+    const int vb = iccg ? std::max(rb * F.rows_max * (vbytes == 4 ? 2 : 1), 8 * baas::kFetchVal64 * F.rows_max)
+                        : rb * F.rows_max;
     return (size_t)baas::fetch_smem_bytes(slot_bytes, srow_bytes, ib0, ib1, vb);
 }
 
@@ -951,7 +954,10 @@ baas::FetchPlan fetch_plan(const baas_schedule *s, int vbytes, bool iccg) {
     p.ints_bytes[0] = 16 * (iccg ? F.dir[0].ints_max : std::max(F.dir[0].ints_max, F.dir[1].ints_max));
     p.ints_bytes[1] = iccg ? 16 * F.dir[1].ints_max : 0;
     const int rb = vbytes == 8 ? 8 * baas::kFetchVal64 : 4 * baas::kFetchVal32;
-    p.vals_bytes = rb * F.rows_max * (iccg && vbytes == 4 ? 2 : 1);
+    // ICCG: FP64 one direction, FP32 both; at least the FP64 layout of one direction, which the
+    // fetch-walk IC0 reads its A values in
+    p.vals_bytes = iccg ? std::max(rb * F.rows_max * (vbytes == 4 ? 2 : 1), 8 * baas::kFetchVal64 * F.rows_max)
+                        : rb * F.rows_max;
     p.ncomp = F.ncomp;
     return p;
 }
@@ -1633,6 +1639,9 @@ static void release_device(baas_schedule *s) {
             if (s->d_gf64[d]) cudaFree(s->d_gf64[d]);
             if (s->d_gf32[d]) cudaFree(s->d_gf32[d]);
             if (s->d_gfT[d]) cudaFree(s->d_gfT[d]);
+        }
+        if (s->d_dg) cudaFree(s->d_dg);
+        for (int d = 0; d < 2; d++) {
             if (s->d_gv64[d]) cudaFree(s->d_gv64[d]);
             if (s->d_gv32[d]) cudaFree(s->d_gv32[d]);
             if (s->d_gvT[d]) cudaFree(s->d_gvT[d]);
@@ -2057,6 +2066,7 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
             BAAS_TRY(dalloc(s->d_gf64[d], (size_t)baas::kFetchVal64 * n));
             BAAS_TRY(dalloc(s->d_gf32[d], (size_t)baas::kFetchVal32 * n));
         }
+        BAAS_TRY(dalloc(s->d_dg, (size_t)n));
     }
     WinCfg *w = nullptr;
     BAAS_TRY(get_windows(s, mixed ? 4 : 8, 1, &w));
@@ -2106,6 +2116,9 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
             a.gf32[d] = s->d_gf32[d];
         }
         smem = fetch_smem(s->fch, mixed ? 4 : 8, true);
+        // IC0 by the fetch walk when no entry's dot product has a column match
+        a.fac_fetch = s->fwd.mpair.empty() ? 1 : 0;
+        a.dg = s->d_dg;
     }
     s->last_walk = fw ? BAAS_WALK_FETCH : BAAS_WALK_CHUNKED;
     void *args[] = {(void *)&a};

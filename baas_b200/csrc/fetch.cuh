@@ -75,7 +75,7 @@ struct FetchPlan {
 // lower | int block upper | values | control]; all but the slots and values stay resident for the
 // launch.
 struct FetchCtl {
-    unsigned long long mbar_ints, mbar_vals;
+    unsigned long long mbar_ints, mbar_vals, mbar_fac;  // int blocks; record values; IC0's A values
     int err;
     int pad;
 };
@@ -297,6 +297,76 @@ __device__ __forceinline__ void fetch_pack(const FetchDir &D, const int *code, c
             g[2] = __double2float_rn(a1);
             g[3] = __double2float_rn(a2);
         }
+    }
+}
+
+// IC0 on the lower fetch plan, for patterns in which no entry's dot product has a column match
+// (the 5- and 7-point stencils): row i's entry (i, j) is then l_ij = a_ij / l_jj and its diagonal
+// l_ii = sqrt(a_ii - sum_j l_ij^2) (merge/IC.cpp:296-393 with an empty sparse_dot_product;
+// a_ij - 0.0 is a_ij bit for bit, so that subtraction is left out), the same correctly rounded
+// operations in the same order as k_factor_part. A row needs only its dependencies' final
+// diagonals, so the walk passes l_jj where the sweeps pass x_j: the row's own slot and dg[row]
+// (its ready flag for other CTAs) receive l_ii. A non-positive pivot leaves a_ii in place (and is
+// counted once per row), as the reference does. Absent entries read the zero slot, which holds
+// +1 here: 0 / 1 = +0 adds +0 to the sum of squares, which starts at +0 and never becomes -0.
+// V holds the records' A values in the FP64 record layout {a_ii, -, a0, a1, a2, -}; code are the
+// records' A positions (global; the lu writes), rec0 the CTA's first record.
+__device__ __forceinline__ void walk_ic0_fetch(unsigned int I, unsigned int V, unsigned int SL, unsigned int RW, int ns,
+                                               int ncomp, double *dg, double *lu, const int4 *__restrict__ code,
+                                               int rec0, unsigned int limit, DevStatus *st, FetchCtl *ctl) {
+    constexpr unsigned int S = 8u, RB = 8u * kFetchVal64;
+    if (ns == 0) return;
+    const int tid = (int)threadIdx.x;
+    const unsigned int R0 = I + 16u * (unsigned int)(ns + 2);
+    volatile int *cerr = &ctl->err;
+    int4 stp = ldsh4(I);
+    int4 rec = ldsh4(R0 + 16u * (unsigned int)(stp.x + min(tid, stp.y - 1)));
+    int row = Sh<int>::ldu(RW + 4u * (unsigned int)rec.x);
+    int4 cd = __ldg(code + rec0 + stp.x + min(tid, stp.y - 1));
+    for (int s = 0; s < ns; s++) {
+        const int4 stn = ldsh4(I + 16u * (unsigned int)(s + 1));
+        const int nl = stp.y;
+        const int q = min(tid, nl - 1);
+        const unsigned int va = V + RB * (unsigned int)(stp.x + q);
+        const unsigned int ko = SL + S * (unsigned int)rec.x;
+        double x0 = Sh<double>::ldu(SL + S * (unsigned int)rec.y);
+        double x1 = Sh<double>::ldu(SL + S * (unsigned int)rec.z);
+        double x2 = Sh<double>::ldu(SL + S * (unsigned int)rec.w);
+        const int4 recn = ldsh4(R0 + 16u * (unsigned int)(stn.x + min(tid, stn.y - 1)));
+        const int4 cdn = __ldg(code + rec0 + stn.x + min(tid, stn.y - 1));
+        const double2 d0 = ldsh_d2(va), a01 = ldsh_d2(va + 16u), a2 = ldsh_d2(va + 32u);
+        const bool miss = Sent<double>::is(x0) | Sent<double>::is(x1) | Sent<double>::is(x2);
+        if (__any_sync(0xffffffffu, miss)) {
+            FetchWait w{0u, limit};
+            while ((Sent<double>::is(x0) | Sent<double>::is(x1) | Sent<double>::is(x2)) && !*cerr) {
+                if (!w.tick(st, cerr, row)) *cerr = 1;
+                x0 = Sh<double>::ldu(SL + S * (unsigned int)rec.y);
+                x1 = Sh<double>::ldu(SL + S * (unsigned int)rec.z);
+                x2 = Sh<double>::ldu(SL + S * (unsigned int)rec.w);
+            }
+        }
+        const double v0 = __ddiv_rn(a01.x, x0), v1 = __ddiv_rn(a01.y, x1), v2 = __ddiv_rn(a2.x, x2);
+        double dv = 0.0;
+        dv = __dadd_rn(dv, __dmul_rn(v0, v0));
+        dv = __dadd_rn(dv, __dmul_rn(v1, v1));
+        dv = __dadd_rn(dv, __dmul_rn(v2, v2));
+        const double t = __dsub_rn(d0.x, dv);
+        const bool pos = t > 0.0;
+        const double lii = pos ? __dsqrt_rn(t) : d0.x;
+        if ((tid & ~31) < nl) {  // a warp wholly past the step's rows stores nothing
+            Sh<double>::stu(ko, lii);
+            if (cd.y >= 0) lu[cd.y] = v0;
+            if (cd.z >= 0) lu[cd.z] = v1;
+            if (cd.w >= 0) lu[cd.w] = v2;
+            lu[cd.x] = lii;
+            Sent<double>::store(dg + row, lii);
+            if (!pos && tid < nl) atomicAdd(&st->zero_pivots, 1);
+        }
+        row = Sh<int>::ldu(RW + 4u * (unsigned int)recn.x);
+        rec = recn;
+        stp = stn;
+        cd = cdn;
+        bar_compute(ncomp);
     }
 }
 

@@ -821,6 +821,8 @@ struct IccgArgs {
     FetchPlan fp;      // fetch-walk plan (kernels instantiated with FW)
     double *gf64[2];   // fetch-walk record values per direction, FP64 factors
     float *gf32[2];    // the same, FP32 factors
+    int fac_fetch;     // FW: IC0 by the fetch walk (no entry's dot product has a column match)
+    double *dg;        // with fac_fetch: each row's final diagonal, its ready flag for other CTAs
 };
 
 // Vector phases take L rows (or elements) per thread per pass: rows i, i + W, ..., i + (L-1) W
@@ -908,7 +910,9 @@ template <typename T>
 __device__ __forceinline__ FetchSh fetch_layout(const FetchPlan &fp, unsigned char *smem, bool two_dirs) {
     const int c = blockIdx.x;
     FetchSh F;
-    const unsigned int slot_bytes = ((unsigned int)fp.nslot * (unsigned int)sizeof(T) + 15u) & ~15u;
+    // an ICCG (two_dirs) reserves 8-byte slots in both precisions: its IC0 walk passes FP64 diagonals
+    const unsigned int slot_elem = two_dirs ? 8u : (unsigned int)sizeof(T);
+    const unsigned int slot_bytes = ((unsigned int)fp.nslot * slot_elem + 15u) & ~15u;
     F.s0 = __ldg(fp.soff + c);
     F.nrows = __ldg(fp.soff + c + 1) - F.s0;
     F.SL = smem_u32(smem);
@@ -1067,6 +1071,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
             F.ctl->err = 0;
             mbar_init(&F.ctl->mbar_ints, 1);
             mbar_init(&F.ctl->mbar_vals, 1);
+            mbar_init(&F.ctl->mbar_fac, 1);
             fence_mbar_init();
         }
         __syncthreads();
@@ -1100,10 +1105,55 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     if (!A.reuse) {
         const int nnz = __ldg(A.a_rowptr + n);
         for (int e = gt; e < nnz; e += W) A.lu[e] = A.a_val[e];
+        if (FW && A.fac_fetch)
+            for (int i = gt; i < n; i += W) A.dg[i] = Sent<double>::value();
         BAAS_BARRIER();
         trace_mark(A.trace, 1);
 
-        factor_part<false>(A.fac, A.a_rowptr, A.a_colidx, A.a_diag, A.lu, A.gflag, A.epoch, w, A.st);
+        if constexpr (FW) {
+            if (A.fac_fetch) {
+                // IC0 by the fetch walk: the lower records' A values into shared memory (FP64
+                // layout), the zero slot to +1, then the lower walk with l_jj as the value passed
+                fetch_pack<double>(A.fp.dir[0], A.fp.dir[0].code, A.a_val, A.gf64[0]);
+                fence_async_global();
+                fetch_reset_slots<double>(F.SL, F.nrows, F.nf0 + F.nf1);
+                if (threadIdx.x == 0) Sh<double>::stu(F.SL + 8u * (unsigned int)F.nrows, 1.0);
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    fence_async_shared();
+                    const unsigned int bytes = 8u * kFetchVal64 * (unsigned int)F.nrows;
+                    mbar_expect_tx(&F.ctl->mbar_fac, bytes);
+                    if (bytes > 0)
+                        fetch_copy(F.V[0], A.gf64[0] + (size_t)kFetchVal64 * (size_t)__ldg(A.fp.dir[0].cblk + blockIdx.x).w,
+                                   bytes, &F.ctl->mbar_fac);
+                }
+                bool ok = mbar_wait(&F.ctl->mbar_ints, 0u, A.spin_limit);
+                ok = mbar_wait(&F.ctl->mbar_fac, 0u, A.spin_limit) && ok;
+                if (!ok && atomicCAS(&A.st->code, kOk, kTimeout) == kOk) A.st->where = -3000003;
+                if (__syncthreads_or(!ok)) {
+                    if (threadIdx.x == 0) mbar_wait(&F.ctl->mbar_fac, 0u, A.spin_limit);
+                    drain();
+                    return;
+                }
+                ints_pending = false;
+                const int tid = (int)threadIdx.x;
+                if (tid >= kFetchWarp * 32) {
+                    fetch_run<double>(F.FL[0], F.nf0, A.dg, F.SL + 8u * (unsigned int)(F.nrows + 1), A.spin_limit, A.st, F.ctl);
+                } else if (tid < A.fp.ncomp) {
+                    walk_ic0_fetch(F.I[0], F.V[0], F.SL, F.RW, F.ns[0], A.fp.ncomp, A.dg, A.lu,
+                                   reinterpret_cast<const int4 *>(A.fp.dir[0].code), __ldg(A.fp.dir[0].cblk + blockIdx.x).w,
+                                   A.spin_limit, A.st, F.ctl);
+                }
+                if (__syncthreads_or(F.ctl->err)) {
+                    drain();
+                    return;
+                }
+            } else {
+                factor_part<false>(A.fac, A.a_rowptr, A.a_colidx, A.a_diag, A.lu, A.gflag, A.epoch, w, A.st);
+            }
+        } else {
+            factor_part<false>(A.fac, A.a_rowptr, A.a_colidx, A.a_diag, A.lu, A.gflag, A.epoch, w, A.st);
+        }
         BAAS_BARRIER();
         trace_mark(A.trace, 2);
 
