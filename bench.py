@@ -50,6 +50,7 @@ SWEEP_BYTES = 12 * NNZ_L + 4 * (N + 1) + 16 * N
 VEC_BYTES = 112 * N
 ITER_BYTES = SPMV_BYTES + 2 * SWEEP_BYTES + VEC_BYTES
 IC0_BYTES = 12 * NNZ_A + 4 * (N + 1) + 8 * NNZ_A
+CPU_BASELINES = True  # --no-cpu-baseline clears it
 
 
 def _peaks():
@@ -142,10 +143,10 @@ def reference_arm(args):
     b = gen.uniform_rhs(A.n, 1)
     for _ in range(args.warmup):
         Ref.pcg(A, b, maxiter=MAXITER, tol=TOL, mode=1, nthread=cores)
-    times, iters, pre = [], 0, []
+    times, iters, pre, rel = [], 0, [], None
     for _ in range(args.steps):
         x, iters, rel, t = Ref.pcg(A, b, maxiter=MAXITER, tol=TOL, mode=1, nthread=cores)
-        times.append(t[1] + t[2])  # IC0 + PCG loop (analysis excluded, as on the GPU arm)
+        times.append(t[1] + t[2])  # IC0 + initial residual + PCG loop (analysis excluded, as on the GPU arm)
         pre.append(t[0])
     v = float(np.mean(times))
     line = {
@@ -153,7 +154,8 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "iccg_laplace3d_64_shift1e-3", "n": A.n, "nnz": A.nnz, "tol": TOL,
-                   "iterations": int(iters), "l2": "host CPU run"},
+                   "iterations": int(iters), "relres": rel, "parallelism": f"openmp{cores}",
+                   "l2": "host CPU run"},
         "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": f"{args.steps} full solves (IC0 + PCG to 1e-10) with the reference's "
                                    f"Scheduler P2P_RULE at nthread={cores}"},
@@ -173,10 +175,10 @@ def cpu_baseline_sample():
         return None
     A = gen.laplace3d(K_GRID, 1e-3)
     b = gen.uniform_rhs(A.n, 1)
-    _, it, _, t = Ref.pcg(A, b, maxiter=MAXITER, tol=TOL, mode=1, nthread=cores)
+    xr, it, _, t = Ref.pcg(A, b, maxiter=MAXITER, tol=TOL, mode=1, nthread=cores)
     return {"value": round(float(t[1] + t[2]), 3), "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": f"1 full solve (IC0 + {it} PCG iterations to 1e-10) with the reference's OpenMP "
-                      f"Scheduler P2P_RULE path, nthread={cores}; analysis {t[0]:.1f} ms excluded"}
+                      f"Scheduler P2P_RULE path, nthread={cores}; analysis {t[0]:.1f} ms excluded"}, xr
 
 
 def _event_ms(fn, reps=3, flush=None):
@@ -198,6 +200,51 @@ def _event_ms(fn, reps=3, flush=None):
     return float(min(ts))
 
 
+# Latency model of a triangular sweep (the sweeps are dependency-chain bound, not bandwidth bound:
+# the whole working set stays in L2). A sweep cannot finish before its critical path has run one
+# compute step per level of the group DAG and one CTA-to-CTA hop per partition boundary on that
+# path. Both constants are B200 measurements of the fetch walk (fetch.cuh): STEP_US is a step of a
+# CTA that never waits (the 64^3 FP64 lower sweep's first CTA: 46 steps in 7.3 us, %globaltimer
+# stamps); HOP_US is one value crossing between CTAs through L2 (store, then a poll that sees it:
+# 889 cycles one way at 1965 MHz, a two-CTA ping-pong).
+STEP_US = 0.16
+HOP_US = 0.45
+
+
+def sweep_latency_bound(s):
+    """Lower bound (us) of one sweep of schedule s: levels x STEP_US + hops x HOP_US, where hops
+    are the box boundaries a monotone path crosses (grid boxes) or the CTA boundaries (ranges)."""
+    levels = int(s.export("nlevels")[0])
+    parts, box, nbox = s.plan_parts()
+    hops = sum(c - 1 for c in nbox) if nbox else max(parts - 1, 0)
+    return {"levels": levels, "hops": hops, "step_us": STEP_US, "hop_us": HOP_US,
+            "bound_us": round(levels * STEP_US + hops * HOP_US, 2), "parts": parts,
+            "box": list(box) if box else None}
+
+
+def _ref_ms(fn, reps):
+    """Mean wall time (ms) of fn() on the host over reps runs, after one untimed run."""
+    fn()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    return (time.perf_counter() - t0) * 1e3 / reps
+
+
+def c1_cpu_baseline(L, b):
+    """The reference's BAAS p2p forward sweep (SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule's
+    schedule, merge/SpTRSV.cpp:421-478) on all host cores."""
+    from oracle.oracle import Ref, ref_available
+
+    if not ref_available():
+        return None
+    cores = _host_cores()
+    rs = Ref.Schedule(0, L, cores)
+    ms = _ref_ms(lambda: rs.forward(L, b), 200)
+    return {"value": round(ms, 4), "unit": "ms", "cores": cores, "kind": "reference",
+            "sample": f"200 forward sweeps of the 128^2 lower triangle, reference p2p sweep at nthread={cores} (mean)"}
+
+
 def c1_sptrsv(flush):
     """The 128x128 5-point lower-triangle forward sweep (SpTRSV HBM GB/s)."""
     import torch
@@ -211,9 +258,20 @@ def c1_sptrsv(flush):
     x = torch.zeros_like(db)
     ms = _event_ms(lambda: s.forward(dL, db, x), 10, flush)
     nbytes = 12 * L.nnz + 4 * (L.n + 1) + 16 * L.n
-    err = float(np.max(np.abs(x.cpu().numpy() - x_true)))
-    return {"workload": "sptrsv_laplace2d_128_lower", "ms": round(ms, 4), "bytes": nbytes,
-            "gbps": round(nbytes / (ms * 1e-3) / 1e9, 2), "max_abs_err_vs_x_true": err}
+    xg = x.cpu().numpy()
+    err = float(np.max(np.abs(xg - x_true)))
+    peak, peak_kind = _peaks()
+    gbps = nbytes / (ms * 1e-3) / 1e9
+    lat = sweep_latency_bound(s)
+    lat["frac"] = round(lat["bound_us"] / (ms * 1e3), 4)
+    out = {"workload": "sptrsv_laplace2d_128_lower", "ms": round(ms, 4), "bytes": nbytes, "gbps": round(gbps, 2),
+           "max_abs_err_vs_x_true": err, "walk": s.last_walk,
+           "roofline": {"bound": "hbm", "achieved": round(gbps, 2), "peak": peak, "unit": "GB/s",
+                        "frac": round(gbps / peak, 5), "peak_kind": peak_kind, "kernel": "k_sweep_fetch"},
+           "latency_bound": lat}
+    if CPU_BASELINES:
+        out["cpu_baseline"] = c1_cpu_baseline(L, b)
+    return out
 
 
 def c3_ilu(flush):
@@ -239,10 +297,41 @@ def c3_ilu(flush):
     bwd = _event_ms(lambda: s.backward(dU, Y, Z), 5, flush)
     nnz_t = Lo.nnz
     nbytes = 12 * nnz_t + 4 * (C.n + 1) + 16 * C.n * 8
-    return {"workload": "ilu0_convdiff3d_96_8rhs", "n": C.n, "nnz": C.nnz, "ilu0_ms": round(ilu_ms, 4),
-            "forward_8rhs_ms": round(fwd, 4), "backward_8rhs_ms": round(bwd, 4),
-            "sweep_bytes_8rhs": nbytes, "forward_gbps": round(nbytes / (fwd * 1e-3) / 1e9, 2),
-            "backward_gbps": round(nbytes / (bwd * 1e-3) / 1e9, 2)}
+    peak, peak_kind = _peaks()
+    gb_f, gb_b = nbytes / (fwd * 1e-3) / 1e9, nbytes / (bwd * 1e-3) / 1e9
+    out = {"workload": "ilu0_convdiff3d_96_8rhs", "n": C.n, "nnz": C.nnz, "ilu0_ms": round(ilu_ms, 4),
+           "forward_8rhs_ms": round(fwd, 4), "backward_8rhs_ms": round(bwd, 4),
+           "total_ms": round(ilu_ms + fwd + bwd, 4),
+           "sweep_bytes_8rhs": nbytes, "forward_gbps": round(gb_f, 2), "backward_gbps": round(gb_b, 2),
+           "roofline": {"bound": "hbm", "achieved": round(gb_f, 2), "peak": peak, "unit": "GB/s",
+                        "frac": round(gb_f / peak, 5), "peak_kind": peak_kind,
+                        "kernel": "k_sweep_chunked<multi-RHS> (forward, 8 right-hand sides)"}}
+    if CPU_BASELINES:
+        out["cpu_baseline"] = c3_cpu_baseline(C, Lo, Up, B.cpu().numpy())
+    return out
+
+
+def c3_cpu_baseline(C, Lo, Up, B):
+    """The reference on all host cores: ILU0 (ilu0_p2p_csr_group_merge_no_perm_alloc) and, for
+    each of the 8 right-hand sides, its p2p forward and backward sweeps (one right-hand side per
+    call, as the reference's sweeps take)."""
+    from oracle.oracle import Ref, ref_available
+
+    if not ref_available():
+        return None
+    cores = _host_cores()
+    rs = Ref.Schedule(3, C, cores)
+    ilu_ms = _ref_ms(lambda: rs.ilu0(C), 2)
+    R = B.shape[0]
+
+    def apply():
+        for r in range(R):
+            rs.backward(Up, rs.forward(Lo, B[r]))
+
+    sw_ms = _ref_ms(apply, 2)
+    return {"value": round(ilu_ms + sw_ms, 3), "unit": "ms", "cores": cores, "kind": "reference",
+            "ilu0_ms": round(ilu_ms, 3), "forward_backward_8rhs_ms": round(sw_ms, 3),
+            "sample": f"the whole configuration (ILU0 + 8 x forward/backward p2p sweeps), mean of 2, nthread={cores}"}
 
 
 def c4_batched():
@@ -283,12 +372,214 @@ def c4_batched():
         a, b = int(off[q]), int(off[q + 1])
         d = torch.linalg.norm(x32[:, a:b] - x64[:, a:b], dim=1) / torch.linalg.norm(x64[:, a:b], dim=1)
         errs.append(float(d.max()))
-    return {"workload": "batched_vardiff2d_64sys_k64-512_4rhs", "n_total": A.n, "nnz_total": A.nnz,
-            "systems": len(systems), "rhs": 4, "ms_fp32_factors": round(ms32, 3), "ms_fp64": round(ms64, 3),
-            "iterations_fp32": {"min": int(it32.min()), "median": float(np.median(it32)), "max": int(it32.max())},
-            "max_relres": float(rel32.max()), "rel_err_vs_fp64_per_system": {"max": max(errs),
-                                                                              "median": float(np.median(errs))},
-            "autotuned": tuned["best"], "analysis_s": round(analysis_s, 2)}
+    # algorithmic bytes (the reference's model, test/iccg_level_merge.cpp:509-510) summed over
+    # the (system, right-hand side) instances, each for the iterations it ran: SpMV, two FP32-factor
+    # sweeps (8 bytes per factor entry) and the vector work, per iteration
+    itm = np.asarray(it32).reshape(len(systems), -1) if np.asarray(it32).size == 4 * len(systems) else None
+    nbytes = 0
+    for q, S in enumerate(systems):
+        nnz_l = (S.nnz + S.n) // 2
+        per_it = (12 * S.nnz + 4 * (S.n + 1) + 16 * S.n) + 2 * (8 * nnz_l + 4 * (S.n + 1) + 16 * S.n) + 112 * S.n
+        iters_q = int(itm[q].sum()) if itm is not None else int(np.max(it32)) * 4
+        nbytes += per_it * iters_q
+    peak, peak_kind = _peaks()
+    gbps = nbytes / (ms32 * 1e-3) / 1e9
+    out = {"workload": "batched_vardiff2d_64sys_k64-512_4rhs", "n_total": A.n, "nnz_total": A.nnz,
+           "systems": len(systems), "rhs": 4, "ms_fp32_factors": round(ms32, 3), "ms_fp64": round(ms64, 3),
+           "iterations_fp32": {"min": int(it32.min()), "median": float(np.median(it32)), "max": int(it32.max())},
+           "max_relres": float(rel32.max()), "rel_err_fp32_vs_fp64_gpu_per_system": {"max": max(errs),
+                                                                                     "median": float(np.median(errs))},
+           "roofline": {"bound": "hbm", "achieved": round(gbps, 2), "peak": peak, "unit": "GB/s",
+                        "frac": round(gbps / peak, 5), "peak_kind": peak_kind, "kernel": "k_iccg_batched<float>",
+                        "algorithmic_bytes_per_launch": int(nbytes)},
+           "autotuned": tuned["best"], "analysis_s": round(analysis_s, 2)}
+    if CPU_BASELINES:
+        out["cpu_baseline"] = c4_cpu_baseline(systems, B.cpu().numpy(), x32.cpu().numpy(), x64.cpu().numpy(), off)
+    return out
+
+
+def c4_cpu_baseline(systems, B, x32, x64, off):
+    """The reference's ICCG (Scheduler P2P_RULE IC0 + p2p sweeps, pcg_opt loop) on all host cores,
+    on a bounded sample: every 8th system (by size) with its first right-hand side; the time is
+    scaled to all 64 systems x 4 right-hand sides by the sample's share of the batch's rows. The
+    same FP64 solves are the oracle for the GPU's per-system errors (FP32 factors and FP64)."""
+    from oracle.oracle import Ref, ref_available
+
+    if not ref_available():
+        return None
+    cores = _host_cores()
+    order = np.argsort([S.n for S in systems])
+    pick = [int(q) for q in order[::8]]
+    t_ms, e32, e64, rows = 0.0, [], [], 0
+    for q in pick:
+        S = systems[q]
+        a, b = int(off[q]), int(off[q + 1])
+        xr, it, rel, t = Ref.pcg(S, B[0, a:b], maxiter=20000, tol=TOL, mode=1, nthread=cores)
+        t_ms += float(t[1] + t[2])
+        rows += S.n
+        e32.append(float(np.linalg.norm(x32[0, a:b] - xr) / np.linalg.norm(xr)))
+        e64.append(float(np.linalg.norm(x64[0, a:b] - xr) / np.linalg.norm(xr)))
+    total_rows = sum(S.n for S in systems)
+    est = t_ms * (total_rows / rows) * B.shape[0]
+    return {"value": round(est, 1), "unit": "ms", "cores": cores, "kind": "reference",
+            "sample": f"{len(pick)} of 64 systems (every 8th by size), right-hand side 0: {t_ms:.1f} ms of IC0 + PCG "
+                      f"to 1e-10 at nthread={cores}, scaled by rows ({total_rows}/{rows}) and by 4 right-hand sides",
+            "rel_err_vs_reference_fp64": {"systems": pick, "fp32_factors_max": max(e32),
+                                          "fp32_factors_median": float(np.median(e32)), "fp64_max": max(e64)}}
+
+
+def _iccg_case(name, A, b_h, flush, reps=3):
+    """One ICCG configuration: GPU FP64 solve time (L2 flushed, CUDA events), iterations, the walk
+    that ran, and beside it the reference's OpenMP solve of the same system (whose solution is the
+    FP64 oracle the GPU's is compared with)."""
+    import torch
+
+    from baas_b200 import KERNEL_ICCG, PREC_FP32_FACTORS, PREC_FP64, DeviceCSR, Schedule
+
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    dA = DeviceCSR.from_host(A)
+    b = torch.from_numpy(b_h).cuda()
+    x = torch.zeros_like(b)
+
+    def solve(prec):
+        x.zero_()
+        return s.iccg(dA, b, x, tol=TOL, maxiter=MAXITER, precision=prec)
+
+    it, rel = solve(PREC_FP64)
+    ms = _event_ms(lambda: solve(PREC_FP64), reps, flush)
+    x64 = x.cpu().numpy()
+    it32, _ = solve(PREC_FP32_FACTORS)
+    ms32 = _event_ms(lambda: solve(PREC_FP32_FACTORS), reps, flush)
+    x32 = x.cpu().numpy()
+    out = {"workload": name, "n": A.n, "nnz": A.nnz, "ms_fp64": round(ms, 4), "iterations": int(it), "relres": rel,
+           "ms_fp32_factors": round(ms32, 4), "iterations_fp32": int(it32), "walk": s.last_walk,
+           "partition": list(s.plan_parts()[1]) if s.plan_parts()[1] else f"ranges x{s.plan_parts()[0]}",
+           "analysis_ms": round(s.analysis_ms, 2)}
+    if CPU_BASELINES:
+        from oracle.oracle import Ref, ref_available
+
+        if ref_available():
+            cores = _host_cores()
+            xr, itr, relr, t = Ref.pcg(A, b_h, maxiter=MAXITER, tol=TOL, mode=1, nthread=cores)
+            out["cpu_baseline"] = {
+                "value": round(float(t[1] + t[2]), 3), "unit": "ms", "cores": cores, "kind": "reference",
+                "iterations": int(itr),
+                "sample": f"1 full solve (IC0 + PCG to 1e-10), Scheduler P2P_RULE at nthread={cores}",
+                "rel_err_vs_reference_fp64": {
+                    "fp64": float(np.linalg.norm(x64 - xr) / np.linalg.norm(xr)),
+                    "fp32_factors": float(np.linalg.norm(x32 - xr) / np.linalg.norm(xr))}}
+    return out
+
+
+def c2_variants(flush):
+    """Configuration 2's other inputs: the 64^3 system under the seeded random symmetric
+    permutation, and the k-NN (k = 12) 3-dof stiffness-like SPD matrix (n = 12,000)."""
+    from baas_b200 import gen
+
+    out = {}
+    P = gen.c2_system(permuted=True)
+    out["c2_permuted"] = _iccg_case("iccg_laplace3d_64_shift1e-3_permuted", P, gen.uniform_rhs(P.n, 1), flush)
+    K = gen.knn_stiffness(nodes=4000, k=12, seed=3)
+    out["c2_knn"] = _iccg_case("iccg_knn_stiffness_4000_nodes_k12", K, gen.uniform_rhs(K.n, 1), flush)
+    return out
+
+
+def c5_adjoint():
+    """Differentiated ICCG on 64^3 variable-coefficient diffusion (face kappa = exp(theta), sigma
+    0.5), FP64 CG with FP32 IC0 factors: loss 1/2 ||x - x_obs||^2, gradients w.r.t. theta and b by
+    the adjoint kernel, checked against central differences (h = 1e-6) along 32 random directions;
+    beside it the 16^3 gradient against an FP64 CPU gradient built on the reference's own PCG."""
+    import torch
+
+    from baas_b200 import PREC_FP32_FACTORS, gen
+    from baas_b200.autograd import DiffIccg, FaceDiffusion3D, face_shapes
+
+    def theta_of(k, seed, sigma=0.5):
+        return np.concatenate([gen.gaussian_field(shp, sigma, 4.0, seed + j).ravel()
+                               for j, shp in enumerate(face_shapes(k))])
+
+    def problem(k, tol):
+        op = FaceDiffusion3D(k)
+        solver = DiffIccg(op, tol=tol, maxiter=20000, precision=PREC_FP32_FACTORS)
+        theta = torch.from_numpy(theta_of(k, 11)).cuda()
+        b = torch.from_numpy(gen.uniform_rhs(op.n, 4)).cuda()
+        with torch.no_grad():
+            xp = solver.solve(theta + torch.from_numpy(theta_of(k, 23, 0.1)).cuda(), b)
+        x_obs = xp + torch.from_numpy(np.random.default_rng(5).normal(0.0, 1e-3, op.n)).cuda()
+        return op, solver, theta, b, x_obs
+
+    def grads(solver, theta, b, x_obs):
+        th = theta.clone().requires_grad_(True)
+        bb = b.clone().requires_grad_(True)
+        x = solver.solve(th, bb)
+        (0.5 * ((x - x_obs) ** 2).sum()).backward()
+        return th.grad.detach(), bb.grad.detach()
+
+    op, solver, theta, b, x_obs = problem(64, 1e-14)
+    gth, gb = grads(solver, theta, b, x_obs)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    gth, gb = grads(solver, theta, b, x_obs)
+    e1.record()
+    e1.synchronize()
+    grad_ms = e0.elapsed_time(e1)
+    rng = np.random.default_rng(7)
+    h = 1e-6
+    ad, fd = [], []
+    with torch.no_grad():
+        x0 = solver.solve(theta, b)
+
+        def perturbed(sign, vt, vb):
+            x = x0.clone()
+            vals = op.values(torch.exp(theta + sign * h * vt))
+            solver.sched.iccg(op.device_csr(vals), b + sign * h * vb, x, tol=1e-12, maxiter=20000,
+                              precision=PREC_FP32_FACTORS)
+            return x
+
+        for _ in range(32):
+            vt = torch.from_numpy(rng.standard_normal(theta.numel())).cuda()
+            vb = torch.from_numpy(rng.standard_normal(b.numel())).cuda()
+            vt /= vt.norm()
+            vb /= vb.norm()
+            xp, xm = perturbed(1.0, vt, vb), perturbed(-1.0, vt, vb)
+            fd.append(float(0.5 * ((xp - xm) * (xp + xm - 2.0 * x_obs)).sum() / (2 * h)))
+            ad.append(float((gth * vt).sum() + (gb * vb).sum()))
+    ad, fd = np.array(ad), np.array(fd)
+    out = {"workload": "adjoint_iccg_vardiff3d_64_fp32_factors", "n": op.n,
+           "forward_plus_adjoint_ms": round(grad_ms, 3),
+           "fd_rel_err_32_directions": float(np.linalg.norm(ad - fd) / np.linalg.norm(ad)), "fd_h": h}
+    if CPU_BASELINES:
+        out["cpu_baseline"] = c5_cpu_gradient(problem, grads)
+    return out
+
+
+def c5_cpu_gradient(problem, grads):
+    """FP64 CPU gradient at 16^3: forward and adjoint solves with the reference's PCG (pcg_opt
+    structure, Scheduler P2P_RULE), then dL/dtheta_f = -kappa_f (lam_p - lam_q)(x_p - x_q) for each
+    interior face and dL/db = lam; compared with the GPU adjoint's gradients."""
+    import torch
+
+    from baas_b200 import gen
+    from oracle.oracle import Ref, ref_available
+
+    if not ref_available():
+        return None
+    cores = _host_cores()
+    op, solver, theta, b, x_obs = problem(16, 1e-12)
+    gth, gb = grads(solver, theta, b, x_obs)
+    kappa = np.exp(theta.cpu().numpy())
+    A = gen.CSR(op.n, op.pattern.rowptr, op.pattern.colidx, op.values(torch.from_numpy(kappa).cuda()).cpu().numpy())
+    t0 = time.perf_counter()
+    x, _, _, _ = Ref.pcg(A, b.cpu().numpy(), maxiter=20000, tol=1e-14, mode=1, nthread=cores)
+    lam, _, _, _ = Ref.pcg(A, x - x_obs.cpu().numpy(), maxiter=20000, tol=1e-14, mode=1, nthread=cores)
+    rows = np.repeat(np.arange(op.n), np.diff(A.rowptr))
+    p, q = rows[op.pq], A.colidx[op.pq]
+    gth_ref = -kappa * (lam[p] - lam[q]) * (x[p] - x[q])
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    return {"value": round(cpu_ms, 3), "unit": "ms", "cores": cores, "kind": "reference",
+            "sample": "16^3 forward + adjoint FP64 solves (reference PCG) and the face-gradient formula",
+            "grad_theta_rel_err": float(np.linalg.norm(gth.cpu().numpy() - gth_ref) / np.linalg.norm(gth_ref)),
+            "grad_b_rel_err": float(np.linalg.norm(gb.cpu().numpy() - lam) / np.linalg.norm(lam))}
 
 
 def gpu_arm(args):
@@ -404,10 +695,14 @@ def gpu_arm(args):
     # the other configurations (1 GPU only: replicas would repeat them)
     extras = {}
     if world == 1 and not args.headline_only:
-        for name, fn in (("sptrsv_c1", lambda: c1_sptrsv(flush)), ("ilu0_c3", lambda: c3_ilu(flush)),
-                         ("batched_c4", c4_batched)):
+        for name, fn in (("sptrsv_c1", lambda: c1_sptrsv(flush)), ("c2_variants", lambda: c2_variants(flush)),
+                         ("ilu0_c3", lambda: c3_ilu(flush)), ("batched_c4", c4_batched), ("adjoint_c5", c5_adjoint)):
             try:
-                extras[name] = fn()
+                r = fn()
+                if name == "c2_variants":
+                    extras.update(r)
+                else:
+                    extras[name] = r
             except Exception as e:  # a failure here must not cost the headline line
                 extras[name] = {"error": f"{type(e).__name__}: {str(e)[:160]}"}
 
@@ -418,6 +713,13 @@ def gpu_arm(args):
 
     peak, peak_kind = _peaks()
     launch_bytes = IC0_BYTES + it * ITER_BYTES
+    # latency bounds: one sweep; the ICCG launch = two sweeps per preconditioner apply (it + 1
+    # applies) plus the IC0 walk, each at the sweep bound
+    sweep_lat = sweep_latency_bound(s)
+    sweep_lat["frac"] = round(sweep_lat["bound_us"] / (sweep_ms * 1e3), 4)
+    iccg_bound_ms = (2 * (it + 1) + 1) * sweep_lat["bound_us"] * 1e-3
+    iccg_lat = {"bound_ms": round(iccg_bound_ms, 3), "sweeps": 2 * (it + 1) + 1, "per_sweep_us": sweep_lat["bound_us"],
+                "frac": round(iccg_bound_ms / ms64, 4)}
     achieved = launch_bytes / (ms64 * 1e-3) / 1e9
     # DRAM bytes of one launch, from the ncu capture summarised in profiles/
     traffic = None
@@ -427,9 +729,15 @@ def gpu_arm(args):
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = int(line.split(":")[1])
     if rank == 0:
-        cpu = None
+        cpu, xref = None, None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline_sample()
+            got = cpu_baseline_sample()
+            if got is not None:
+                cpu, xref = got
+                # the reference's FP64 solution is the oracle for both GPU forms' errors
+                cpu["rel_err_vs_reference_fp64"] = {
+                    "fp64": float(np.linalg.norm(x64.cpu().numpy() - xref) / np.linalg.norm(xref)),
+                    "fp32_factors": float(np.linalg.norm(x32.cpu().numpy() - xref) / np.linalg.norm(xref))}
         clocks = clk.summary()
         line = {
             "metric": METRIC, "value": round(ms64, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -444,14 +752,17 @@ def gpu_arm(args):
             "gpu_launches": int(args.steps),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "traffic": traffic,
-                         "peak_kind": peak_kind, "kernel": "k_iccg_chunked<double>",
-                         "algorithmic_bytes_per_launch": int(launch_bytes)},
+                         "peak_kind": peak_kind, "kernel": "k_iccg_chunked<double, fetch walk>",
+                         "algorithmic_bytes_per_launch": int(launch_bytes),
+                         "latency_bound": iccg_lat},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "fp32_factors": {"ms": round(ms32, 4), "iterations": int(it32), "relres": rel32,
                              "rel_err_vs_fp64": err32},
             "sptrsv": {"ms": round(sweep_ms, 4), "bytes": SWEEP_BYTES,
-                       "gbps": round(SWEEP_BYTES / (sweep_ms * 1e-3) / 1e9, 2)},
+                       "gbps": round(SWEEP_BYTES / (sweep_ms * 1e-3) / 1e9, 2),
+                       "hbm_frac": round(SWEEP_BYTES / (sweep_ms * 1e-3) / 1e9 / peak, 5),
+                       "latency_bound": sweep_lat},
             "analysis_ms": round(analysis_ms, 2),
             "configs": extras,
             "wall_s_timed_region": round(wall, 3),
@@ -522,6 +833,17 @@ def main():
                     choices=["iccg", "iccg_fp32", "ic0", "sweep_lower", "sweep_upper", "batched_small"],
                     help="run one kernel of the workload only (for ncu captures)")
     args = ap.parse_args()
+    global CPU_BASELINES
+    CPU_BASELINES = not args.no_cpu_baseline
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch this command under torchrun (rendezvous on 127.0.0.1)
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", os.environ.get("BAAS_BENCH_PORT", "29531"),
+               str(Path(__file__).resolve())] + sys.argv[1:]
+        raise SystemExit(subprocess.call(cmd))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.gpus != world and args.impl != "reference":
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     if args.impl == "reference":
         reference_arm(args)
     elif args.profile_case:
