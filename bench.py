@@ -723,7 +723,7 @@ def gpu_arm(args):
     achieved = launch_bytes / (ms64 * 1e-3) / 1e9
     # DRAM bytes of one launch, from the ncu capture summarised in profiles/
     traffic = None
-    tp = ROOT / "profiles" / "k_iccg_chunked_laplace3d_64.md"
+    tp = ROOT / "profiles" / "k_iccg_fetch_laplace3d_64.md"
     if tp.exists():
         for line in tp.read_text().splitlines():
             if line.startswith("traffic_bytes_per_launch:"):
