@@ -202,6 +202,23 @@ struct FetchDev {
     }
 };
 
+// Level-walk plan (staged.cuh level_walk): the whole schedule as one partition, per direction.
+struct LevelHostDir {
+    std::vector<int> lev, item, row, eptr, dep, src, dsrc, srcT, dsrcT;
+};
+struct LevelDevDir {
+    int *lev = nullptr, *item = nullptr, *row = nullptr, *eptr = nullptr, *dep = nullptr, *src = nullptr,
+        *dsrc = nullptr, *srcT = nullptr, *dsrcT = nullptr;
+    int nlev = 0, nent = 0, npos = 0;
+    baas::LevelDir view() const { return baas::LevelDir{lev, item, row, eptr, dep, src, dsrc, srcT, dsrcT, nlev, nent, npos}; }
+    void release() {
+        int *ptrs[] = {lev, item, row, eptr, dep, src, dsrc, srcT, dsrcT};
+        for (int *p : ptrs)
+            if (p) cudaFree(p);
+        *this = LevelDevDir();
+    }
+};
+
 baas_status upload_fetch(FetchDev &d, const FetchHost &h) {
     for (int k = 0; k < 2; k++) {
         const FetchHostDir &H = h.dir[k];
@@ -264,6 +281,10 @@ struct baas_schedule {
     double *d_gfT[2] = {nullptr, nullptr};   // record values of the caller's factor (sweeps)
     int last_walk = 0;                       // walk of the last sweep / ICCG launch (BAAS_WALK_*)
     double *d_dg = nullptr;                  // fetch-walk IC0: each row's diagonal (its ready flag)
+    LevelDevDir d_lv[2];                     // level-walk plan, per direction
+    double *d_lv64[2] = {nullptr, nullptr}, *d_ld64[2] = {nullptr, nullptr};  // its values (ICCG, FP64)
+    float *d_lv32[2] = {nullptr, nullptr}, *d_ld32[2] = {nullptr, nullptr};   // (ICCG, FP32 factors)
+    double *d_lvT[2] = {nullptr, nullptr}, *d_ldT[2] = {nullptr, nullptr};    // (caller's factor, sweeps)
     std::map<int, WinCfg> wins;  // key: value bytes * 16 + right-hand sides
     int smem_budget = 0;
     int rmax64 = 1;  // most FP64 right-hand sides one sweep walks together
@@ -808,6 +829,75 @@ void build_fetch(baas_schedule *s) {
     if (!F.ok) F = FetchHost();
 }
 
+// Level-walk plan of one direction: levels in execution order (descending for U = L^T), the
+// groups of a level in LevelSet order (reversed for U), a group's rows ascending (descending for
+// U); each row's entries in the reference's order -- L: off-diagonals ascending, diagonal last;
+// U = L^T: diagonal first, off-diagonals descending -- with the row each reads and the value's
+// position in A (through the lower triangle's source map) and in the caller's triangular CSR.
+void build_level_dir(const baas_schedule *s, bool upper, LevelHostDir &D) {
+    const baas::HostSchedule &h = s->hs;
+    const int nl = (int)h.exec_level_ptr.size() - 1;
+    D = LevelHostDir();
+    D.lev.assign(1, 0);
+    D.item.assign(1, 0);
+    D.eptr.assign(1, 0);
+    for (int li = 0; li < nl; li++) {
+        const int l = upper ? nl - 1 - li : li;
+        const int qb = h.exec_level_ptr[l], qe = h.exec_level_ptr[l + 1];
+        for (int qi = 0; qi < qe - qb; qi++) {
+            const int g = h.perm_to_orig[upper ? qe - 1 - qi : qb + qi];
+            const int rb = h.group_ptr[g], re = h.group_ptr[g + 1];
+            for (int k = 0; k < re - rb; k++) {
+                const int r = h.group_set[upper ? re - 1 - k : rb + k];
+                D.row.push_back(r);
+                if (!upper) {
+                    const int lb = h.l_rowptr[r], le = h.l_rowptr[r + 1];
+                    for (int e = lb; e < le - 1; e++) {
+                        D.dep.push_back(h.l_colidx[e]);
+                        D.src.push_back(h.l_src[e]);
+                        D.srcT.push_back(e);
+                    }
+                    D.dsrc.push_back(h.l_src[le - 1]);
+                    D.dsrcT.push_back(le - 1);
+                } else {
+                    const int cb = s->cptr[r], ce = s->cptr[r + 1];
+                    for (int e = ce - 1; e > cb; e--) {
+                        D.dep.push_back(s->crow[e]);
+                        D.src.push_back(h.l_src[s->cpos[e]]);
+                        D.srcT.push_back(e);
+                    }
+                    D.dsrc.push_back(h.l_src[s->cpos[cb]]);
+                    D.dsrcT.push_back(cb);
+                }
+                D.eptr.push_back((int)D.dep.size());
+            }
+            D.item.push_back((int)D.row.size());
+        }
+        D.lev.push_back((int)D.item.size() - 1);
+    }
+}
+
+baas_status upload_level(baas_schedule *s) {
+    for (int d = 0; d < 2; d++) {
+        LevelHostDir H;
+        build_level_dir(s, d == 1, H);
+        LevelDevDir &D = s->d_lv[d];
+        BAAS_TRY(upload(D.lev, H.lev));
+        BAAS_TRY(upload(D.item, H.item));
+        BAAS_TRY(upload(D.row, H.row));
+        BAAS_TRY(upload(D.eptr, H.eptr));
+        BAAS_TRY(upload(D.dep, H.dep));
+        BAAS_TRY(upload(D.src, H.src));
+        BAAS_TRY(upload(D.dsrc, H.dsrc));
+        BAAS_TRY(upload(D.srcT, H.srcT));
+        BAAS_TRY(upload(D.dsrcT, H.dsrcT));
+        D.nlev = (int)H.lev.size() - 1;
+        D.nent = (int)H.dep.size();
+        D.npos = (int)H.row.size();
+    }
+    return BAAS_OK;
+}
+
 // Shared bytes of a fetch-walk launch: ICCG (both directions' int blocks resident; values: FP64
 // one direction at a time, FP32 both) or a standalone sweep (one direction).
 size_t fetch_smem(const FetchHost &F, int vbytes, bool iccg) {
@@ -984,14 +1074,28 @@ void build_plans(baas_schedule *s, int P, int num_sms) {
     }
 }
 
-// Whether a launch takes the fetch walk (values of vbytes bytes; ICCG or a standalone sweep of
-// one right-hand side). BAAS_WALK_FETCH turns a plan that does not qualify into an error.
-baas_status pick_walk(const baas_schedule *s, int vbytes, bool iccg, bool &fw) {
+// Most group levels for which AUTO takes the level walk: one grid barrier (~2 us) per level and
+// direction then costs less than the chunked walk's per-row waits between CTAs on such wide,
+// unstructured levels.
+constexpr int kLevelWalkMaxLevels = 64;
+
+// The walk of a launch (values of vbytes bytes; ICCG, or a standalone sweep of one right-hand
+// side): FETCH where the fetch plan qualifies and fits shared memory, else LEVELS for shallow
+// group DAGs, else CHUNKED. An explicitly requested walk that cannot run is an error.
+baas_status pick_walk(const baas_schedule *s, int vbytes, bool iccg, int &walk) {
     const bool fits = s->fch.ok && fetch_smem(s->fch, vbytes, iccg) <= (size_t)kMaxDynSmem;
-    if (s->opt.walk == BAAS_WALK_FETCH && !fits)
-        return fail(BAAS_ERR_BAD_ARG, "the fetch walk needs rows of at most 3 off-diagonal entries, steps of at most " +
-                                          std::to_string(baas::kFetchMaxRows) + " rows and a plan that fits shared memory");
-    fw = fits && s->opt.walk != BAAS_WALK_CHUNKED;
+    const int nlev = (int)s->hs.exec_level_ptr.size() - 1;
+    switch (s->opt.walk) {
+        case BAAS_WALK_FETCH:
+            if (!fits)
+                return fail(BAAS_ERR_BAD_ARG, "the fetch walk needs rows of at most 3 off-diagonal entries, steps of at most " +
+                                                  std::to_string(baas::kFetchMaxRows) + " rows and a plan that fits shared memory");
+            walk = BAAS_WALK_FETCH;
+            break;
+        case BAAS_WALK_CHUNKED: walk = BAAS_WALK_CHUNKED; break;
+        case BAAS_WALK_LEVELS: walk = BAAS_WALK_LEVELS; break;
+        default: walk = fits ? BAAS_WALK_FETCH : (nlev <= kLevelWalkMaxLevels ? BAAS_WALK_LEVELS : BAAS_WALK_CHUNKED);
+    }
     return BAAS_OK;
 }
 
@@ -1004,16 +1108,20 @@ void *sweep_kernel(bool mr, bool stg, bool ieee) {
     return mr ? (stg ? (void *)baas::k_sweep_chunked<true, true, false> : (void *)baas::k_sweep_chunked<true, false, false>)
               : (stg ? (void *)baas::k_sweep_chunked<false, true, false> : (void *)baas::k_sweep_chunked<false, false, false>);
 }
-void *iccg_kernel(bool mixed, bool stg, bool ieee, bool fw = false) {
-    if (fw) {
-        if (mixed) return (void *)baas::k_iccg_chunked<float, false, false, true>;
-        return ieee ? (void *)baas::k_iccg_chunked<double, false, true, true> : (void *)baas::k_iccg_chunked<double, false, false, true>;
+// walk: BAAS_WALK_CHUNKED, BAAS_WALK_FETCH or BAAS_WALK_LEVELS (the level walk divides with
+// __ddiv_rn and never needs the IEEE repeat).
+void *iccg_kernel(bool mixed, bool stg, bool ieee, int walk = BAAS_WALK_CHUNKED) {
+    using baas::k_iccg_chunked;
+    constexpr int C = baas::kWalkChunked, F = baas::kWalkFetch, L = baas::kWalkLevels;
+    if (walk == BAAS_WALK_LEVELS)
+        return mixed ? (void *)k_iccg_chunked<float, false, false, L> : (void *)k_iccg_chunked<double, false, false, L>;
+    if (walk == BAAS_WALK_FETCH) {
+        if (mixed) return (void *)k_iccg_chunked<float, false, false, F>;
+        return ieee ? (void *)k_iccg_chunked<double, false, true, F> : (void *)k_iccg_chunked<double, false, false, F>;
     }
-    if (mixed)
-        return stg ? (void *)baas::k_iccg_chunked<float, true, false, false> : (void *)baas::k_iccg_chunked<float, false, false, false>;
-    if (ieee)
-        return stg ? (void *)baas::k_iccg_chunked<double, true, true, false> : (void *)baas::k_iccg_chunked<double, false, true, false>;
-    return stg ? (void *)baas::k_iccg_chunked<double, true, false, false> : (void *)baas::k_iccg_chunked<double, false, false, false>;
+    if (mixed) return stg ? (void *)k_iccg_chunked<float, true, false, C> : (void *)k_iccg_chunked<float, false, false, C>;
+    if (ieee) return stg ? (void *)k_iccg_chunked<double, true, true, C> : (void *)k_iccg_chunked<double, false, true, C>;
+    return stg ? (void *)k_iccg_chunked<double, true, false, C> : (void *)k_iccg_chunked<double, false, false, C>;
 }
 void *sweep_fetch_kernel(bool ieee) {
     return ieee ? (void *)baas::k_sweep_fetch<true> : (void *)baas::k_sweep_fetch<false>;
@@ -1087,7 +1195,8 @@ baas_status ensure_device(baas_schedule *s) {
                                    batched_kernel(true, true, false, 4), batched_kernel(true, true, false, 2)};
             for (const void *k : kerns)
                 BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
-            const void *fk[] = {iccg_kernel(a, false, b, true), sweep_fetch_kernel(a)};
+            const void *fk[] = {iccg_kernel(a, false, b, BAAS_WALK_FETCH), sweep_fetch_kernel(a),
+                                iccg_kernel(a, false, b, BAAS_WALK_LEVELS)};
             for (const void *k : fk)
                 BAAS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
         }
@@ -1221,7 +1330,7 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     if (o.parts < 0) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 0");
     if (o.smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
-    if (o.walk < BAAS_WALK_AUTO || o.walk > BAAS_WALK_FETCH) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
+    if (o.walk < BAAS_WALK_AUTO || o.walk > BAAS_WALK_LEVELS) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
     if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_AFFINITY)
         return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
     if (o.mapping != BAAS_MAPPING_FOUR_RULE && kind != BAAS_KERNEL_ICCG)
@@ -1642,6 +1751,12 @@ static void release_device(baas_schedule *s) {
         }
         if (s->d_dg) cudaFree(s->d_dg);
         for (int d = 0; d < 2; d++) {
+            s->d_lv[d].release();
+            void *lp[] = {s->d_lv64[d], s->d_ld64[d], s->d_lv32[d], s->d_ld32[d], s->d_lvT[d], s->d_ldT[d]};
+            for (void *p : lp)
+                if (p) cudaFree(p);
+        }
+        for (int d = 0; d < 2; d++) {
             if (s->d_gv64[d]) cudaFree(s->d_gv64[d]);
             if (s->d_gv32[d]) cudaFree(s->d_gv32[d]);
             if (s->d_gvT[d]) cudaFree(s->d_gvT[d]);
@@ -1686,7 +1801,7 @@ baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
     if (opt->nthread != s->hs.nthread) return fail(BAAS_ERR_BAD_ARG, "nthread is fixed by the analysis");
     if (opt->mapping != s->opt.mapping) return fail(BAAS_ERR_BAD_ARG, "mapping is fixed by the analysis");
     if (opt->parts < 0 || opt->smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "parts and smem_budget must be >= 0");
-    if (opt->walk < BAAS_WALK_AUTO || opt->walk > BAAS_WALK_FETCH) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
+    if (opt->walk < BAAS_WALK_AUTO || opt->walk > BAAS_WALK_LEVELS) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
     if (opt->partition == BAAS_PARTITION_CUSTOM) {
         if (s->custom_part.empty()) return fail(BAAS_ERR_BAD_ARG, "no custom partition: use baas_replan_custom");
         if (opt->parts != s->opt.parts) return fail(BAAS_ERR_BAD_ARG, "a custom partition fixes parts");
@@ -1724,8 +1839,26 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
     BAAS_TRY(ensure_device(s));
     cudaStream_t stream = (cudaStream_t)stream_;
     const int d = upper ? 1 : 0;
-    bool fw = false;
-    if (nrhs == 1) BAAS_TRY(pick_walk(s, 8, false, fw));
+    int walk = BAAS_WALK_CHUNKED;
+    if (nrhs == 1) BAAS_TRY(pick_walk(s, 8, false, walk));
+    if (walk == BAAS_WALK_LEVELS) {
+        if (!s->d_lv[0].lev) BAAS_TRY(upload_level(s));
+        if (!s->d_lvT[d]) {
+            BAAS_TRY(dalloc(s->d_lvT[d], (size_t)s->d_lv[d].nent));
+            BAAS_TRY(dalloc(s->d_ldT[d], (size_t)s->d_lv[d].npos));
+        }
+        baas::LevelDir D = s->d_lv[d].view();
+        unsigned int spin = s->spin();
+        double *v = s->d_lvT[d], *dd = s->d_ldT[d];
+        void *args[] = {(void *)&D, (void *)&T->values, (void *)&v, (void *)&dd, (void *)&b, (void *)&x,
+                        (void *)&s->d_bar, (void *)&s->d_status, (void *)&spin};
+        s->last_walk = BAAS_WALK_LEVELS;
+        BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+        BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
+        BAAS_CUDA(cudaLaunchCooperativeKernel((void *)baas::k_sweep_levels, s->P, baas::kStageBlock, args, 0, stream));
+        return read_status(s, stream);
+    }
+    const bool fw = walk == BAAS_WALK_FETCH;
     if (fw) {
         if (!s->d_gfT[d]) BAAS_TRY(dalloc(s->d_gfT[d], (size_t)baas::kFetchVal64 * n));
         baas::FetchPlan fp = fetch_plan(s, 8, false);
@@ -1748,7 +1881,8 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
         return fail(BAAS_ERR_CUDA, "IEEE sweep reported a fast-path division");
     }
     s->last_walk = BAAS_WALK_CHUNKED;
-    if (s->opt.walk == BAAS_WALK_FETCH) return fail(BAAS_ERR_BAD_ARG, "the fetch walk takes one right-hand side");
+    if (s->opt.walk == BAAS_WALK_FETCH || s->opt.walk == BAAS_WALK_LEVELS)
+        return fail(BAAS_ERR_BAD_ARG, "the fetch and level walks take one right-hand side");
     // right-hand sides walked together: as many as the solution slots leave room for
     const int R = std::min(nrhs, s->rmax64);
     WinCfg *w = nullptr;
@@ -2059,8 +2193,18 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
         s->ws_ready = true;
     }
     const bool mixed = precision == BAAS_PREC_FP32_FACTORS;
-    bool fw = false;
-    BAAS_TRY(pick_walk(s, mixed ? 4 : 8, true, fw));
+    int walk = BAAS_WALK_CHUNKED;
+    BAAS_TRY(pick_walk(s, mixed ? 4 : 8, true, walk));
+    const bool fw = walk == BAAS_WALK_FETCH, lw = walk == BAAS_WALK_LEVELS;
+    if (lw && !s->d_lv[0].lev) BAAS_TRY(upload_level(s));
+    if (lw && !s->d_lv64[0]) {
+        for (int d = 0; d < 2; d++) {
+            BAAS_TRY(dalloc(s->d_lv64[d], (size_t)s->d_lv[d].nent));
+            BAAS_TRY(dalloc(s->d_ld64[d], (size_t)s->d_lv[d].npos));
+            BAAS_TRY(dalloc(s->d_lv32[d], (size_t)s->d_lv[d].nent));
+            BAAS_TRY(dalloc(s->d_ld32[d], (size_t)s->d_lv[d].npos));
+        }
+    }
     if (fw && !s->d_gf64[0]) {
         for (int d = 0; d < 2; d++) {
             BAAS_TRY(dalloc(s->d_gf64[d], (size_t)baas::kFetchVal64 * n));
@@ -2120,7 +2264,17 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
         a.fac_fetch = s->fwd.mpair.empty() ? 1 : 0;
         a.dg = s->d_dg;
     }
-    s->last_walk = fw ? BAAS_WALK_FETCH : BAAS_WALK_CHUNKED;
+    if (lw) {
+        for (int d = 0; d < 2; d++) {
+            a.lv[d] = s->d_lv[d].view();
+            a.lv64[d] = s->d_lv64[d];
+            a.ld64[d] = s->d_ld64[d];
+            a.lv32[d] = s->d_lv32[d];
+            a.ld32[d] = s->d_ld32[d];
+        }
+        smem = 0;
+    }
+    s->last_walk = walk;
     void *args[] = {(void *)&a};
     const bool stg = w->rhs_bytes > 0;
     int it = 0;
@@ -2132,8 +2286,8 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
         a.epoch = s->epoch;
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
         BAAS_CUDA(cudaMemsetAsync(s->d_bar, 0, sizeof(unsigned int), stream));
-        BAAS_CUDA(cudaLaunchCooperativeKernel(iccg_kernel(mixed, fw ? false : stg, ieee != 0, fw), P, baas::kStageBlock, args,
-                                              smem, stream));
+        BAAS_CUDA(cudaLaunchCooperativeKernel(iccg_kernel(mixed, (fw || lw) ? false : stg, ieee != 0, walk), P,
+                                              baas::kStageBlock, args, smem, stream));
         BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));
         BAAS_CUDA(cudaMemcpyAsync(&rr, s->d_relres, sizeof(double), cudaMemcpyDeviceToHost, stream));
         dump_trace(s, "iccg", stream);

@@ -39,6 +39,8 @@ namespace baas {
 // every step barrier; and the pipelined walk gets up to 255 registers.
 constexpr int kStageBlock = 256;
 static_assert(kStageBlock == kFetchBlock, "the fetch walk runs in the chunked kernels' CTAs");
+// walks of the persistent ICCG kernel
+constexpr int kWalkChunked = 0, kWalkFetch = 1, kWalkLevels = 2;
 constexpr int kChunkHdr = 4;
 constexpr int kIssuer = kStageBlock - 32;  // lane 0 of the last warp issues the bulk copies
 constexpr int kMaxRhs = 8;                 // right-hand sides walked together
@@ -791,6 +793,93 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_chunked(ChunkPlan pl, 
 // the chunk value slots, and the pcg_opt loop (test/iccg_level_merge.cpp:380-533, break at
 // tol) in one cooperative launch of P CTAs.
 // ---------------------------------------------------------------------------------------
+// ---------------------------------------------------------------------------------------
+// Level walk: for shallow group DAGs (a few dozen levels, each thousands of groups wide: an
+// unstructured or randomly permuted pattern), where per-row waits between CTAs would cost more
+// than one grid barrier per level. Every thread of the launch takes groups of the current level
+// in turn (grid stride) and solves their rows in order, reading the rows of earlier levels from
+// L2; a grid barrier ends the level (its fences publish the level's results). Entries are summed
+// in the plan's order with the same correctly rounded operations as the other walks (the FP64
+// quotient by __ddiv_rn, which the chunked walk's div_fast reproduces), so results are
+// bit-identical to theirs.
+// ---------------------------------------------------------------------------------------
+struct LevelDir {
+    const int *lev;    // nlev + 1: items (groups) of each level, in execution order
+    const int *item;   // nitem + 1: positions (rows) of each item
+    const int *row;    // position -> row
+    const int *eptr;   // position -> its entries
+    const int *dep;    // entry -> the row it reads
+    const int *src;    // entry -> A position (factor values)
+    const int *dsrc;   // position -> the diagonal's A position
+    const int *srcT;   // entry -> position in the caller's triangular CSR
+    const int *dsrcT;  // position -> the diagonal's position there
+    int nlev, nent, npos;
+};
+
+// Packs a direction's values (grid stride): v[e] per entry, d[pos] per row (FP64: the diagonal;
+// FP32: 1/diag, as the other FP32 walks store it).
+template <typename T>
+__device__ __forceinline__ void level_pack(const LevelDir &D, const int *src, const int *dsrc, const double *vals,
+                                           T *v, T *d, int gt, int W) {
+    for (int e = gt; e < D.nent; e += W) v[e] = (T)Sent<double>::load(vals + __ldg(src + e));
+    for (int p = gt; p < D.npos; p += W) {
+        const double dv = Sent<double>::load(vals + __ldg(dsrc + p));
+        if constexpr (sizeof(T) == 4)
+            d[p] = __frcp_rn(__double2float_rn(dv));
+        else
+            d[p] = dv;
+    }
+}
+
+// One direction: out[row] = (rhs[row] - sum_e v[e] out[dep[e]]) / d[pos], level by level. False
+// (uniformly) if a grid barrier gave up.
+template <typename T, typename RT>
+__device__ __forceinline__ bool level_walk(const LevelDir &D, const T *v, const T *d, const RT *rhs, T *out,
+                                           unsigned int *bar, unsigned int &nb, DevStatus *st, unsigned int limit) {
+    const int W = gridDim.x * blockDim.x;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int l = 0; l < D.nlev; l++) {
+        const int ib = __ldg(D.lev + l), ie = __ldg(D.lev + l + 1);
+        for (int it = ib + gt; it < ie; it += W) {
+            for (int p = __ldg(D.item + it), pe = __ldg(D.item + it + 1); p < pe; p++) {
+                const int row = __ldg(D.row + p);
+                T sum = T(0);
+                // eight entries' loads in flight at once (dependency rows, then their values),
+                // then their products summed in entry order
+                for (int e0 = __ldg(D.eptr + p), ee = __ldg(D.eptr + p + 1); e0 < ee; e0 += 8) {
+                    int dr[8];
+                    T vv[8], xv[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const bool in = e0 + u < ee;
+                        dr[u] = in ? __ldg(D.dep + e0 + u) : row;
+                        vv[u] = in ? __ldg(v + e0 + u) : T(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) xv[u] = __ldcg(out + dr[u]);
+#pragma unroll
+                    for (int u = 0; u < 8; u++)
+                        if (e0 + u < ee) {
+                            if constexpr (sizeof(T) == 8)
+                                sum = __dadd_rn(sum, __dmul_rn(xv[u], vv[u]));
+                            else
+                                sum = fmaf(xv[u], vv[u], sum);
+                        }
+                }
+                const T r = (T)__ldcg(rhs + row);
+                T o;
+                if constexpr (sizeof(T) == 8)
+                    o = __ddiv_rn(__dsub_rn(r, sum), __ldg(d + p));
+                else
+                    o = (r - sum) * __ldg(d + p);
+                __stcg(out + row, o);
+            }
+        }
+        if (!grid_barrier(bar, nb, st, limit)) return false;
+    }
+    return true;
+}
+
 struct IccgArgs {
     int n;
     const int *a_rowptr, *a_colidx, *a_diag;
@@ -818,6 +907,9 @@ struct IccgArgs {
     int reuse;         // 1: the value slots already hold the factors (adjoint solves)
     const double *xf;  // with grad_a: the forward solution x
     double *grad_a;    // if set: grad_a[e] = -x_i * xf_j for each entry e = (i, j) of A
+    LevelDir lv[2];     // level-walk plan per direction (kernels instantiated with the level walk)
+    double *lv64[2], *ld64[2];  // its packed values and diagonals, FP64 factors
+    float *lv32[2], *ld32[2];   // the same, FP32 factors (1/diag)
     FetchPlan fp;      // fetch-walk plan (kernels instantiated with FW)
     double *gf64[2];   // fetch-walk record values per direction, FP64 factors
     float *gf32[2];    // the same, FP32 factors
@@ -894,6 +986,32 @@ __device__ __forceinline__ bool chunk_precond(const IccgArgs &A, WinStream<T> &w
         const double zd = STG ? (double)rs[k] : (double)Sent<T>::load(zg + row);
         rz = __dadd_rn(rz, __dmul_rn(A.r[row], zd));
         if (set_p) A.p[row] = zd;
+    }
+    trace_mark(A.trace, 59);
+    return true;
+}
+
+// Level-walk preconditioner: z = U^-1 L^-1 r by the level walk (lower into y, upper into z, both
+// in global memory), p = z if set_p, and this thread's share of r.z (grid stride). nb: the
+// caller's grid-barrier count. False (uniformly) if a barrier gave up.
+template <typename T>
+__device__ __forceinline__ bool level_precond(const IccgArgs &A, bool set_p, double &rz, unsigned int &nb) {
+    constexpr bool kMixed = sizeof(T) == 4;
+    T *yg = kMixed ? (T *)A.y32 : (T *)A.y;
+    T *zg = kMixed ? (T *)A.z32 : (T *)A.z;
+    const T *v0 = kMixed ? (const T *)A.lv32[0] : (const T *)A.lv64[0];
+    const T *d0 = kMixed ? (const T *)A.ld32[0] : (const T *)A.ld64[0];
+    const T *v1 = kMixed ? (const T *)A.lv32[1] : (const T *)A.lv64[1];
+    const T *d1 = kMixed ? (const T *)A.ld32[1] : (const T *)A.ld64[1];
+    trace_mark(A.trace, 56);
+    if (!level_walk<T, double>(A.lv[0], v0, d0, A.r, yg, A.bar, nb, A.st, A.spin_limit)) return false;
+    if (!level_walk<T, T>(A.lv[1], v1, d1, yg, zg, A.bar, nb, A.st, A.spin_limit)) return false;
+    trace_mark(A.trace, 57);
+    const int W = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += W) {
+        const double zd = (double)__ldcg(zg + i);
+        rz = __dadd_rn(rz, __dmul_rn(A.r[i], zd));
+        if (set_p) A.p[i] = zd;
     }
     trace_mark(A.trace, 59);
     return true;
@@ -1051,8 +1169,9 @@ __device__ __forceinline__ void pack_factor(const ChunkDir &D, const double *lu,
 // staged in shared memory (when they fit). One instantiation per combination keeps each one's
 // register budget to what it uses. IEEE (FP64 factors only): sweep divisions by __ddiv_rn, for the
 // repeat of a launch whose div_fast divisions left their range.
-template <typename T, bool STG, bool IEEE, bool FW>
+template <typename T, bool STG, bool IEEE, int WK>
 __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
+    constexpr bool FW = WK == kWalkFetch, LW = WK == kWalkLevels;
     constexpr bool kMixed = sizeof(T) == 4;
     constexpr int kLanes = kMixed ? 1 : 4;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -1077,7 +1196,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
         __syncthreads();
         if (threadIdx.x == 0) fetch_issue_ints(A.fp, F, true, 0);
         fetch_stage_lists(A.fp, F);
-    } else {
+    } else if constexpr (!LW) {
         ws.init(A.pl, 0, true, kMixed ? (const T *)A.gv32[0] : (const T *)A.gv64[0],
                 kMixed ? (const T *)A.gv32[1] : (const T *)A.gv64[1], smem, 0xFFFFFFFFu);
     }
@@ -1089,7 +1208,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
                 if (vpend >= 0) mbar_wait(&F.ctl->mbar_vals, (unsigned int)vpend, A.spin_limit);
             }
             __syncthreads();
-        } else {
+        } else if constexpr (!LW) {
             ws.drain(A.spin_limit);
         }
     };
@@ -1162,6 +1281,10 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
         if constexpr (FW) {
             for (int d = 0; d < 2; d++)
                 fetch_pack<T>(A.fp.dir[d], A.fp.dir[d].code, A.lu, kMixed ? (T *)A.gf32[d] : (T *)A.gf64[d]);
+        } else if constexpr (LW) {
+            for (int d = 0; d < 2; d++)
+                level_pack<T>(A.lv[d], A.lv[d].src, A.lv[d].dsrc, A.lu, kMixed ? (T *)A.lv32[d] : (T *)A.lv64[d],
+                              kMixed ? (T *)A.ld32[d] : (T *)A.ld64[d], gt, W);
         } else {
             pack_factor<T>(A.pl.dir[0], A.lu, A.gv64[0], A.gv32[0]);
             pack_factor<T>(A.pl.dir[1], A.lu, A.gv64[1], A.gv32[1]);
@@ -1213,7 +1336,15 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
         ints_pending = false;
         if (kMixed && threadIdx.x == 0) vpend = -1;
     }
-    if (!(FW ? fetch_precond<T, IEEE>(A, F, true, rzl, vpend) : chunk_precond<T, STG, IEEE>(A, ws, smem, true, rzl, w))) {
+    auto precond = [&](bool set_p, double &rzp) -> bool {
+        if constexpr (FW)
+            return fetch_precond<T, IEEE>(A, F, set_p, rzp, vpend);
+        else if constexpr (LW)
+            return level_precond<T>(A, set_p, rzp, nb);
+        else
+            return chunk_precond<T, STG, IEEE>(A, ws, smem, set_p, rzp, w);
+    };
+    if (!precond(true, rzl)) {
         drain();
         return;
     }
@@ -1278,7 +1409,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
         if (rel < A.tol) break;
 
         rzl = 0.0;
-        if (!(FW ? fetch_precond<T, IEEE>(A, F, false, rzl, vpend) : chunk_precond<T, STG, IEEE>(A, ws, smem, false, rzl, w))) {
+        if (!precond(false, rzl)) {
             drain();
             return;
         }
@@ -1377,6 +1508,18 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_fetch(FetchPlan fp, in
     if (!IEEE && slow) st->slow_div = 1;
     __syncthreads();
     trace_mark(trace, 2);
+}
+
+// Standalone sweep of the caller's triangular CSR by the level walk: one right-hand side,
+// values packed from tval into v/d here; bar must be 0 on entry.
+__global__ void __launch_bounds__(kStageBlock, 1) k_sweep_levels(LevelDir D, const double *__restrict__ tval, double *v,
+                                                                double *d, const double *b, double *x, unsigned int *bar,
+                                                                DevStatus *st, unsigned int spin) {
+    unsigned int nb = 0;
+    const int W = gridDim.x * blockDim.x, gt = blockIdx.x * blockDim.x + threadIdx.x;
+    level_pack<double>(D, D.srcT, D.dsrcT, tval, v, d, gt, W);
+    if (!grid_barrier(bar, nb, st, spin)) return;
+    level_walk<double, double>(D, v, d, b, x, bar, nb, st, spin);
 }
 
 }  // namespace baas

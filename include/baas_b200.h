@@ -111,16 +111,20 @@ typedef struct baas_options {
                          window buffers (0 = library default, 220 KiB; at most 224 KiB) */
     int mapping;      /* BAAS_MAPPING_FOUR_RULE (default) or, for BAAS_KERNEL_ICCG, one of the
                          Scheduler's other mappings; fixed by the analysis */
-    int walk;         /* BAAS_WALK_AUTO (default) or BAAS_WALK_CHUNKED: which triangular-sweep
-                         kernel the single-right-hand-side sweeps and ICCG use */
+    int walk;         /* BAAS_WALK_AUTO (default), BAAS_WALK_CHUNKED, BAAS_WALK_FETCH or
+                         BAAS_WALK_LEVELS: which triangular-sweep kernel the single-right-hand-side
+                         sweeps and ICCG use */
 } baas_options;
 
 /* Triangular-sweep kernels. CHUNKED: the plan streamed through shared memory in windows, any row
  * width, up to 8 right-hand sides walked together. FETCH: rows of at most 3 off-diagonal entries
  * (stencil matrices) and one right-hand side; the compute warps read every dependency from shared
- * memory while the CTA's last warp brings other CTAs' results in. AUTO: FETCH wherever the plan
- * qualifies and fits shared memory, else CHUNKED. Results are bit-identical between the two. */
-enum { BAAS_WALK_AUTO = 0, BAAS_WALK_CHUNKED = 1, BAAS_WALK_FETCH = 2 };
+ * memory while the CTA's last warp brings other CTAs' results in. LEVELS: one right-hand side;
+ * every thread of the launch takes groups of a level and a grid barrier ends the level -- for
+ * shallow group DAGs (unstructured or permuted patterns: a few dozen wide levels). AUTO: FETCH
+ * wherever the plan qualifies and fits shared memory, else LEVELS when the DAG has at most 64
+ * group levels, else CHUNKED. Sweeps and factors are bit-identical between the walks. */
+enum { BAAS_WALK_AUTO = 0, BAAS_WALK_CHUNKED = 1, BAAS_WALK_FETCH = 2, BAAS_WALK_LEVELS = 3 };
 
 /* How the analysis maps groups to the reference's virtual threads (Schedule::ALG_SCHEDULE,
  * test/Schedule.hpp:31-37, 263-281). FOUR_RULE: P2P_RULE, the BAAS four-rule mapping
