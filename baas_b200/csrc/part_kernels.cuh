@@ -81,40 +81,35 @@ __device__ __forceinline__ double ldv(const double *p) {
 }
 
 // IC0 row i (merge/IC.cpp:296-393; sparse_dot_product :6-29), correctly rounded FP64.
-template <bool LOCAL>
-__device__ __forceinline__ double ic0_dot(int l1, int u1, int l2, int u2, const int *__restrict__ colidx, const double *lu) {
-    double dp = 0.0;
-    while (l1 < u1 && l2 < u2) {
-        const int c1 = __ldg(colidx + l1), c2 = __ldg(colidx + l2);
-        if (c1 == c2) {
-            dp = __dadd_rn(dp, __dmul_rn(lu[l1], ldv<LOCAL>(lu + l2)));
-            l1++;
-            l2++;
-        } else if (c1 < c2) {
-            l1++;
-        } else {
-            l2++;
-        }
-    }
-    return dp;
-}
-
+// Rows wider than the register path: the same operations, with each entry's dot product taken
+// from the host-built column-match pairs (the merge's matches, in its order) instead of a merge
+// over column indices, and eight pairs' loads in flight at once.
 __device__ __forceinline__ bool ic0_row_part(const PartView &pv, int pos, int i, const int *__restrict__ rowptr,
                                              const int *__restrict__ colidx, const int *__restrict__ diagptr, double *lu,
                                              const int *gflag, int epoch, Waiter &w, DevStatus *st) {
+    constexpr int B = 8;
     const int rb = __ldg(rowptr + i), di = __ldg(diagptr + i), e0 = __ldg(pv.eptr + pos);
     for (int k = rb; k < di; k++) {
-        const int j = __ldg(colidx + k);
-        const int d = __ldg(pv.dep + e0 + (k - rb));
-        const int l2 = __ldg(rowptr + j), u2 = __ldg(diagptr + j);
-        double dp, ljj;
-        if (d < 0) {
-            dp = ic0_dot<true>(rb, di, l2, u2, colidx, lu);
-            ljj = ldv<true>(lu + u2);
-        } else {
-            if (!wait_flag(gflag + j, epoch, w, i)) return false;
-            dp = ic0_dot<false>(rb, di, l2, u2, colidx, lu);
-            ljj = ldv<false>(lu + u2);
+        const int t = k - rb;
+        const int d = __ldg(pv.dep + e0 + t);
+        const bool loc = d < 0;
+        if (!loc && !wait_flag(gflag + __ldg(colidx + k), epoch, w, i)) return false;
+        const int pj = __ldg(pv.epiv + e0 + t);
+        const double ljj = loc ? ldv<true>(lu + pj) : ldv<false>(lu + pj);
+        double dp = 0.0;
+        for (int m0 = __ldg(pv.mptr + e0 + t), m1 = __ldg(pv.mptr + e0 + t + 1); m0 < m1; m0 += B) {
+            int2 pr[B];
+            double av[B], bv[B];
+#pragma unroll
+            for (int u = 0; u < B; u++) pr[u] = m0 + u < m1 ? __ldg(pv.mpair + m0 + u) : make_int2(0, -1);
+#pragma unroll
+            for (int u = 0; u < B; u++) {
+                av[u] = pr[u].y < 0 ? 0.0 : lu[rb + pr[u].x];
+                bv[u] = pr[u].y < 0 ? 0.0 : (loc ? ldv<true>(lu + pr[u].y) : ldv<false>(lu + pr[u].y));
+            }
+#pragma unroll
+            for (int u = 0; u < B; u++)
+                if (m0 + u < m1) dp = __dadd_rn(dp, __dmul_rn(av[u], bv[u]));
         }
         lu[k] = __ddiv_rn(__dsub_rn(lu[k], dp), ljj);
     }

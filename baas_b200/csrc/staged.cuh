@@ -841,6 +841,16 @@ __device__ __forceinline__ bool level_walk(const LevelDir &D, const T *v, const 
     for (int l = 0; l < D.nlev; l++) {
         const int ib = __ldg(D.lev + l), ie = __ldg(D.lev + l + 1);
         for (int it = ib + gt; it < ie; it += W) {
+            // the group's last kWin results stay in registers: a row that reads one of them (the
+            // rows of a coarsened group form chains) takes it from there, not from L2
+            constexpr int kWin = 4;
+            int wr[kWin];
+            T wv[kWin];
+#pragma unroll
+            for (int k = 0; k < kWin; k++) {
+                wr[k] = -1;
+                wv[k] = T(0);
+            }
             for (int p = __ldg(D.item + it), pe = __ldg(D.item + it + 1); p < pe; p++) {
                 const int row = __ldg(D.row + p);
                 T sum = T(0);
@@ -856,7 +866,18 @@ __device__ __forceinline__ bool level_walk(const LevelDir &D, const T *v, const 
                         vv[u] = in ? __ldg(v + e0 + u) : T(0);
                     }
 #pragma unroll
-                    for (int u = 0; u < 8; u++) xv[u] = __ldcg(out + dr[u]);
+                    for (int u = 0; u < 8; u++) {
+                        bool hit = false;
+                        T hv = T(0);
+#pragma unroll
+                        for (int k = 0; k < kWin; k++)
+                            if (dr[u] == wr[k]) {
+                                hit = true;
+                                hv = wv[k];
+                            }
+                        xv[u] = hv;
+                        if (!hit) xv[u] = __ldcg(out + dr[u]);
+                    }
 #pragma unroll
                     for (int u = 0; u < 8; u++)
                         if (e0 + u < ee) {
@@ -873,6 +894,13 @@ __device__ __forceinline__ bool level_walk(const LevelDir &D, const T *v, const 
                 else
                     o = (r - sum) * __ldg(d + p);
                 __stcg(out + row, o);
+#pragma unroll
+                for (int k = kWin - 1; k > 0; k--) {
+                    wr[k] = wr[k - 1];
+                    wv[k] = wv[k - 1];
+                }
+                wr[0] = row;
+                wv[0] = o;
             }
         }
         if (!grid_barrier(bar, nb, st, limit)) return false;
