@@ -56,11 +56,19 @@ def build_lib(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+def reference_tree():
+    """The reference's source tree: $BAAS_REFERENCE, else a `reference` directory beside this
+    repository; None when neither exists (the reference-built checker is then skipped)."""
+    cand = os.environ.get("BAAS_REFERENCE") or str(ROOT.parent / "reference")
+    return Path(cand) if Path(cand).is_dir() else None
+
+
 def build_oracle(verbose: bool = False) -> None:
     mk = ["make", "-s", "-C", str(ROOT / "oracle")]
     subprocess.run(mk + ["oracle"], check=True)
-    if Path(os.environ.get("BAAS_REFERENCE", "/root/reference")).is_dir():
-        subprocess.run(mk + ["ref", f"REF={os.environ.get('BAAS_REFERENCE', '/root/reference')}"], check=True)
+    ref = reference_tree()
+    if ref is not None:
+        subprocess.run(mk + ["ref", f"REF={ref}"], check=True)
 
 
 if __name__ == "__main__":

@@ -105,15 +105,15 @@ baas_csr host_pattern(const CSR *A) {
 }  // namespace detail
 
 // Schedule::Scheduler (test/Schedule.hpp:39-353): owns the BAAS schedule of A's lower triangle
-// and runs IC0 and the two sweeps. isSymmetric must be true (the IC0 / ICCG schedule), as in the
-// reference's ICCG driver (test/iccg_level_merge.cpp); isTRSVPerm = false only (the
-// thread-contiguous permuted variant is not built).
+// and runs IC0 and the two sweeps. isSymmetric = false builds the same schedule without the
+// backward one, as the reference's preprocessing does (test/Schedule.hpp:289-292): IC0 and the
+// forward sweep run, and a backward sweep throws (the reference has no schedule for it then).
+// isTRSVPerm = false only (the thread-contiguous permuted variant is not built).
 template <typename CSR>
 class Scheduler {
    public:
     Scheduler(const CSR *csrA, bool isSymmetric, bool isTRSVPerm, ALG_SCHEDULE alg, int num_thread)
-        : csrA_(csrA), num_thread_(num_thread) {
-        if (!isSymmetric) throw std::runtime_error("Scheduler: only the symmetric (IC0/ICCG) schedule is built");
+        : csrA_(csrA), num_thread_(num_thread), symmetric_(isSymmetric) {
         if (isTRSVPerm) throw std::runtime_error("Scheduler: the permuted (isTRSVPerm) variant is not built");
         mapping_ = alg == P2P           ? BAAS_MAPPING_COST_SPLIT
                    : alg == P2P_TIME    ? BAAS_MAPPING_FINISH_TIME
@@ -145,7 +145,10 @@ class Scheduler {
     // x = L^-1 b, L lower with the diagonal last in each row.
     void runForwardTRSVNoPerm(const CSR *L, double *x, const double *b) { sweep(L, x, b, 0); }
     // x = U^-1 b, U = L^T upper with the diagonal first in each row.
-    void runBackwardTRSVNoPerm(const CSR *U, double *x, const double *b) { sweep(U, x, b, 1); }
+    void runBackwardTRSVNoPerm(const CSR *U, double *x, const double *b) {
+        if (!symmetric_) throw std::runtime_error("Scheduler: built with isSymmetric = false, so it has no backward schedule");
+        sweep(U, x, b, 1);
+    }
     void runForwardTRSV(const CSR *L, double *x, const double *b, bool isPerm) {
         if (isPerm) throw std::runtime_error("Scheduler: the permuted variant is not built");
         runForwardTRSVNoPerm(L, x, b);
@@ -171,6 +174,7 @@ class Scheduler {
     }
     const CSR *csrA_;
     int num_thread_;
+    bool symmetric_;
     int mapping_ = BAAS_MAPPING_FOUR_RULE;
     baas_schedule *s_ = nullptr;
     detail::DevCsr dA_, dL_, dU_;

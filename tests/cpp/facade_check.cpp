@@ -140,6 +140,16 @@ int main(int argc, char **argv) {
     sch.runBackwardTRSVNoPerm(&U, z.data(), y.data());
     orc_upper_solve_desc(n, U.rowptr, U.colidx, U.values, yw.data(), zw.data());
     if (std::memcmp(z.data(), zw.data(), sizeof(double) * n) != 0) return fail("runBackwardTRSVNoPerm");
+    // isSymmetric = false: the forward schedule only (test/Schedule.hpp:289-292)
+    baas_b200::Scheduler<CSR> fwd_only(&A, false, false, baas_b200::P2P_RULE, 8);
+    std::vector<double> y2(n);
+    fwd_only.runForwardTRSVNoPerm(&L, y2.data(), b.data());
+    if (std::memcmp(y2.data(), yw.data(), sizeof(double) * n) != 0) return fail("forward sweep (isSymmetric = false)");
+    try {
+        fwd_only.runBackwardTRSVNoPerm(&U, z.data(), y.data());
+        return fail("backward sweep without a backward schedule accepted");
+    } catch (const std::runtime_error &) {
+    }
 
     // runtime classes
     std::vector<double> xtrue(n);

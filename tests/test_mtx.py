@@ -3,6 +3,7 @@ error handling, and -- where the reference tree is present -- against the refere
 (SPM::CSR(fileName), spm/CSR.cpp:90-112) on the two real SPD stiffness matrices it ships
 (data/bcsstk18.mtx, data/bcsstk38.mtx), followed by the BAAS schedule, IC0 and the plan's sweeps
 on them, each bit for bit against the reference or the oracle."""
+import os
 from pathlib import Path
 
 import numpy as np
@@ -11,7 +12,8 @@ import pytest
 from baas_b200 import KERNEL_ICCG, BaasError, Schedule, gen
 from oracle.oracle import Port
 
-REF_DATA = Path("/root/reference/data")
+# the reference's shipped fixtures: $BAAS_REFERENCE/data, else beside this repository
+REF_DATA = Path(os.environ.get("BAAS_REFERENCE") or Path(__file__).resolve().parents[2] / "reference") / "data"
 
 
 def _same(a, b):
