@@ -582,6 +582,29 @@ def c5_cpu_gradient(problem, grads):
             "grad_b_rel_err": float(np.linalg.norm(gb.cpu().numpy() - lam) / np.linalg.norm(lam))}
 
 
+def c4_sharded(rank, world, dev):
+    """Configuration 4 split across the ranks by whole systems (baas_b200.distributed): each rank
+    solves its share in one batched launch, with no communication during the solve, then one
+    gather of every system's iterations, residuals and solution to rank 0. The time is the max
+    over ranks of their launch times (CUDA events); total work is fixed, so the scaling is strong."""
+    from baas_b200 import PREC_FP32_FACTORS, gen
+    from baas_b200.distributed import batched_solve, solve_sharded
+
+    systems = gen.batch_vardiff2d()
+    rhs = lambda q: gen.uniform_rhs(systems[q].n, 1000 + q, nrhs=4)  # noqa: E731
+    got = solve_sharded(systems, lambda idx: batched_solve(systems, idx, rhs, device=dev, tol=TOL,
+                                                           precision=PREC_FP32_FACTORS), rank, world)
+    if got is None:
+        return None
+    times = got.pop(-1)
+    it = np.array([got[q]["iterations"] for q in range(len(systems))])
+    rel = np.array([got[q]["relres"] for q in range(len(systems))])
+    return {"workload": "batched_vardiff2d_64sys_k64-512_4rhs_sharded", "ranks": world, "scaling": "strong",
+            "ms_fp32_factors": round(max(times.values()), 3),
+            "ms_per_rank": {int(r): round(t, 3) for r, t in sorted(times.items())},
+            "iterations": {"min": int(it.min()), "max": int(it.max())}, "max_relres": float(rel.max())}
+
+
 def gpu_arm(args):
     import torch
 
@@ -705,6 +728,15 @@ def gpu_arm(args):
                     extras[name] = r
             except Exception as e:  # a failure here must not cost the headline line
                 extras[name] = {"error": f"{type(e).__name__}: {str(e)[:160]}"}
+
+    if world > 1 and not args.headline_only:
+        # the configuration that shards: the batch split by whole systems (every rank takes part)
+        try:
+            r = c4_sharded(rank, world, dev)
+            if r is not None:
+                extras["batched_c4_sharded"] = r
+        except Exception as e:
+            extras["batched_c4_sharded"] = {"error": f"{type(e).__name__}: {str(e)[:160]}"}
 
     vals = torch.tensor([ms64, e2e_ms, ms32], dtype=torch.float64, device=dev)
     if world > 1:

@@ -102,3 +102,25 @@ def test_row_wide_sweeps_match_pair_sweeps(monkeypatch, nrhs):
     assert np.array_equal(out[0][0].view(np.int64), out[1][0].view(np.int64))
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
     assert np.all(out[1][2] < 1e-10)
+
+
+def test_rank_share_of_a_batch_matches_the_oracle():
+    """baas_b200.distributed.batched_solve (one rank's share of a batch split across GPUs) on one
+    GPU: every system of the share solved to tol, solutions within 1e-9 of the oracle's FP64 PCG
+    (FP32 factors) and the split a partition of the batch."""
+    from baas_b200.distributed import batched_solve, split_systems
+    from oracle.oracle import Port
+
+    systems = gen.batch_vardiff2d(nsys=6, kmin=16, kmax=40, seed=9)
+    parts = split_systems([S.n for S in systems], 2)
+    rhs = lambda q: gen.uniform_rhs(systems[q].n, 500 + q, nrhs=2)  # noqa: E731
+    for idx in parts:
+        got = batched_solve(systems, idx, rhs, tol=1e-10, precision=1)
+        assert got[-1] > 0.0
+        for q in idx:
+            B = rhs(q)
+            for r in range(2):
+                xo, _, _ = Port.pcg(systems[q], B[r], tol=1e-10)
+                x = got[q]["x"][r]
+                assert got[q]["relres"][r] < 1e-10
+                assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-9
