@@ -1272,6 +1272,7 @@ bool csr_ok(const baas_csr *m, int n, int nnz) {
 // ---------------------------------------------------------------------------------------
 constexpr int kNoAllocMaxRows = 1 << 21;  // 2,097,152 rows
 constexpr int kNoAllocStatusInts = 4;     // a DevStatus at the front
+static_assert(sizeof(DevStatus) <= kNoAllocStatusInts * sizeof(int), "the status word must fit in front of the row flags");
 static __device__ __align__(256) int g_noalloc_scratch[kNoAllocStatusInts + kNoAllocMaxRows];
 
 constexpr int kMaxDevices = 64;

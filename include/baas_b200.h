@@ -285,7 +285,8 @@ baas_status baas_ic0(baas_schedule *s, const baas_csr *A, double *lu, void *stre
  *  - The schedule's device plan must already be resident: make one ordinary GPU call on the
  *    schedule (e.g. baas_ic0) during set-up; otherwise this returns BAAS_ERR_STATE.
  *  - Its first call on a device looks up that device's address of the static array (with the
- *    device current); make that first call before any stream capture.
+ *    device current) and keeps it for the process; after a device reset (cudaDeviceReset) or a
+ *    rebuilt primary context that address is stale, so do not call it again after one.
  *  - All calls share the one array (it keeps the last call's contents; each call clears what
  *    must start at zero): calls that overlap on the GPU -- on two streams, or on two schedules
  *    at once -- race and must not be issued.

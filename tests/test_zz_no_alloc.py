@@ -24,10 +24,16 @@ def test_ic0_noalloc_matches_ic0_on_two_calls_in_a_row():
     ref = dA.values.clone()
     s.ic0(dA, ref)  # ordinary entry point; also makes the schedule's device plan resident
     want = ref.cpu().numpy()
-    for _ in range(2):
-        lu = dA.values.clone()
+    lus = [dA.values.clone() for _ in range(3)]
+    s.ic0_noalloc(dA, lus[0])  # a first call (it looks the static array's address up)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for lu in lus[1:]:  # two calls in a row
         s.ic0_noalloc(dA, lu)
         torch.cuda.synchronize()
+        # the property the entry point exists for: the device's free memory does not move
+        assert torch.cuda.mem_get_info()[0] == free0
+    for lu in lus:
         # same tolerance as the other IC0 tests: the factors are bit-identical
         assert np.array_equal(lu.cpu().numpy(), want)
 
