@@ -21,14 +21,15 @@ from . import _native
 from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, MAPPING_COST_SPLIT,
                       MAPPING_AFFINITY, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_FOUR_RULE, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
                       PARTITION_RANGES, PARTITION_BLOCKS, PARTITION_AUTO, WALK_AUTO, WALK_CHUNKED, WALK_FETCH, WALK_LEVELS,
-                      PREC_FP32_FACTORS, PREC_FP64, BaasError)
+                      ANALYSIS_HOST, ANALYSIS_DEVICE, PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
 
 __all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV",
            "KERNEL_ICCG", "KERNEL_IC0", "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "PARTITION_RANGES",
            "PARTITION_BAAS_THREADS", "PARTITION_CUSTOM", "MAPPING_FOUR_RULE", "MAPPING_COST_SPLIT",
            "MAPPING_COST_SPLIT_BARRIER", "MAPPING_FINISH_TIME", "MAPPING_AFFINITY", "WALK_AUTO", "WALK_CHUNKED",
-           "WALK_FETCH", "WALK_LEVELS", "PARTITION_BLOCKS", "PARTITION_AUTO", "version"]
+           "WALK_FETCH", "WALK_LEVELS", "PARTITION_BLOCKS", "PARTITION_AUTO", "ANALYSIS_HOST", "ANALYSIS_DEVICE",
+           "version"]
 
 
 def version() -> str:
@@ -82,7 +83,7 @@ class Schedule:
 
     def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
                  parts: int = 0, partition: int = PARTITION_AUTO, smem_budget: int = 0, mapping: int = 0,
-                 walk: int = 0):
+                 walk: int = 0, analysis: int = ANALYSIS_HOST):
         L = _native.lib()
         self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
         self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
@@ -96,6 +97,7 @@ class Schedule:
         opt.smem_budget = smem_budget
         opt.mapping = mapping
         opt.walk = walk
+        opt.analysis = analysis
         h = C.c_void_p()
         _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
         self._h = h
@@ -117,7 +119,7 @@ class Schedule:
     # ---- schedule export (host only) ----
     def export(self, field: str) -> np.ndarray:
         L = _native.lib()
-        fid = _native.FIELDS[field]
+        fid = _native.FIELDS[field] if field in _native.FIELDS else _native.GROUP_DAG_FIELDS[field]
         n = L.baas_schedule_export(self._h, fid, None)
         if n < 0:
             raise KeyError(field)
@@ -283,7 +285,8 @@ def batch_concat(systems) -> tuple[CSR, np.ndarray]:
 class BatchSchedule(Schedule):
     """One ICCG schedule for a batch of independent SPD systems (block-diagonal concatenation)."""
 
-    def __init__(self, systems, nthread: int = 8, spin_limit: int = 0, parts: int = 0, smem_budget: int = 0):
+    def __init__(self, systems, nthread: int = 8, spin_limit: int = 0, parts: int = 0, smem_budget: int = 0,
+                 analysis: int = ANALYSIS_HOST):
         A, off = batch_concat(systems)
         self.combined = A
         self.sys_off = off
@@ -297,6 +300,7 @@ class BatchSchedule(Schedule):
         opt.spin_limit = spin_limit
         opt.parts = parts
         opt.smem_budget = smem_budget
+        opt.analysis = analysis
         h = C.c_void_p()
         _native.check(L.baas_analyze_batch(C.byref(c), _ptr(off), self.nsys, C.byref(opt), C.byref(h)),
                       "baas_analyze_batch")

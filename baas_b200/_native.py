@@ -27,6 +27,7 @@ KERNEL_SPTRSV, KERNEL_ICCG, KERNEL_IC0, KERNEL_ILU0 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32_FACTORS = 0, 1
 PARTITION_RANGES, PARTITION_BAAS_THREADS, PARTITION_CUSTOM, PARTITION_BLOCKS, PARTITION_AUTO = 0, 1, 2, 3, 4
 WALK_AUTO, WALK_CHUNKED, WALK_FETCH, WALK_LEVELS = 0, 1, 2, 3
+ANALYSIS_HOST, ANALYSIS_DEVICE = 0, 1
 MAPPING_FOUR_RULE, MAPPING_COST_SPLIT, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_AFFINITY = 0, 1, 2, 3, 4
 
 FIELDS = {
@@ -35,6 +36,9 @@ FIELDS = {
     "task_boundaries": 10, "thread_cont_to_orig": 11, "orig_to_thread_cont": 12, "task_ptr": 13,
     "task_set": 14, "btask_ptr": 15, "btask_set": 16, "cost": 17,
 }
+# the final group DAG (CSC, each group's column: its children and itself, ascending): not one of
+# the reference's exported arrays, but what the device plans are built from
+GROUP_DAG_FIELDS = {"group_dag_ptr": 18, "group_dag_set": 19}
 
 # every symbol include/baas_b200.h declares
 EXPORTS = [
@@ -52,7 +56,8 @@ class BaasCsr(C.Structure):
 
 class BaasOptions(C.Structure):
     _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("parts", C.c_int),
-                ("partition", C.c_int), ("smem_budget", C.c_int), ("mapping", C.c_int), ("walk", C.c_int)]
+                ("partition", C.c_int), ("smem_budget", C.c_int), ("mapping", C.c_int), ("walk", C.c_int),
+                ("analysis", C.c_int)]
 
 
 class BaasError(RuntimeError):

@@ -1305,6 +1305,7 @@ void baas_options_default(baas_options *opt) {
     opt->smem_budget = 0;
     opt->mapping = BAAS_MAPPING_FOUR_RULE;
     opt->walk = BAAS_WALK_AUTO;
+    opt->analysis = BAAS_ANALYSIS_HOST;
 }
 
 const char *baas_last_error_string(void) { return g_err.c_str(); }
@@ -1334,6 +1335,8 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     if (o.walk < BAAS_WALK_AUTO || o.walk > BAAS_WALK_LEVELS) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
     if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_AFFINITY)
         return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
+    if (o.analysis != BAAS_ANALYSIS_HOST && o.analysis != BAAS_ANALYSIS_DEVICE)
+        return fail(BAAS_ERR_BAD_ARG, "unknown analysis placement");
     if (o.mapping != BAAS_MAPPING_FOUR_RULE && kind != BAAS_KERNEL_ICCG)
         return fail(BAAS_ERR_BAD_ARG, "the P2P, barrier, P2P_TIME and P2P_MAPPING mappings are the Scheduler's (kind BAAS_KERNEL_ICCG)");
     if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
@@ -1346,9 +1349,20 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     baas_schedule *s = new baas_schedule();
     s->opt = o;
     s->nnz_a = A->nnz;
-    if (!baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping)) {
+    const bool dev = o.analysis == BAAS_ANALYSIS_DEVICE;
+    if (dev) {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+            cudaGetLastError();
+            delete s;
+            return fail(BAAS_ERR_NO_DEVICE, "BAAS_ANALYSIS_DEVICE needs a CUDA device");
+        }
+    }
+    std::string reason;
+    if (!baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping, dev,
+                              reason)) {
         delete s;
-        return fail(BAAS_ERR_BAD_ARG, "the P2P_MAPPING scan left a group on a thread that does not execute");
+        return fail(dev && reason.rfind("device analysis", 0) == 0 ? BAAS_ERR_CUDA : BAAS_ERR_BAD_ARG, reason);
     }
     s->nnz_l = (int)s->hs.l_colidx.size();
     if (sk != baas::SchedKind::SpTRSV && s->nnz_a != 2 * s->nnz_l - A->n) {
@@ -1389,6 +1403,8 @@ int baas_schedule_export(const baas_schedule *s, int field, int *out) {
         case BAAS_FIELD_TASK_SET: return put(h.task_set);
         case BAAS_FIELD_BTASK_PTR: return put(h.btask_ptr);
         case BAAS_FIELD_BTASK_SET: return put(h.btask_set);
+        case BAAS_FIELD_GROUP_DAG_PTR: return put(h.fdag_ptr);
+        case BAAS_FIELD_GROUP_DAG_SET: return put(h.fdag_set);
         case BAAS_FIELD_COST: {
             std::vector<int> c(h.cost.size());
             for (size_t i = 0; i < c.size(); i++) c[i] = (int)h.cost[i];

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdint>
 #include <limits>
+#include <memory>
 #include <numeric>
 #include <unordered_set>
 
@@ -110,9 +111,12 @@ void relabel_groups(int n, Grouping &g, bool by_max) {
 
 // Stages 3 and 5: BFS tree coarsening. `reverse` grows groups from sinks towards parents that
 // have exactly one child; otherwise from sources towards children that have exactly one parent.
-Grouping tree_coarsen(const Csx &dag, bool reverse) {
+// `inv_pre`: dag's transpose when the caller has it already (the device stages make it).
+Grouping tree_coarsen(const Csx &dag, bool reverse, const Csx *inv_pre = nullptr) {
     const int n = dag.n();
-    const Csx inv = transpose(dag);
+    Csx inv_own;
+    if (!inv_pre) inv_own = transpose(dag);
+    const Csx &inv = inv_pre ? *inv_pre : inv_own;
     const Csx &up = reverse ? inv : dag;    // where the next tree members come from
     const Csx &down = reverse ? dag : inv;  // whose length decides "single edge" (self + 1)
 
@@ -944,7 +948,7 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
 }
 
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
-                    Mapping mapping) {
+                    Mapping mapping, bool device, std::string &why) {
     auto t0 = std::chrono::steady_clock::now();
     // BAAS_ANALYSIS_TRACE=1: stage times of the analysis on stderr
     const bool trace = getenv("BAAS_ANALYSIS_TRACE") && atoi(getenv("BAAS_ANALYSIS_TRACE")) > 0;
@@ -979,16 +983,61 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
             s.l_colidx[s.l_rowptr[i] + e - rowptr[i]] = colidx[e];
             s.l_src[s.l_rowptr[i] + e - rowptr[i]] = e;
         }
-    Csx lower{s.l_rowptr, s.l_colidx};
-    Csx dag0 = transpose(lower);  // column j: j itself, then the rows that depend on j
-    stage("lower triangle + CSC");
-
-    Csx dag = two_hop_reduce(dag0);                   // stage 2
-    stage("two-hop reduction");
-    Grouping rev = tree_coarsen(dag, true);           // stage 3
-    Csx gdag = group_dag(n, rev, dag);                // stage 4
-    Grouping fwd = tree_coarsen(gdag, false);         // stage 5
-    stage("tree coarsening + group DAGs");
+    // With `device`, the transposes, the two-hop reduction, the group DAGs and the level sets run
+    // on the GPU (DeviceStages), the DAGs staying resident there between the stages; the BFS
+    // coarsenings, the mappings and the task DAGs run here on the host in both cases.
+    std::unique_ptr<DeviceStages> D;
+    DeviceStages::Graph dL, d0, dd, dinv, dg, dginv, df, dfcsr;
+    auto dev_failed = [&]() {
+        why = D->err;
+        return false;
+    };
+    Csx dag, gdag, fdag, dag_csr;
+    Grouping rev, fwd;
+    if (device) {
+        D.reset(new DeviceStages());
+        dL = D->upload(s.l_rowptr, s.l_colidx);
+        d0 = D->transpose(dL);  // column j: j itself, then the rows that depend on j
+        D->release(dL);
+        stage("lower triangle + CSC (device)");
+        dd = D->two_hop(d0);  // stage 2
+        D->release(d0);
+        dinv = D->transpose(dd);
+        Csx inv;
+        D->download(dd, dag.ptr, dag.idx);
+        D->download(dinv, inv.ptr, inv.idx);
+        D->release(dinv);
+        if (!D->ok()) return dev_failed();
+        stage("two-hop reduction + inverse (device)");
+        rev = tree_coarsen(dag, true, &inv);  // stage 3
+        stage("reverse-tree coarsening (host)");
+        dg = D->group_dag(dd, rev.ptr, rev.set);  // stage 4
+        D->release(dd);
+        dginv = D->transpose(dg);
+        Csx ginv;
+        D->download(dg, gdag.ptr, gdag.idx);
+        D->download(dginv, ginv.ptr, ginv.idx);
+        D->release(dginv);
+        if (!D->ok()) return dev_failed();
+        stage("group DAG + inverse (device)");
+        fwd = tree_coarsen(gdag, false, &ginv);  // stage 5
+        stage("forward-tree coarsening (host)");
+        df = D->group_dag(dg, fwd.ptr, fwd.set);
+        D->release(dg);
+        D->download(df, fdag.ptr, fdag.idx);
+        if (!D->ok()) return dev_failed();
+        stage("group DAG of the forward groups (device)");
+    } else {
+        Csx lower{s.l_rowptr, s.l_colidx};
+        Csx dag0 = transpose(lower);  // column j: j itself, then the rows that depend on j
+        stage("lower triangle + CSC");
+        dag = two_hop_reduce(dag0);  // stage 2
+        stage("two-hop reduction");
+        rev = tree_coarsen(dag, true);      // stage 3
+        gdag = group_dag(n, rev, dag);      // stage 4
+        fwd = tree_coarsen(gdag, false);    // stage 5
+        stage("tree coarsening + group DAGs");
+    }
     // remap forward groups (of reverse groups) onto rows (merge/Coarsen.cpp:896-928)
     s.ngroups = fwd.ngroups;
     s.group_ptr.assign(1, 0);
@@ -1002,7 +1051,7 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         }
         s.group_ptr.push_back((int)s.group_set.size());
     }
-    Csx fdag = group_dag(rev.ngroups, fwd, gdag);
+    if (!device) fdag = group_dag(rev.ngroups, fwd, gdag);
 
     // Stage 6: cost = rows' lower-triangle lengths summed over the group (merge/Coarsen.cpp:854-891)
     s.cost.assign(s.ngroups, 0.0);
@@ -1013,22 +1062,39 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         }
 
     stage("remap + group DAG + cost");
-    level_sets(fdag, s);  // stage 7
-    stage("level sets");
+    if (device) {  // stage 7 on the device; the dependency-order DAG for the mapping with it
+        s.nlevels = D->levels(df, s.node_to_level, s.perm_to_orig, s.level_ptr);
+        dfcsr = D->transpose(df);
+        D->download(dfcsr, dag_csr.ptr, dag_csr.idx);
+        D->release(df);
+        D->release(dfcsr);
+        if (!D->ok()) return dev_failed();
+        s.exec_level_ptr = s.level_ptr;
+        s.perm.assign(s.ngroups, 0);
+        for (int i = 0; i < s.ngroups; i++) s.perm[s.perm_to_orig[i]] = i;
+        D.reset();
+        stage("level sets + inverse DAG (device)");
+    } else {
+        level_sets(fdag, s);  // stage 7
+        stage("level sets");
+    }
     if (mapping == Mapping::FourRule || mapping == Mapping::FinishTime || mapping == Mapping::Affinity)
         threads_per_level(s);  // stage 8
     else
         merge_levels_group(s);
     for (int g = 0; g < s.ngroups; g++)  // test/Schedule.hpp:72-79
         std::sort(s.group_set.begin() + s.group_ptr[g], s.group_set.begin() + s.group_ptr[g + 1]);
-    Csx dag_csr = transpose(fdag);  // parents of each group, then the group itself
+    if (!device) dag_csr = transpose(fdag);  // parents of each group, then the group itself
     stage("threads per level + group sort + inverse DAG");
     if (mapping == Mapping::FourRule)
         four_rule_map(s, dag_csr);  // stage 9
     else if (mapping == Mapping::FinishTime)
         finish_time_map(s, dag_csr);
     else if (mapping == Mapping::Affinity) {
-        if (!affinity_map(s, dag_csr)) return false;
+        if (!affinity_map(s, dag_csr)) {
+            why = "the P2P_MAPPING scan left a group on a thread that does not execute";
+            return false;
+        }
     }
     else
         cost_split_map(s, mapping == Mapping::CostSplitBarrier);

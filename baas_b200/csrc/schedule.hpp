@@ -16,6 +16,7 @@
 // must run with OMP threads == nthread; see stage 9).
 #pragma once
 
+#include <string>
 #include <vector>
 
 namespace baas {
@@ -64,9 +65,51 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
 // P2P_MAPPING, parent-thread affinity scores with load rebalancing.
 enum class Mapping { FourRule = 0, CostSplit = 1, CostSplitBarrier = 2, FinishTime = 3, Affinity = 4 };
 
-// Runs stages 1-10. `rowptr`/`colidx` are host arrays of the analysed matrix. False when the
-// affinity mapping would leave a group unmapped (the reference's P2P_MAPPING scan can).
+// The data-parallel integer stages on the current CUDA device (analysis.cu): transposes, the
+// two-hop reduction (stage 2), the group DAGs (stage 4 and the one after stage 5) and the level
+// sets (stage 7). Patterns stay resident on the device between stages; every output equals the
+// host stage's. After a CUDA error every call is a no-op and `err` holds the reason.
+class DeviceStages {
+public:
+    struct Graph {  // square pattern on the device: n rows (or columns), m entries
+        int n = 0, m = 0;
+        int *ptr = nullptr, *idx = nullptr;
+    };
+    DeviceStages();
+    ~DeviceStages();
+    DeviceStages(const DeviceStages &) = delete;
+    DeviceStages &operator=(const DeviceStages &) = delete;
+    bool ok() const { return err.empty(); }
+    std::string err;
+
+    Graph upload(const std::vector<int> &ptr, const std::vector<int> &idx);
+    bool download(const Graph &g, std::vector<int> &ptr, std::vector<int> &idx);
+    Graph transpose(const Graph &g);  // each output row's entries ascending
+    Graph two_hop(const Graph &dag);   // CSC DAG, each column's own node first
+    // DAG between the groups (gptr, gset) of dag's nodes: every entry of every member mapped to
+    // its group, sorted and unique per group
+    Graph group_dag(const Graph &dag, const std::vector<int> &gptr, const std::vector<int> &gset);
+    // Kahn levels (1-based per node), nodes ascending inside each level; returns the level count
+    int levels(const Graph &dag, std::vector<int> &node_to_level, std::vector<int> &perm_to_orig,
+               std::vector<int> &level_ptr);
+    void release(Graph &g);
+
+private:
+    struct Impl;
+    Impl *impl_;
+    bool fail(const char *what);
+    bool check(const char *what);
+    void *alloc(size_t bytes);
+    void release(void *p);
+    void *scratch(size_t bytes);
+    bool scan(int *cnt, int *ptr, int n);
+};
+
+// Runs stages 1-10. `rowptr`/`colidx` are host arrays of the analysed matrix. With `device`, the
+// stages DeviceStages covers run on the current CUDA device; the schedule is the same. False with
+// `why` set when the affinity mapping would leave a group unmapped (the reference's P2P_MAPPING
+// scan can) or a device stage failed.
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
-                    Mapping mapping = Mapping::FourRule);
+                    Mapping mapping, bool device, std::string &why);
 
 }  // namespace baas

@@ -1122,7 +1122,7 @@ template <typename T, bool IEEE>
 __device__ __forceinline__ bool fetch_precond(const IccgArgs &A, const FetchSh &F, bool set_p, double &rz, int &vpend) {
     constexpr unsigned int S = sizeof(T);
     const FetchPlan &fp = A.fp;
-    const int tid = (int)threadIdx.x, c = blockIdx.x;
+    const int tid = (int)threadIdx.x;
     T *yg = sizeof(T) == 8 ? (T *)A.y : (T *)A.y32;
     T *zg = sizeof(T) == 8 ? (T *)A.z : (T *)A.z32;
     for (int k = tid; k < F.nrows; k += blockDim.x) Sh<T>::stu(F.SL + S * (unsigned int)k, (T)A.r[__ldg(fp.srow + F.s0 + k)]);
@@ -1495,7 +1495,7 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_fetch(FetchPlan fp, in
                                                                DevStatus *st, unsigned int spin, unsigned long long *trace) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr unsigned int S = sizeof(double);
-    const int tid = (int)threadIdx.x, c = blockIdx.x;
+    const int tid = (int)threadIdx.x;
     trace_mark(trace, 0);
     const FetchSh F = fetch_layout<double>(fp, smem, false);
     if (tid == 0) {

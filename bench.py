@@ -334,6 +334,20 @@ def c3_cpu_baseline(C, Lo, Up, B):
             "sample": f"the whole configuration (ILU0 + 8 x forward/backward p2p sweeps), mean of 2, nthread={cores}"}
 
 
+def _analysis_placements(A, s_host, host_ms):
+    """The schedule analysis with its data-parallel stages on the device (ANALYSIS_DEVICE) next to
+    the all-host analysis: the time of each (the device one after a first, module-loading run) and
+    whether every exported array and the group DAG are identical."""
+    from baas_b200 import ANALYSIS_DEVICE, KERNEL_ICCG, Schedule
+    from baas_b200._native import FIELDS, GROUP_DAG_FIELDS
+
+    Schedule(A, kind=KERNEL_ICCG, nthread=8, analysis=ANALYSIS_DEVICE)
+    sd = Schedule(A, kind=KERNEL_ICCG, nthread=8, analysis=ANALYSIS_DEVICE)
+    same = all(np.array_equal(s_host.export(f), sd.export(f)) for f in list(FIELDS) + list(GROUP_DAG_FIELDS))
+    return {"host_ms": round(host_ms, 2), "device_stages_ms": round(sd.analysis_ms, 2), "identical": bool(same),
+            "device_stages": "transposes, two-hop reduction, group DAGs, level sets"}
+
+
 def c4_batched():
     """64 variable-coefficient 2-D diffusion systems (k ~ U[64, 512]) x 4 right-hand sides, FP32
     IC0 factors, one launch; plan parameters picked by the autotuner on short trial runs."""
@@ -341,10 +355,16 @@ def c4_batched():
 
     from baas_b200 import PREC_FP32_FACTORS, PREC_FP64, BatchSchedule, DeviceCSR, autotune, gen
 
-    t0 = time.time()
     systems = gen.batch_vardiff2d()
+    t0 = time.time()
     s = BatchSchedule(systems, nthread=8)
     analysis_s = time.time() - t0
+    from baas_b200 import ANALYSIS_DEVICE
+
+    t0 = time.time()
+    sd = BatchSchedule(systems, nthread=8, analysis=ANALYSIS_DEVICE)
+    analysis_dev_s = time.time() - t0
+    del sd
     A = s.combined
     dA = DeviceCSR.from_host(A)
     B = torch.from_numpy(gen.uniform_rhs(A.n, 2, nrhs=4).reshape(4, A.n)).cuda()
@@ -392,7 +412,8 @@ def c4_batched():
            "roofline": {"bound": "hbm", "achieved": round(gbps, 2), "peak": peak, "unit": "GB/s",
                         "frac": round(gbps / peak, 5), "peak_kind": peak_kind, "kernel": "k_iccg_batched<float>",
                         "algorithmic_bytes_per_launch": int(nbytes)},
-           "autotuned": tuned["best"], "analysis_s": round(analysis_s, 2)}
+           "autotuned": tuned["best"], "analysis_s": round(analysis_s, 2),
+           "analysis_device_stages_s": round(analysis_dev_s, 2)}
     if CPU_BASELINES:
         out["cpu_baseline"] = c4_cpu_baseline(systems, B.cpu().numpy(), x32.cpu().numpy(), x64.cpu().numpy(), off)
     return out
@@ -622,6 +643,7 @@ def gpu_arm(args):
     b_h = gen.uniform_rhs(A.n, 1)
     s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
     analysis_ms = s.analysis_ms
+    analysis = _analysis_placements(A, s, analysis_ms) if rank == 0 else None
     dA = DeviceCSR.from_host(A, device=dev)
     b = torch.from_numpy(b_h).to(dev)
     x = torch.zeros_like(b)
@@ -796,6 +818,7 @@ def gpu_arm(args):
                        "hbm_frac": round(SWEEP_BYTES / (sweep_ms * 1e-3) / 1e9 / peak, 5),
                        "latency_bound": sweep_lat},
             "analysis_ms": round(analysis_ms, 2),
+            "analysis": analysis,
             "configs": extras,
             "wall_s_timed_region": round(wall, 3),
         }

@@ -79,7 +79,9 @@ typedef enum baas_field {
     BAAS_FIELD_TASK_SET = 14,          /* task DAG parents */
     BAAS_FIELD_BTASK_PTR = 15,         /* backward (inverse) task DAG ptr[ntasks+1] */
     BAAS_FIELD_BTASK_SET = 16,         /* backward parents */
-    BAAS_FIELD_COST = 17               /* Coarsen::costComputation cost[ngroups] (integer-valued) */
+    BAAS_FIELD_COST = 17,              /* Coarsen::costComputation cost[ngroups] (integer-valued) */
+    BAAS_FIELD_GROUP_DAG_PTR = 18,     /* DAG between the final groups, CSC ptr[ngroups+1] */
+    BAAS_FIELD_GROUP_DAG_SET = 19      /* each group's column: its children groups and itself, ascending */
 } baas_field;
 
 typedef enum baas_precision {
@@ -114,7 +116,18 @@ typedef struct baas_options {
     int walk;         /* BAAS_WALK_AUTO (default), BAAS_WALK_CHUNKED, BAAS_WALK_FETCH or
                          BAAS_WALK_LEVELS: which triangular-sweep kernel the single-right-hand-side
                          sweeps and ICCG use */
+    int analysis;     /* BAAS_ANALYSIS_HOST (default) or BAAS_ANALYSIS_DEVICE: where the analysis's
+                         data-parallel stages run; the schedule is identical either way */
 } baas_options;
+
+/* Where baas_analyze runs the schedule's data-parallel integer stages: the transposes of the
+ * lower triangle and of the DAGs (dcsr2csc, spm/CSR.cpp:914-950), the two-hop reduction
+ * (partialSparsification_CSC, spm/DAG.cpp:295-344), the group DAGs (merge/Coarsen.cpp:748-801)
+ * and the level sets (DAG_levelSet_CSC, spm/DAG.cpp:572-629). HOST: all on the calling thread.
+ * DEVICE: those stages on the current CUDA device (stable radix sorts, frontier rounds), the BFS
+ * coarsenings and the mappings on the host; every exported field is identical to HOST's. DEVICE
+ * without a usable device fails with BAAS_ERR_NO_DEVICE. */
+enum { BAAS_ANALYSIS_HOST = 0, BAAS_ANALYSIS_DEVICE = 1 };
 
 /* Triangular-sweep kernels. CHUNKED: the plan streamed through shared memory in windows, any row
  * width, up to 8 right-hand sides walked together. FETCH: rows of at most 3 off-diagonal entries

@@ -76,3 +76,16 @@ def test_bad_arg_on_null_and_size_mismatch():
 def test_analysis_time_reported():
     s = Schedule(gen.laplace3d(8, 1e-3), kind=KERNEL_ICCG, nthread=4)
     assert s.analysis_ms > 0.0
+
+
+def test_analysis_placement_option():
+    from baas_b200 import ANALYSIS_DEVICE, BaasError
+
+    _bad(gen.laplace2d(4), analysis=7)
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present: the device analysis runs (test_gpu_analysis.py)")
+    with pytest.raises(BaasError) as e:
+        Schedule(gen.laplace2d(4), kind=KERNEL_ICCG, nthread=2, analysis=ANALYSIS_DEVICE)
+    assert e.value.status_name == "BAAS_ERR_NO_DEVICE"
