@@ -21,7 +21,8 @@ from . import _native
 from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, MAPPING_COST_SPLIT,
                       MAPPING_AFFINITY, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_FOUR_RULE, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
                       PARTITION_RANGES, PARTITION_BLOCKS, PARTITION_AUTO, WALK_AUTO, WALK_CHUNKED, WALK_FETCH, WALK_LEVELS,
-                      ANALYSIS_HOST, ANALYSIS_DEVICE, PREC_FP32_FACTORS, PREC_FP64, BaasError)
+                      ANALYSIS_HOST, ANALYSIS_DEVICE, ABLATION_NONE, ABLATION_WOS, ABLATION_WOA, ABLATION_WOAS,
+                      PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
 
 __all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError", "CSR", "KERNEL_SPTRSV",
@@ -29,7 +30,7 @@ __all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError"
            "PARTITION_BAAS_THREADS", "PARTITION_CUSTOM", "MAPPING_FOUR_RULE", "MAPPING_COST_SPLIT",
            "MAPPING_COST_SPLIT_BARRIER", "MAPPING_FINISH_TIME", "MAPPING_AFFINITY", "WALK_AUTO", "WALK_CHUNKED",
            "WALK_FETCH", "WALK_LEVELS", "PARTITION_BLOCKS", "PARTITION_AUTO", "ANALYSIS_HOST", "ANALYSIS_DEVICE",
-           "version"]
+           "ABLATION_NONE", "ABLATION_WOS", "ABLATION_WOA", "ABLATION_WOAS", "version"]
 
 
 def version() -> str:
@@ -83,7 +84,7 @@ class Schedule:
 
     def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
                  parts: int = 0, partition: int = PARTITION_AUTO, smem_budget: int = 0, mapping: int = 0,
-                 walk: int = 0, analysis: int = ANALYSIS_HOST):
+                 walk: int = 0, analysis: int = ANALYSIS_HOST, ablation: int = ABLATION_NONE):
         L = _native.lib()
         self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
         self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
@@ -98,6 +99,7 @@ class Schedule:
         opt.mapping = mapping
         opt.walk = walk
         opt.analysis = analysis
+        opt.ablation = ablation
         h = C.c_void_p()
         _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
         self._h = h

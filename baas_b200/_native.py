@@ -28,6 +28,7 @@ PREC_FP64, PREC_FP32_FACTORS = 0, 1
 PARTITION_RANGES, PARTITION_BAAS_THREADS, PARTITION_CUSTOM, PARTITION_BLOCKS, PARTITION_AUTO = 0, 1, 2, 3, 4
 WALK_AUTO, WALK_CHUNKED, WALK_FETCH, WALK_LEVELS = 0, 1, 2, 3
 ANALYSIS_HOST, ANALYSIS_DEVICE = 0, 1
+ABLATION_NONE, ABLATION_WOS, ABLATION_WOA, ABLATION_WOAS = 0, 1, 2, 3
 MAPPING_FOUR_RULE, MAPPING_COST_SPLIT, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_AFFINITY = 0, 1, 2, 3, 4
 
 FIELDS = {
@@ -57,7 +58,7 @@ class BaasCsr(C.Structure):
 class BaasOptions(C.Structure):
     _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("parts", C.c_int),
                 ("partition", C.c_int), ("smem_budget", C.c_int), ("mapping", C.c_int), ("walk", C.c_int),
-                ("analysis", C.c_int)]
+                ("analysis", C.c_int), ("ablation", C.c_int)]
 
 
 class BaasError(RuntimeError):

@@ -1306,6 +1306,7 @@ void baas_options_default(baas_options *opt) {
     opt->mapping = BAAS_MAPPING_FOUR_RULE;
     opt->walk = BAAS_WALK_AUTO;
     opt->analysis = BAAS_ANALYSIS_HOST;
+    opt->ablation = BAAS_ABLATION_NONE;
 }
 
 const char *baas_last_error_string(void) { return g_err.c_str(); }
@@ -1337,6 +1338,10 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
     if (o.analysis != BAAS_ANALYSIS_HOST && o.analysis != BAAS_ANALYSIS_DEVICE)
         return fail(BAAS_ERR_BAD_ARG, "unknown analysis placement");
+    if (o.ablation < BAAS_ABLATION_NONE || o.ablation > BAAS_ABLATION_WOAS)
+        return fail(BAAS_ERR_BAD_ARG, "unknown ablation");
+    if (o.ablation != BAAS_ABLATION_NONE && (kind != BAAS_KERNEL_SPTRSV || o.mapping != BAAS_MAPPING_FOUR_RULE))
+        return fail(BAAS_ERR_BAD_ARG, "the ablations are the SpTRSV runtime's (kind BAAS_KERNEL_SPTRSV, mapping FOUR_RULE)");
     if (o.mapping != BAAS_MAPPING_FOUR_RULE && kind != BAAS_KERNEL_ICCG)
         return fail(BAAS_ERR_BAD_ARG, "the P2P, barrier, P2P_TIME and P2P_MAPPING mappings are the Scheduler's (kind BAAS_KERNEL_ICCG)");
     if (!A->rowptr || !A->colidx || A->n <= 0) return fail(BAAS_ERR_BAD_ARG, "empty or NULL pattern");
@@ -1359,8 +1364,8 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         }
     }
     std::string reason;
-    if (!baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping, dev,
-                              reason)) {
+    if (!baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping,
+                              (baas::Ablation)o.ablation, dev, reason)) {
         delete s;
         return fail(dev && reason.rfind("device analysis", 0) == 0 ? BAAS_ERR_CUDA : BAAS_ERR_BAD_ARG, reason);
     }
@@ -1827,7 +1832,10 @@ baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     }
     release_device(s);
+    const int analysis = s->opt.analysis, ablation = s->opt.ablation;  // fixed by the analysis
     s->opt = *opt;
+    s->opt.analysis = analysis;
+    s->opt.ablation = ablation;
     return BAAS_OK;
 }
 

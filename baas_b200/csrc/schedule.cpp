@@ -268,30 +268,13 @@ void threads_per_level(HostSchedule &s) {
     }
 }
 
-// Stages 8-9 of the cost-split mapping, the Scheduler's P2P algorithm (test/Schedule.hpp:233-240,
-// 263-265). Level merge (level_merge_group, merge/LevelMerge.cpp:372-421): threads per level by
-// level_nthreads_group (:264-294; rule :102-114: one thread below 40 rows or at most 12 groups,
-// else max(ceil(rows / 10), groups) capped by the thread count; a single level gets
-// min(groups, threads)), then consecutive single-thread levels are merged by the reference's
+// The level merge of level_merge_group / level_merge_group_TRSV (merge/LevelMerge.cpp:313-421) on
+// per-level thread counts `t`: consecutive single-thread levels are merged by the reference's
 // two-pointer scan, and the merged levels number their groups from 0 (constructLevelMerge
 // :423-452).
-void merge_levels_group(HostSchedule &s) {
-    const int nl = s.nlevels, nc = s.nthread;
+void merge_levels(HostSchedule &s, std::vector<int> t) {
+    const int nl = s.nlevels;
     const std::vector<int> lp = s.level_ptr;
-    std::vector<int> t(nl, 1);
-    if (nl == 1) {
-        t[0] = std::min(lp[1] - lp[0], nc);
-    } else {
-        for (int l = 0; l < nl; l++) {
-            const int groups = lp[l + 1] - lp[l];
-            int rows = 0;
-            for (int p = lp[l]; p < lp[l + 1]; p++) {
-                const int g = s.perm_to_orig[p];
-                rows += s.group_ptr[g + 1] - s.group_ptr[g];
-            }
-            t[l] = (rows < 40 || groups <= 12) ? 1 : std::min(std::max((rows + 9) / 10, groups), nc);
-        }
-    }
     std::vector<int> mptr(nl + 1, 0);
     int m = 0;
     for (int i = 1; i < nl;) {
@@ -311,6 +294,38 @@ void merge_levels_group(HostSchedule &s) {
     s.nthread_per_level.assign(t.begin(), t.begin() + m);
     for (int l = 0; l < m; l++)
         for (int j = s.level_ptr[l]; j < s.level_ptr[l + 1]; j++) s.node_to_level[s.perm_to_orig[j]] = l;
+}
+
+// Stages 8-9 of the cost-split mapping, the Scheduler's P2P algorithm (test/Schedule.hpp:233-240,
+// 263-265): level_merge_group (merge/LevelMerge.cpp:367-421) with threads per level by
+// level_nthreads_group (:282-311; rule :102-114: one thread below 40 rows or at most 12 groups,
+// else max(ceil(rows / 10), groups) capped by the thread count; a single level gets
+// min(groups, threads)).
+void merge_levels_group(HostSchedule &s) {
+    const int nl = s.nlevels, nc = s.nthread;
+    const std::vector<int> &lp = s.level_ptr;
+    std::vector<int> t(nl, 1);
+    if (nl == 1) {
+        t[0] = std::min(lp[1] - lp[0], nc);
+    } else {
+        for (int l = 0; l < nl; l++) {
+            const int groups = lp[l + 1] - lp[l];
+            int rows = 0;
+            for (int p = lp[l]; p < lp[l + 1]; p++) {
+                const int g = s.perm_to_orig[p];
+                rows += s.group_ptr[g + 1] - s.group_ptr[g];
+            }
+            t[l] = (rows < 40 || groups <= 12) ? 1 : std::min(std::max((rows + 9) / 10, groups), nc);
+        }
+    }
+    merge_levels(s, std::move(t));
+}
+
+// level_nthreads_base (merge/LevelMerge.cpp:265-279): as many threads as groups, at most nthread.
+void threads_per_level_base(HostSchedule &s) {
+    s.nthread_per_level.assign(s.nlevels, 1);
+    for (int l = 0; l < s.nlevels; l++)
+        s.nthread_per_level[l] = std::min(s.level_ptr[l + 1] - s.level_ptr[l], s.nthread);
 }
 
 // Task::constructTask (merge/LevelTask.cpp:42-196): each level's groups are cut into up to
@@ -948,7 +963,9 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
 }
 
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
-                    Mapping mapping, bool device, std::string &why) {
+                    Mapping mapping, Ablation ablation, bool device, std::string &why) {
+    // BAASWOA and BAASWOAS leave the rows ungrouped: one group per row on the two-hop DAG
+    const bool aggregate = ablation == Ablation::None || ablation == Ablation::WOS;
     auto t0 = std::chrono::steady_clock::now();
     // BAAS_ANALYSIS_TRACE=1: stage times of the analysis on stderr
     const bool trace = getenv("BAAS_ANALYSIS_TRACE") && atoi(getenv("BAAS_ANALYSIS_TRACE")) > 0;
@@ -992,7 +1009,7 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         why = D->err;
         return false;
     };
-    Csx dag, gdag, fdag, dag_csr;
+    Csx dag, inv, gdag, fdag, dag_csr;
     Grouping rev, fwd;
     if (device) {
         D.reset(new DeviceStages());
@@ -1003,12 +1020,18 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         dd = D->two_hop(d0);  // stage 2
         D->release(d0);
         dinv = D->transpose(dd);
-        Csx inv;
         D->download(dd, dag.ptr, dag.idx);
         D->download(dinv, inv.ptr, inv.idx);
         D->release(dinv);
         if (!D->ok()) return dev_failed();
         stage("two-hop reduction + inverse (device)");
+    }
+    if (device && !aggregate) {
+        df = dd;
+        dd = DeviceStages::Graph();
+        fdag = dag;
+        dag_csr = std::move(inv);
+    } else if (device) {
         rev = tree_coarsen(dag, true, &inv);  // stage 3
         stage("reverse-tree coarsening (host)");
         dg = D->group_dag(dd, rev.ptr, rev.set);  // stage 4
@@ -1033,25 +1056,40 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         stage("lower triangle + CSC");
         dag = two_hop_reduce(dag0);  // stage 2
         stage("two-hop reduction");
-        rev = tree_coarsen(dag, true);      // stage 3
-        gdag = group_dag(n, rev, dag);      // stage 4
-        fwd = tree_coarsen(gdag, false);    // stage 5
-        stage("tree coarsening + group DAGs");
-    }
-    // remap forward groups (of reverse groups) onto rows (merge/Coarsen.cpp:896-928)
-    s.ngroups = fwd.ngroups;
-    s.group_ptr.assign(1, 0);
-    s.group_ptr.reserve(fwd.ngroups + 1);
-    s.group_set.clear();
-    s.group_set.reserve(n);
-    for (int f = 0; f < fwd.ngroups; f++) {
-        for (int q = fwd.ptr[f]; q < fwd.ptr[f + 1]; q++) {
-            const int g = fwd.set[q];
-            s.group_set.insert(s.group_set.end(), rev.set.begin() + rev.ptr[g], rev.set.begin() + rev.ptr[g + 1]);
+        if (aggregate) {
+            rev = tree_coarsen(dag, true);    // stage 3
+            gdag = group_dag(n, rev, dag);    // stage 4
+            fwd = tree_coarsen(gdag, false);  // stage 5
+            stage("tree coarsening + group DAGs");
+        } else {
+            fdag = dag;
         }
-        s.group_ptr.push_back((int)s.group_set.size());
     }
-    if (!device) fdag = group_dag(rev.ngroups, fwd, gdag);
+    if (aggregate) {
+        // remap forward groups (of reverse groups) onto rows (merge/Coarsen.cpp:896-928)
+        s.ngroups = fwd.ngroups;
+        s.group_ptr.assign(1, 0);
+        s.group_ptr.reserve(fwd.ngroups + 1);
+        s.group_set.clear();
+        s.group_set.reserve(n);
+        for (int f = 0; f < fwd.ngroups; f++) {
+            for (int q = fwd.ptr[f]; q < fwd.ptr[f + 1]; q++) {
+                const int g = fwd.set[q];
+                s.group_set.insert(s.group_set.end(), rev.set.begin() + rev.ptr[g], rev.set.begin() + rev.ptr[g + 1]);
+            }
+            s.group_ptr.push_back((int)s.group_set.size());
+        }
+        if (!device) fdag = group_dag(rev.ngroups, fwd, gdag);
+    } else {  // one group per row (test/SpTRSVRuntime.hpp:925-932, :1148-1156)
+        s.ngroups = n;
+        s.group_ptr.resize(n + 1);
+        s.group_set.resize(n);
+        for (int i = 0; i < n; i++) {
+            s.group_ptr[i + 1] = i + 1;
+            s.group_set[i] = i;
+        }
+        s.group_ptr[0] = 0;
+    }
 
     // Stage 6: cost = rows' lower-triangle lengths summed over the group (merge/Coarsen.cpp:854-891)
     s.cost.assign(s.ngroups, 0.0);
@@ -1064,10 +1102,12 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
     stage("remap + group DAG + cost");
     if (device) {  // stage 7 on the device; the dependency-order DAG for the mapping with it
         s.nlevels = D->levels(df, s.node_to_level, s.perm_to_orig, s.level_ptr);
-        dfcsr = D->transpose(df);
-        D->download(dfcsr, dag_csr.ptr, dag_csr.idx);
+        if (aggregate) {
+            dfcsr = D->transpose(df);
+            D->download(dfcsr, dag_csr.ptr, dag_csr.idx);
+            D->release(dfcsr);
+        }
         D->release(df);
-        D->release(dfcsr);
         if (!D->ok()) return dev_failed();
         s.exec_level_ptr = s.level_ptr;
         s.perm.assign(s.ngroups, 0);
@@ -1078,15 +1118,23 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         level_sets(fdag, s);  // stage 7
         stage("level sets");
     }
-    if (mapping == Mapping::FourRule || mapping == Mapping::FinishTime || mapping == Mapping::Affinity)
+    if (ablation == Ablation::WOAS) {
+        threads_per_level_base(s);
+    } else if (ablation == Ablation::WOS) {  // level_merge_group_TRSV (merge/LevelMerge.cpp:313-365)
+        threads_per_level(s);
+        merge_levels(s, s.nthread_per_level);
+    } else if (mapping == Mapping::FourRule || mapping == Mapping::FinishTime || mapping == Mapping::Affinity) {
         threads_per_level(s);  // stage 8
-    else
+    } else {
         merge_levels_group(s);
+    }
     for (int g = 0; g < s.ngroups; g++)  // test/Schedule.hpp:72-79
         std::sort(s.group_set.begin() + s.group_ptr[g], s.group_set.begin() + s.group_ptr[g + 1]);
     if (!device) dag_csr = transpose(fdag);  // parents of each group, then the group itself
     stage("threads per level + group sort + inverse DAG");
-    if (mapping == Mapping::FourRule)
+    if (ablation == Ablation::WOS || ablation == Ablation::WOAS)
+        cost_split_map(s, false);  // Task::constructTask
+    else if (mapping == Mapping::FourRule)
         four_rule_map(s, dag_csr);  // stage 9
     else if (mapping == Mapping::FinishTime)
         finish_time_map(s, dag_csr);

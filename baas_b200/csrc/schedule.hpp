@@ -65,6 +65,14 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
 // P2P_MAPPING, parent-thread affinity scores with load rebalancing.
 enum class Mapping { FourRule = 0, CostSplit = 1, CostSplitBarrier = 2, FinishTime = 3, Affinity = 4 };
 
+// The SpTRSV runtime's ablation classes (test/SpTRSV_level_merge.cpp:156-299): None is BAAS; WOS
+// keeps the coarsening and replaces the four-rule mapping by a TRSV level merge and the
+// cost-balanced split (SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P); WOA keeps the four-rule mapping on
+// ungrouped rows (...MapFourRuleAblationWOAggregation); WOAS does neither: ungrouped rows, as
+// many threads per level as rows (level_nthreads_base), the cost-balanced split
+// (...MapFourRuleAblationBase).
+enum class Ablation { None = 0, WOS = 1, WOA = 2, WOAS = 3 };
+
 // The data-parallel integer stages on the current CUDA device (analysis.cu): transposes, the
 // two-hop reduction (stage 2), the group DAGs (stage 4 and the one after stage 5) and the level
 // sets (stage 7). Patterns stay resident on the device between stages; every output equals the
@@ -110,6 +118,6 @@ private:
 // `why` set when the affinity mapping would leave a group unmapped (the reference's P2P_MAPPING
 // scan can) or a device stage failed.
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
-                    Mapping mapping, bool device, std::string &why);
+                    Mapping mapping, Ablation ablation, bool device, std::string &why);
 
 }  // namespace baas

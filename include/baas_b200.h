@@ -118,7 +118,19 @@ typedef struct baas_options {
                          sweeps and ICCG use */
     int analysis;     /* BAAS_ANALYSIS_HOST (default) or BAAS_ANALYSIS_DEVICE: where the analysis's
                          data-parallel stages run; the schedule is identical either way */
+    int ablation;     /* BAAS_ABLATION_NONE (default) or, for BAAS_KERNEL_SPTRSV with the four-rule
+                         mapping, one of the SpTRSV runtime's ablation schedules */
 } baas_options;
+
+/* The SpTRSV runtime's ablation classes (test/SpTRSV_level_merge.cpp:156-299), kind
+ * BAAS_KERNEL_SPTRSV only. NONE: BAAS (SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule). WOS
+ * (BAASWOS, SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P, test/SpTRSVRuntime.hpp:448-535): both coarsenings,
+ * then level_merge_group_TRSV and the cost-balanced split (Task::constructTask) instead of the
+ * four-rule mapping. WOA (BAASWOA, ...MapFourRuleAblationWOAggregation, :1114-1190): no coarsening
+ * (one group per row of the two-hop DAG), the four-rule mapping. WOAS (BAASWOAS,
+ * ...MapFourRuleAblationBase, :913-975): no coarsening, min(rows, nthread) threads per level
+ * (level_nthreads_base), the cost-balanced split. The GPU sweep runs any of them. */
+enum { BAAS_ABLATION_NONE = 0, BAAS_ABLATION_WOS = 1, BAAS_ABLATION_WOA = 2, BAAS_ABLATION_WOAS = 3 };
 
 /* Where baas_analyze runs the schedule's data-parallel integer stages: the transposes of the
  * lower triangle and of the DAGs (dcsr2csc, spm/CSR.cpp:914-950), the two-hop reduction

@@ -70,6 +70,7 @@ class Ref:
             L.ref_pcg.argtypes = [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _i, _d, _vp, _vp]
             L.ref_pcg.restype = _i
             L.ref_set_mapping.argtypes = [_i]
+            L.ref_set_ablation.argtypes = [_i]
             L.ref_mtx_read.argtypes = [C.c_char_p, _vp, _vp]
             L.ref_mtx_read.restype = _vp
             L.ref_mtx_copy.argtypes = [_vp, _vp, _vp, _vp]
@@ -95,16 +96,20 @@ class Ref:
         return _CSR(n.value, rowptr, colidx, values)
 
     class Schedule:
-        def __init__(self, kind: int, A, nthread: int, mapping: int = 0):
+        def __init__(self, kind: int, A, nthread: int, mapping: int = 0, ablation: int = 0):
+            """ablation (kind SPTRSV): 0 BAAS, 1 BAASWOS, 2 BAASWOA, 3 BAASWOAS -- the SpTRSV
+            runtime's ablation classes (test/SpTRSV_level_merge.cpp:156-299)."""
             L = Ref.lib()
             self.rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
             self.colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
             self.n = A.n
             L.ref_set_mapping(mapping)
+            L.ref_set_ablation(ablation)
             try:
                 self.h = L.ref_schedule_build(kind, A.n, _p(self.rowptr), _p(self.colidx), nthread)
             finally:
                 L.ref_set_mapping(0)
+                L.ref_set_ablation(0)
 
         def __del__(self):
             if getattr(self, "h", None):

@@ -187,6 +187,98 @@ namespace refdrv
         h->schedule->constructInverseSchedule(h->taskDAG);
     }
 
+    // The SpTRSV runtime's ablation classes (test/SpTRSV_level_merge.cpp:156-299), their buildset()
+    // call sequences on the lower triangle: 1 = BAASWOS, SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P
+    // (test/SpTRSVRuntime.hpp:448-535: both coarsenings, level_merge_group_TRSV, constructTask,
+    // constructTaskDAGParallel); 2 = BAASWOA, ...MapFourRuleAblationWOAggregation (:1114-1190: one
+    // group per row on the two-hop DAG, level_nthreads_group_TRSV, the four-rule mapping,
+    // constructTaskDAG); 3 = BAASWOAS, ...MapFourRuleAblationBase (:913-975: one group per row,
+    // level_nthreads_base, constructTask, constructTaskDAG).
+    static void ablation_buildset(Handle *h, const CSR *csrA, const CSC *cscA, int nnz, int ablation)
+    {
+        const int n = h->n;
+        h->taskDAG = new DAG();
+        DAG *dag = new DAG(n, nnz);
+        dag->DAG_ptr.clear();
+        dag->DAG_set.clear();
+        DAG::partialSparsification_CSC(n, nnz, cscA->colptr, cscA->rowidx, dag->DAG_ptr, dag->DAG_set, false);
+        LevelSet *levelset = new LevelSet();
+        if (ablation == 1)
+        {
+            h->dag_group = new DAG();
+            Coarsen::reverseTreeCoarseningBFS_all(n, dag->DAG_ptr, dag->DAG_set, h->ngroups, h->group_ptr, h->group_set);
+            Coarsen::buildGroupDAG(n, h->ngroups, h->group_ptr.data(), h->group_set.data(), dag->DAG_ptr.data(),
+                                   dag->DAG_set.data(), h->dag_group->DAG_ptr, h->dag_group->DAG_set);
+            h->dag_group->setNodeNum(h->ngroups);
+            delete dag;
+            std::vector<int> group_ptr_f, group_set_f;
+            DAG *dag_group_f = new DAG();
+            int ngroups_f = 0;
+            Coarsen::forwardTreeCoarseningBFS_all(h->ngroups, h->dag_group->DAG_ptr, h->dag_group->DAG_set, ngroups_f,
+                                                  group_ptr_f, group_set_f, false);
+            Coarsen::groupRemapping(h->group_ptr, h->group_set, group_ptr_f, group_set_f, ngroups_f);
+            Coarsen::buildGroupDAG(h->ngroups, ngroups_f, group_ptr_f.data(), group_set_f.data(),
+                                   h->dag_group->DAG_ptr.data(), h->dag_group->DAG_set.data(), dag_group_f->DAG_ptr,
+                                   dag_group_f->DAG_set);
+            h->ngroups = ngroups_f;
+            dag_group_f->setNodeNum(ngroups_f);
+            dag_group_f->updateEdges();
+            dag_group_f->findLevelsPostOrder(levelset);
+            delete h->dag_group;
+            h->dag_group = dag_group_f;
+        }
+        else
+        {
+            h->group_ptr.assign(n + 1, 0);
+            h->group_set.assign(n, 0);
+            for (int i = 0; i < n; i++)
+            {
+                h->group_set[i] = i;
+                h->group_ptr[i + 1] = i + 1;
+            }
+            h->ngroups = n;
+            h->dag_group = dag;
+            h->dag_group->setNodeNum(n);
+            h->dag_group->updateEdges();
+            h->dag_group->findLevelsPostOrder(levelset);
+        }
+        Coarsen::costComputation(h->ngroups, nullptr, nullptr, csrA->rowptr, csrA->colidx, Coarsen::Kernel::SpTRSV_LL,
+                                 h->group_ptr.data(), h->group_set.data(), true, h->cost);
+        if (ablation == 1)
+        {
+            h->levelset = new LevelSet();
+            Merge::level_merge_group_TRSV(levelset, csrA, h->cost.data(), h->nthread_per_level, h->levelset, h->nthread,
+                                          h->group_ptr.data(), h->group_set.data(), h->ngroups);
+            delete levelset;
+        }
+        else
+        {
+            h->levelset = levelset;
+            if (ablation == 2)
+                Merge::level_nthreads_group_TRSV(levelset, csrA, h->group_ptr.data(), h->group_set.data(), h->nthread,
+                                                 h->nthread_per_level);
+            else
+                Merge::level_nthreads_base(levelset, csrA, h->nthread, h->nthread_per_level);
+        }
+        orderingGroupSet(h->ngroups, h->group_ptr, h->group_set);
+        h->task = new Merge::Task(h->ngroups, false);
+        DAG *inv = DAG::inverseDAG(*h->dag_group);
+        if (ablation == 2)
+            h->task->constructMappingByFourRuleParallel(h->dag_group, inv, h->levelset, h->cost.data(), h->nthread,
+                                                        h->nthread_per_level, h->group_ptr.data(), h->group_set.data());
+        else
+            h->task->constructTask(h->levelset, h->cost.data(), h->nthread, h->nthread_per_level);
+        if (ablation == 1)
+            h->task->constructTaskDAGParallel(h->dag_group, inv, h->taskDAG, h->nthread, false);
+        else
+            h->task->constructTaskDAG(h->dag_group, inv, h->taskDAG, h->nthread, false);
+        delete inv;
+        h->schedule = new Merge::TaskSchedule(h->taskDAG->getNodeNum(), h->taskDAG->DAG_ptr.back());
+        h->schedule->constructTaskSchedule(h->taskDAG);
+        // the exported backward task DAG, built as for the BAAS class above
+        h->schedule->constructInverseSchedule(h->taskDAG);
+    }
+
     static int copy_out(const int *src, int len, int *out)
     {
         if (out && len > 0)
@@ -199,6 +291,8 @@ using namespace refdrv;
 
 // the mapping the next ICCG schedule build uses (ref_set_mapping)
 static int g_mapping = BAAS_MAPPING_FOUR_RULE;
+// the SpTRSV ablation class the next SpTRSV build uses (ref_set_ablation; 0 = BAAS)
+static int g_ablation = 0;
 
 extern "C"
 {
@@ -206,6 +300,9 @@ extern "C"
      * COST_SPLIT_BARRIER with P2P followed by the barrier-mode task layout, FINISH_TIME with
      * P2P_TIME, AFFINITY with P2P_MAPPING. */
     void ref_set_mapping(int mapping) { g_mapping = mapping; }
+
+    /* 0: BAAS (SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule); 1: BAASWOS; 2: BAASWOA; 3: BAASWOAS. */
+    void ref_set_ablation(int ablation) { g_ablation = ablation; }
 
     /* kind: a baas_kernel value. The matrix is the lower triangle incl. diagonal (diagonal last
      * in each row) for BAAS_KERNEL_SPTRSV and the full matrix for the other kinds. */
@@ -241,7 +338,10 @@ extern "C"
             // test/SpTRSV_level_merge.cpp:59-60 builds the CSC this way
             h->csc = new CSC();
             CSR::transpositionToCSC(h->A, h->csc);
-            class_buildset(h, h->A, h->csc, h->A, nnz);
+            if (g_ablation == 0)
+                class_buildset(h, h->A, h->csc, h->A, nnz);
+            else
+                ablation_buildset(h, h->A, h->csc, nnz, g_ablation);
         }
         else
         {
