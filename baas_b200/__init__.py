@@ -20,7 +20,7 @@ import numpy as np
 from . import _native
 from ._native import (KERNEL_IC0, KERNEL_ICCG, KERNEL_ILU0, KERNEL_SPTRSV, MAPPING_COST_SPLIT,
                       MAPPING_AFFINITY, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_FOUR_RULE, PARTITION_BAAS_THREADS, PARTITION_CUSTOM,
-                      PARTITION_RANGES, PARTITION_BLOCKS, PARTITION_AUTO, WALK_AUTO, WALK_CHUNKED, WALK_FETCH, WALK_LEVELS,
+                      PARTITION_RANGES, PARTITION_BLOCKS, PARTITION_AUTO, WALK_AUTO, WALK_CHUNKED, WALK_FETCH, WALK_LEVELS, WALK_SMALL,
                       ANALYSIS_HOST, ANALYSIS_DEVICE, ABLATION_NONE, ABLATION_WOS, ABLATION_WOA, ABLATION_WOAS,
                       PREC_FP32_FACTORS, PREC_FP64, BaasError)
 from .gen import CSR
@@ -29,7 +29,7 @@ __all__ = ["Schedule", "BatchSchedule", "batch_concat", "DeviceCSR", "BaasError"
            "KERNEL_ICCG", "KERNEL_IC0", "KERNEL_ILU0", "PREC_FP64", "PREC_FP32_FACTORS", "PARTITION_RANGES",
            "PARTITION_BAAS_THREADS", "PARTITION_CUSTOM", "MAPPING_FOUR_RULE", "MAPPING_COST_SPLIT",
            "MAPPING_COST_SPLIT_BARRIER", "MAPPING_FINISH_TIME", "MAPPING_AFFINITY", "WALK_AUTO", "WALK_CHUNKED",
-           "WALK_FETCH", "WALK_LEVELS", "PARTITION_BLOCKS", "PARTITION_AUTO", "ANALYSIS_HOST", "ANALYSIS_DEVICE",
+           "WALK_FETCH", "WALK_LEVELS", "WALK_SMALL", "PARTITION_BLOCKS", "PARTITION_AUTO", "ANALYSIS_HOST", "ANALYSIS_DEVICE",
            "ABLATION_NONE", "ABLATION_WOS", "ABLATION_WOA", "ABLATION_WOAS", "version"]
 
 

@@ -26,7 +26,7 @@ STATUS_NAMES = {
 KERNEL_SPTRSV, KERNEL_ICCG, KERNEL_IC0, KERNEL_ILU0 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32_FACTORS = 0, 1
 PARTITION_RANGES, PARTITION_BAAS_THREADS, PARTITION_CUSTOM, PARTITION_BLOCKS, PARTITION_AUTO = 0, 1, 2, 3, 4
-WALK_AUTO, WALK_CHUNKED, WALK_FETCH, WALK_LEVELS = 0, 1, 2, 3
+WALK_AUTO, WALK_CHUNKED, WALK_FETCH, WALK_LEVELS, WALK_SMALL = 0, 1, 2, 3, 4
 ANALYSIS_HOST, ANALYSIS_DEVICE = 0, 1
 ABLATION_NONE, ABLATION_WOS, ABLATION_WOA, ABLATION_WOAS = 0, 1, 2, 3
 MAPPING_FOUR_RULE, MAPPING_COST_SPLIT, MAPPING_COST_SPLIT_BARRIER, MAPPING_FINISH_TIME, MAPPING_AFFINITY = 0, 1, 2, 3, 4

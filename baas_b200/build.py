@@ -18,7 +18,8 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libbaas_b200.so"
 SOURCES = ["capi.cu", "analysis.cu", "schedule.cpp", "mtx.cpp"]
-HEADERS = ["kernels.cuh", "part_kernels.cuh", "staged.cuh", "fetch.cuh", "batched.cuh", "device_common.cuh", "schedule.hpp"]
+HEADERS = ["kernels.cuh", "part_kernels.cuh", "staged.cuh", "fetch.cuh", "batched.cuh", "small.cuh", "device_common.cuh",
+           "schedule.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

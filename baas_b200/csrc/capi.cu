@@ -23,6 +23,7 @@
 #include "part_kernels.cuh"
 #include "batched.cuh"
 #include "staged.cuh"
+#include "small.cuh"
 #include "schedule.hpp"
 
 using baas::DevStatus;
@@ -202,6 +203,19 @@ struct FetchDev {
     }
 };
 
+// Single-CTA walk plan (small.cuh): row levels of both directions and each row's record in the
+// caller's triangular layouts (rec_t: L diagonal last, U = L^T diagonal first) and in the full
+// matrix's layouts ICCG and IC0 read (rec_a: A's lower part; U's off-diagonal entries gathered
+// from the IC0 factor), plus the IC0 column-match pairs.
+struct SmallHost {
+    bool built = false;
+    int nlev[2] = {0, 0};
+    std::vector<int> lev[2];
+    std::vector<int4> rec_t[2], rec_a[2];
+    std::vector<int> ic_ptr, ub_col, ub_pos;
+    std::vector<int2> ic_pair;
+};
+
 // Level-walk plan (staged.cuh level_walk): the whole schedule as one partition, per direction.
 struct LevelHostDir {
     std::vector<int> lev, item, row, eptr, dep, src, dsrc, srcT, dsrcT;
@@ -285,6 +299,13 @@ struct baas_schedule {
     double *d_lv64[2] = {nullptr, nullptr}, *d_ld64[2] = {nullptr, nullptr};  // its values (ICCG, FP64)
     float *d_lv32[2] = {nullptr, nullptr}, *d_ld32[2] = {nullptr, nullptr};   // (ICCG, FP32 factors)
     double *d_lvT[2] = {nullptr, nullptr}, *d_ldT[2] = {nullptr, nullptr};    // (caller's factor, sweeps)
+    SmallHost sm;                            // single-CTA walk plan (host), built on first use
+    int *d_sm_lev[2] = {nullptr, nullptr};
+    int4 *d_sm_rec_t[2] = {nullptr, nullptr}, *d_sm_rec_a[2] = {nullptr, nullptr};
+    int *d_sm_ic_ptr = nullptr, *d_sm_ub_col = nullptr, *d_sm_ub_pos = nullptr;
+    int2 *d_sm_ic_pair = nullptr;
+    double *d_sm_ut = nullptr;
+    float *d_sm_lf32 = nullptr, *d_sm_ut32 = nullptr, *d_sm_rcp32 = nullptr;
     std::map<int, WinCfg> wins;  // key: value bytes * 16 + right-hand sides
     int smem_budget = 0;
     int rmax64 = 1;  // most FP64 right-hand sides one sweep walks together
@@ -1082,10 +1103,158 @@ constexpr int kLevelWalkMaxLevels = 64;
 // The walk of a launch (values of vbytes bytes; ICCG, or a standalone sweep of one right-hand
 // side): FETCH where the fetch plan qualifies and fits shared memory, else LEVELS for shallow
 // group DAGs, else CHUNKED. An explicitly requested walk that cannot run is an error.
-baas_status pick_walk(const baas_schedule *s, int vbytes, bool iccg, int &walk) {
+// Dynamic shared memory the single-CTA walk may use: 227 KB less its static level offsets.
+constexpr size_t kSmallMaxDyn = 227 * 1024 - 2 * baas::kSmallLevShared * sizeof(int) - 2048;
+// Automatic choice of the single-CTA walk: row DAGs of at most this many levels per direction.
+constexpr int kSmallAutoLevels = 64;
+
+// The single-CTA walk's host plan (small.cuh): row levels from the analysed lower pattern, U's
+// pattern by a transpose that keeps each entry's L position, and the IC0 column-match pairs.
+void build_small(baas_schedule *s) {
+    SmallHost &m = s->sm;
+    if (m.built) return;
+    const baas::HostSchedule &h = s->hs;
+    const int n = h.n;
+    const std::vector<int> &lp = h.l_rowptr, &lc = h.l_colidx;
+    const bool full = h.kind != baas::SchedKind::SpTRSV;
+    // U = L^T: row c holds its diagonal first, then the rows k > c whose L row has column c
+    std::vector<int> urp(n + 1, 0), ucol(lc.size()), upos(lc.size());
+    for (int c : lc) urp[c + 1]++;
+    for (int i = 0; i < n; i++) urp[i + 1] += urp[i];
+    std::vector<int> cur(urp.begin(), urp.end() - 1);
+    for (int k = 0; k < n; k++)
+        for (int e = lp[k]; e < lp[k + 1]; e++) {
+            const int c = lc[e];
+            ucol[cur[c]] = k;
+            upos[cur[c]++] = e;
+        }
+    // row levels: forward over L's off-diagonal columns, backward over U's
+    std::vector<int> lv[2] = {std::vector<int>(n), std::vector<int>(n)};
+    for (int i = 0; i < n; i++) {
+        int v = 0;
+        for (int e = lp[i]; e < lp[i + 1] - 1; e++) v = std::max(v, lv[0][lc[e]]);
+        lv[0][i] = v + 1;
+    }
+    for (int i = n - 1; i >= 0; i--) {
+        int v = 0;
+        for (int e = urp[i] + 1; e < urp[i + 1]; e++) v = std::max(v, lv[1][ucol[e]]);
+        lv[1][i] = v + 1;
+    }
+    for (int d = 0; d < 2; d++) {
+        int nl = 0;
+        for (int i = 0; i < n; i++) nl = std::max(nl, lv[d][i]);
+        m.nlev[d] = nl;
+        m.lev[d].assign(nl + 1, 0);
+        for (int i = 0; i < n; i++) m.lev[d][lv[d][i]]++;
+        for (int l = 0; l < nl; l++) m.lev[d][l + 1] += m.lev[d][l];
+        std::vector<int> at(m.lev[d].begin(), m.lev[d].end() - 1);
+        m.rec_t[d].assign(n, int4{0, 0, 0, 0});
+        if (full) m.rec_a[d].assign(n, int4{0, 0, 0, 0});
+        for (int i = 0; i < n; i++) {  // rows ascending inside each level
+            const int q = at[lv[d][i] - 1]++;
+            if (d == 0) {
+                m.rec_t[0][q] = int4{i, lp[i], lp[i + 1] - 1 - lp[i], lp[i + 1] - 1};
+                if (full) m.rec_a[0][q] = int4{i, h.a_rowptr[i], h.a_diagptr[i] - h.a_rowptr[i], h.a_diagptr[i]};
+            } else {
+                m.rec_t[1][q] = int4{i, urp[i] + 1, urp[i + 1] - urp[i] - 1, urp[i]};
+                if (full) m.rec_a[1][q] = int4{i, urp[i] - i, urp[i + 1] - urp[i] - 1, h.a_diagptr[i]};
+            }
+        }
+    }
+    if (full) {
+        for (int i = 0; i < n; i++)
+            for (int e = urp[i] + 1; e < urp[i + 1]; e++) {
+                m.ub_col.push_back(ucol[e]);
+                m.ub_pos.push_back(h.l_src[upos[e]]);
+            }
+        // IC0: for lower entry k of row i (column j), the positions in rows i and j of the columns
+        // both hold below j, ascending (sparse_dot's merge, merge/IC.cpp:6-29)
+        const std::vector<int> &rp = h.a_rowptr, &ci = h.a_colidx, &dg = h.a_diagptr;
+        m.ic_ptr.assign(rp[n] + 1, 0);
+        for (int i = 0; i < n; i++)
+            for (int k = rp[i]; k < dg[i]; k++) {
+                const int j = ci[k];
+                int a = rp[i], b = rp[j];
+                while (a < dg[i] && b < dg[j]) {
+                    if (ci[a] == ci[b]) {
+                        m.ic_pair.push_back(int2{a, b});
+                        a++;
+                        b++;
+                    } else if (ci[a] < ci[b]) {
+                        a++;
+                    } else {
+                        b++;
+                    }
+                }
+                m.ic_ptr[k + 1] = (int)m.ic_pair.size();
+            }
+        for (int k = 0; k < rp[n]; k++) m.ic_ptr[k + 1] = std::max(m.ic_ptr[k + 1], m.ic_ptr[k]);
+    }
+    m.built = true;
+}
+
+baas_status upload_small(baas_schedule *s, bool full) {
+    build_small(s);
+    const SmallHost &m = s->sm;
+    for (int d = 0; d < 2; d++) {
+        if (!s->d_sm_lev[d]) BAAS_TRY(upload(s->d_sm_lev[d], m.lev[d]));
+        if (!s->d_sm_rec_t[d]) BAAS_TRY(upload(s->d_sm_rec_t[d], m.rec_t[d]));
+        if (full && !s->d_sm_rec_a[d]) BAAS_TRY(upload(s->d_sm_rec_a[d], m.rec_a[d]));
+    }
+    if (full && !s->d_sm_ic_ptr) {
+        BAAS_TRY(upload(s->d_sm_ic_ptr, m.ic_ptr));
+        BAAS_TRY(upload(s->d_sm_ic_pair, m.ic_pair));
+        BAAS_TRY(upload(s->d_sm_ub_col, m.ub_col));
+        BAAS_TRY(upload(s->d_sm_ub_pos, m.ub_pos));
+        BAAS_TRY(dalloc(s->d_sm_ut, std::max<size_t>(m.ub_col.size(), 1)));
+        BAAS_TRY(dalloc(s->d_sm_ut32, std::max<size_t>(m.ub_col.size(), 1)));
+        BAAS_TRY(dalloc(s->d_sm_lf32, (size_t)s->nnz_a));
+        BAAS_TRY(dalloc(s->d_sm_rcp32, (size_t)s->hs.n));
+    }
+    return BAAS_OK;
+}
+
+baas::SmallArgs small_args(const baas_schedule *s, bool full) {
+    baas::SmallArgs a{};
+    a.n = s->hs.n;
+    for (int d = 0; d < 2; d++)
+        a.dir[d] = baas::SmallDir{s->sm.nlev[d], s->d_sm_lev[d], full ? s->d_sm_rec_a[d] : s->d_sm_rec_t[d]};
+    a.st = s->d_status;
+    if (full) {
+        a.a_diag = s->d_a_diag;
+        a.ic_ptr = s->d_sm_ic_ptr;
+        a.ic_pair = s->d_sm_ic_pair;
+        a.ub_col = s->d_sm_ub_col;
+        a.ub_pos = s->d_sm_ub_pos;
+        a.nub = (int)s->sm.ub_col.size();
+        a.ut = s->d_sm_ut;
+        a.lf32 = s->d_sm_lf32;
+        a.ut32 = s->d_sm_ut32;
+        a.rcp32 = s->d_sm_rcp32;
+    }
+    return a;
+}
+
+// One launch of a single-CTA kernel with `dyn` bytes of dynamic shared memory.
+baas_status launch_small(const void *kern, size_t dyn, void **args, cudaStream_t stream) {
+    BAAS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    BAAS_CUDA(cudaLaunchKernel(kern, dim3(1), dim3(baas::kSmallBlock), args, dyn, stream));
+    return BAAS_OK;
+}
+
+baas_status pick_walk(baas_schedule *s, int vbytes, bool iccg, int &walk) {
     const bool fits = s->fch.ok && fetch_smem(s->fch, vbytes, iccg) <= (size_t)kMaxDynSmem;
     const int nlev = (int)s->hs.exec_level_ptr.size() - 1;
+    // the single-CTA walk keeps the sweep's solution (and ICCG's p, FP64) in shared memory
+    const size_t small_row = iccg ? 8 + (size_t)vbytes : 8;
+    const bool small_fits = (size_t)s->hs.n * small_row <= kSmallMaxDyn;
     switch (s->opt.walk) {
+        case BAAS_WALK_SMALL:
+            if (!small_fits)
+                return fail(BAAS_ERR_BAD_ARG, "the single-CTA walk holds at most " + std::to_string(kSmallMaxDyn / small_row) +
+                                                  " rows here");
+            walk = BAAS_WALK_SMALL;
+            return BAAS_OK;
         case BAAS_WALK_FETCH:
             if (!fits)
                 return fail(BAAS_ERR_BAD_ARG, "the fetch walk needs rows of at most 3 off-diagonal entries, steps of at most " +
@@ -1094,7 +1263,14 @@ baas_status pick_walk(const baas_schedule *s, int vbytes, bool iccg, int &walk) 
             break;
         case BAAS_WALK_CHUNKED: walk = BAAS_WALK_CHUNKED; break;
         case BAAS_WALK_LEVELS: walk = BAAS_WALK_LEVELS; break;
-        default: walk = fits ? BAAS_WALK_FETCH : (nlev <= kLevelWalkMaxLevels ? BAAS_WALK_LEVELS : BAAS_WALK_CHUNKED);
+        default:
+            if (fits) {
+                walk = BAAS_WALK_FETCH;
+            } else if (small_fits && (build_small(s), std::max(s->sm.nlev[0], s->sm.nlev[1]) <= kSmallAutoLevels)) {
+                walk = BAAS_WALK_SMALL;
+            } else {
+                walk = nlev <= kLevelWalkMaxLevels ? BAAS_WALK_LEVELS : BAAS_WALK_CHUNKED;
+            }
     }
     return BAAS_OK;
 }
@@ -1333,7 +1509,7 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         return fail(BAAS_ERR_BAD_ARG, "unknown partition");
     if (o.parts < 0) return fail(BAAS_ERR_BAD_ARG, "parts must be >= 0");
     if (o.smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "smem_budget must be >= 0");
-    if (o.walk < BAAS_WALK_AUTO || o.walk > BAAS_WALK_LEVELS) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
+    if (o.walk < BAAS_WALK_AUTO || o.walk > BAAS_WALK_SMALL) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
     if (o.mapping < BAAS_MAPPING_FOUR_RULE || o.mapping > BAAS_MAPPING_AFFINITY)
         return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
     if (o.analysis != BAAS_ANALYSIS_HOST && o.analysis != BAAS_ANALYSIS_DEVICE)
@@ -1782,7 +1958,14 @@ static void release_device(baas_schedule *s) {
             if (s->d_gv64[d]) cudaFree(s->d_gv64[d]);
             if (s->d_gv32[d]) cudaFree(s->d_gv32[d]);
             if (s->d_gvT[d]) cudaFree(s->d_gvT[d]);
+            void *sp[] = {s->d_sm_lev[d], s->d_sm_rec_t[d], s->d_sm_rec_a[d]};
+            for (void *p : sp)
+                if (p) cudaFree(p);
         }
+        void *smp[] = {s->d_sm_ic_ptr, s->d_sm_ub_col, s->d_sm_ub_pos, s->d_sm_ic_pair, s->d_sm_ut, s->d_sm_lf32,
+                       s->d_sm_ut32, s->d_sm_rcp32};
+        for (void *p : smp)
+            if (p) cudaFree(p);
         void *ptrs[] = {s->d_a_diag, s->d_status, s->d_flags, s->d_bar, s->d_lu, s->d_r, s->d_y, s->d_z, s->d_p,
                         s->d_Ap, s->d_y32, s->d_z32, s->d_part, s->d_iters, s->d_relres, s->d_x0};
         for (void *p : ptrs)
@@ -1809,6 +1992,7 @@ static void release_device(baas_schedule *s) {
     fresh.sys_off = std::move(s->sys_off);
     fresh.nsys = s->nsys;
     fresh.custom_part = std::move(s->custom_part);
+    fresh.sm = std::move(s->sm);
     *s = std::move(fresh);
 }
 
@@ -1823,7 +2007,7 @@ baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
     if (opt->nthread != s->hs.nthread) return fail(BAAS_ERR_BAD_ARG, "nthread is fixed by the analysis");
     if (opt->mapping != s->opt.mapping) return fail(BAAS_ERR_BAD_ARG, "mapping is fixed by the analysis");
     if (opt->parts < 0 || opt->smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "parts and smem_budget must be >= 0");
-    if (opt->walk < BAAS_WALK_AUTO || opt->walk > BAAS_WALK_LEVELS) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
+    if (opt->walk < BAAS_WALK_AUTO || opt->walk > BAAS_WALK_SMALL) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
     if (opt->partition == BAAS_PARTITION_CUSTOM) {
         if (s->custom_part.empty()) return fail(BAAS_ERR_BAD_ARG, "no custom partition: use baas_replan_custom");
         if (opt->parts != s->opt.parts) return fail(BAAS_ERR_BAD_ARG, "a custom partition fixes parts");
@@ -1866,6 +2050,20 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
     const int d = upper ? 1 : 0;
     int walk = BAAS_WALK_CHUNKED;
     if (nrhs == 1) BAAS_TRY(pick_walk(s, 8, false, walk));
+    if (walk == BAAS_WALK_SMALL) {
+        BAAS_TRY(upload_small(s, false));
+        baas::SmallArgs a = small_args(s, false);
+        a.b = b;
+        a.x = x;
+        const int *tcol = T->colidx;
+        const double *tval = T->values;
+        void *args[] = {(void *)&a, (void *)&tcol, (void *)&tval};
+        s->last_walk = BAAS_WALK_SMALL;
+        BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+        BAAS_TRY(launch_small(upper ? (const void *)baas::k_sweep_small<true> : (const void *)baas::k_sweep_small<false>,
+                              sizeof(double) * (size_t)n, args, stream));
+        return read_status(s, stream);
+    }
     if (walk == BAAS_WALK_LEVELS) {
         if (!s->d_lv[0].lev) BAAS_TRY(upload_level(s));
         if (!s->d_lvT[d]) {
@@ -1906,8 +2104,8 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
         return fail(BAAS_ERR_CUDA, "IEEE sweep reported a fast-path division");
     }
     s->last_walk = BAAS_WALK_CHUNKED;
-    if (s->opt.walk == BAAS_WALK_FETCH || s->opt.walk == BAAS_WALK_LEVELS)
-        return fail(BAAS_ERR_BAD_ARG, "the fetch and level walks take one right-hand side");
+    if (s->opt.walk == BAAS_WALK_FETCH || s->opt.walk == BAAS_WALK_LEVELS || s->opt.walk == BAAS_WALK_SMALL)
+        return fail(BAAS_ERR_BAD_ARG, "the fetch, level and single-CTA walks take one right-hand side");
     // right-hand sides walked together: as many as the solution slots leave room for
     const int R = std::min(nrhs, s->rmax64);
     WinCfg *w = nullptr;
@@ -1940,6 +2138,19 @@ static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void 
         return fail(BAAS_ERR_BAD_ARG, "matrix does not match the analysed pattern");
     BAAS_TRY(ensure_device(s));
     cudaStream_t stream = (cudaStream_t)stream_;
+    int walk = BAAS_WALK_CHUNKED;
+    if (!ilu && (s->opt.walk == BAAS_WALK_AUTO || s->opt.walk == BAAS_WALK_SMALL)) BAAS_TRY(pick_walk(s, 8, true, walk));
+    if (walk == BAAS_WALK_SMALL) {  // IC0 by one CTA over the row levels (its shared memory holds no rows)
+        BAAS_TRY(upload_small(s, true));
+        baas::SmallArgs a = small_args(s, true);
+        a.a_rowptr = A->rowptr;
+        a.a_colidx = A->colidx;
+        a.lu = lu;
+        void *args[] = {(void *)&a};
+        BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+        BAAS_CUDA(cudaLaunchKernel((const void *)baas::k_ic0_small, dim3(1), dim3(baas::kSmallBlock), args, 0, stream));
+        return read_status(s, stream);
+    }
     BAAS_TRY(next_epoch(s, stream));
     BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
     baas::PartView pv = s->d_fwd.view(s->P);
@@ -2220,6 +2431,41 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
     const bool mixed = precision == BAAS_PREC_FP32_FACTORS;
     int walk = BAAS_WALK_CHUNKED;
     BAAS_TRY(pick_walk(s, mixed ? 4 : 8, true, walk));
+    if (walk == BAAS_WALK_SMALL) {
+        BAAS_TRY(upload_small(s, true));
+        baas::SmallArgs a = small_args(s, true);
+        a.a_rowptr = A->rowptr;
+        a.a_colidx = A->colidx;
+        a.a_val = A->values;
+        a.lu = s->d_lu;
+        a.b = b;
+        a.x = x;
+        a.r = s->d_r;
+        a.Ap = s->d_Ap;
+        a.maxiter = maxiter;
+        a.tol = tol;
+        a.reuse = reuse ? 1 : 0;
+        a.out_iters = s->d_iters;
+        a.out_relres = s->d_relres;
+        a.xf = xf;
+        a.grad_a = grad_a;
+        void *args[] = {(void *)&a};
+        s->last_walk = BAAS_WALK_SMALL;
+        BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
+        BAAS_TRY(launch_small(mixed ? (const void *)baas::k_iccg_small<float> : (const void *)baas::k_iccg_small<double>,
+                              (size_t)n * (8 + (mixed ? 4 : 8)), args, stream));
+        int it = 0;
+        double rr = 0.0;
+        BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        BAAS_CUDA(cudaMemcpyAsync(&rr, s->d_relres, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        const baas_status st = read_status(s, stream);
+        if (iters) *iters = it;
+        if (relres) *relres = rr;
+        if (!reuse) s->factor_prec = st == BAAS_OK || st == BAAS_ERR_NOT_CONVERGED ? precision : -1;
+        if (st != BAAS_OK) return st;
+        if (!(rr < tol)) return fail(BAAS_ERR_NOT_CONVERGED, "maxiter reached before tol");
+        return BAAS_OK;
+    }
     const bool fw = walk == BAAS_WALK_FETCH, lw = walk == BAAS_WALK_LEVELS;
     if (lw && !s->d_lv[0].lev) BAAS_TRY(upload_level(s));
     if (lw && !s->d_lv64[0]) {

@@ -264,8 +264,16 @@ def c1_sptrsv(flush):
     gbps = nbytes / (ms * 1e-3) / 1e9
     lat = sweep_latency_bound(s)
     lat["frac"] = round(lat["bound_us"] / (ms * 1e3), 4)
+    # the single-CTA walk on the same sweep (253 row levels: the automatic choice keeps the fetch walk)
+    from baas_b200 import WALK_SMALL
+
+    s1 = Schedule(L, kind=KERNEL_SPTRSV, nthread=8, walk=WALK_SMALL)
+    x1 = torch.zeros_like(db)
+    ms1 = _event_ms(lambda: s1.forward(dL, db, x1), 10, flush)
+    same1 = bool(torch.equal(x1, x))
     out = {"workload": "sptrsv_laplace2d_128_lower", "ms": round(ms, 4), "bytes": nbytes, "gbps": round(gbps, 2),
            "max_abs_err_vs_x_true": err, "walk": s.last_walk,
+           "single_cta_walk": {"ms": round(ms1, 4), "bitexact_vs_auto": same1},
            "roofline": {"bound": "hbm", "achieved": round(gbps, 2), "peak": peak, "unit": "GB/s",
                         "frac": round(gbps / peak, 5), "peak_kind": peak_kind, "kernel": "k_sweep_fetch"},
            "latency_bound": lat}

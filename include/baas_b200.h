@@ -113,9 +113,9 @@ typedef struct baas_options {
                          window buffers (0 = library default, 220 KiB; at most 224 KiB) */
     int mapping;      /* BAAS_MAPPING_FOUR_RULE (default) or, for BAAS_KERNEL_ICCG, one of the
                          Scheduler's other mappings; fixed by the analysis */
-    int walk;         /* BAAS_WALK_AUTO (default), BAAS_WALK_CHUNKED, BAAS_WALK_FETCH or
-                         BAAS_WALK_LEVELS: which triangular-sweep kernel the single-right-hand-side
-                         sweeps and ICCG use */
+    int walk;         /* BAAS_WALK_AUTO (default), BAAS_WALK_CHUNKED, BAAS_WALK_FETCH,
+                         BAAS_WALK_LEVELS or BAAS_WALK_SMALL: which triangular-sweep kernel the
+                         single-right-hand-side sweeps and ICCG use */
     int analysis;     /* BAAS_ANALYSIS_HOST (default) or BAAS_ANALYSIS_DEVICE: where the analysis's
                          data-parallel stages run; the schedule is identical either way */
     int ablation;     /* BAAS_ABLATION_NONE (default) or, for BAAS_KERNEL_SPTRSV with the four-rule
@@ -146,10 +146,15 @@ enum { BAAS_ANALYSIS_HOST = 0, BAAS_ANALYSIS_DEVICE = 1 };
  * (stencil matrices) and one right-hand side; the compute warps read every dependency from shared
  * memory while the CTA's last warp brings other CTAs' results in. LEVELS: one right-hand side;
  * every thread of the launch takes groups of a level and a grid barrier ends the level -- for
- * shallow group DAGs (unstructured or permuted patterns: a few dozen wide levels). AUTO: FETCH
- * wherever the plan qualifies and fits shared memory, else LEVELS when the DAG has at most 64
- * group levels, else CHUNKED. Sweeps and factors are bit-identical between the walks. */
-enum { BAAS_WALK_AUTO = 0, BAAS_WALK_CHUNKED = 1, BAAS_WALK_FETCH = 2, BAAS_WALK_LEVELS = 3 };
+ * shallow group DAGs (unstructured or permuted patterns: a few dozen wide levels). SMALL: one
+ * right-hand side, one CTA: the whole solution in shared memory (8 bytes a row; ICCG adds p, and
+ * z is 8 or 4 bytes), rows by row level with a block barrier per level, the next level's entries
+ * loaded while the current one computes -- for systems of up to about 26,000 rows (sweeps) or
+ * 13,000 (FP64 ICCG) / 17,000 (FP32 factors); baas_ic0 takes it at any size. AUTO: FETCH wherever
+ * the plan qualifies and fits shared memory, else SMALL when the system fits it and its row DAG
+ * has at most 64 levels each way, else LEVELS when the group DAG has at most 64 levels, else
+ * CHUNKED. Sweeps and factors are bit-identical between the walks. */
+enum { BAAS_WALK_AUTO = 0, BAAS_WALK_CHUNKED = 1, BAAS_WALK_FETCH = 2, BAAS_WALK_LEVELS = 3, BAAS_WALK_SMALL = 4 };
 
 /* How the analysis maps groups to the reference's virtual threads (Schedule::ALG_SCHEDULE,
  * test/Schedule.hpp:31-37, 263-281). FOUR_RULE: P2P_RULE, the BAAS four-rule mapping

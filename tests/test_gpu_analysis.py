@@ -104,3 +104,12 @@ def test_device_analysed_schedule_solves_like_the_host_one():
         out.append((it, x.cpu().numpy()))
     assert out[0][0] == out[1][0]
     assert np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("ablation", [1, 2, 3])
+def test_device_analysis_of_ablation_schedules(ablation):
+    L = gen.laplace2d(128).lower()
+    for nt in (1, 8):
+        h = Schedule(L, kind=KERNEL_SPTRSV, nthread=nt, ablation=ablation)
+        d = Schedule(L, kind=KERNEL_SPTRSV, nthread=nt, ablation=ablation, analysis=ANALYSIS_DEVICE)
+        _same(h, d, f"ablation={ablation} nthread={nt}")

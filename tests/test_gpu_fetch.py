@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from baas_b200 import (KERNEL_ICCG, KERNEL_SPTRSV, PARTITION_BLOCKS, PREC_FP32_FACTORS, PREC_FP64, WALK_CHUNKED,
-                       WALK_FETCH, WALK_LEVELS, BaasError, DeviceCSR, Schedule, gen)
+                       WALK_FETCH, WALK_SMALL, BaasError, DeviceCSR, Schedule, gen)
 from oracle.oracle import Port
 
 pytestmark = pytest.mark.gpu
@@ -89,9 +89,9 @@ def test_forced_fetch_walk_refuses_wide_rows():
     x = _t(np.zeros(A.n))
     with pytest.raises(BaasError, match="fetch walk"):
         s.iccg(DeviceCSR.from_host(A), _t(gen.uniform_rhs(A.n, 1)), x)
-    s2 = Schedule(A, kind=KERNEL_ICCG, nthread=8)  # automatic: a shallow DAG takes the level walk
+    s2 = Schedule(A, kind=KERNEL_ICCG, nthread=8)  # automatic: a small shallow system takes one CTA
     it, rel = s2.iccg(DeviceCSR.from_host(A), _t(gen.uniform_rhs(A.n, 1)), x)
-    assert s2.last_walk == WALK_LEVELS and rel < 1e-10
+    assert s2.last_walk == WALK_SMALL and rel < 1e-10
 
 
 def test_fetch_walk_timeout_leaves_context_usable():
