@@ -84,7 +84,8 @@ class Schedule:
 
     def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
                  parts: int = 0, partition: int = PARTITION_AUTO, smem_budget: int = 0, mapping: int = 0,
-                 walk: int = 0, analysis: int = ANALYSIS_HOST, ablation: int = ABLATION_NONE):
+                 walk: int = 0, analysis: int = ANALYSIS_HOST, ablation: int = ABLATION_NONE,
+                 small_cluster: int = 0):
         L = _native.lib()
         self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
         self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
@@ -100,6 +101,7 @@ class Schedule:
         opt.walk = walk
         opt.analysis = analysis
         opt.ablation = ablation
+        opt.small_cluster = small_cluster
         h = C.c_void_p()
         _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
         self._h = h
@@ -151,7 +153,7 @@ class Schedule:
         _native.check(_native.lib().baas_test_inject_unsatisfiable_wait(self._h, row), "inject")
 
     def replan(self, parts: int = 0, smem_budget: int = 0, partition: int = PARTITION_AUTO, spin_limit: int = 0,
-               walk: int = 0) -> None:
+               walk: int = 0, small_cluster: int = 0) -> None:
         """Rebuild the device plan with other execution options (baas_replan), keeping the analysis."""
         opt = _native.BaasOptions()
         _native.lib().baas_options_default(C.byref(opt))
@@ -162,6 +164,7 @@ class Schedule:
         opt.partition = partition
         opt.spin_limit = spin_limit
         opt.walk = walk
+        opt.small_cluster = small_cluster
         _native.check(_native.lib().baas_replan(self._h, C.byref(opt)), "baas_replan")
 
     def replan_custom(self, row_part, parts: int | None = None, smem_budget: int = 0) -> None:

@@ -58,7 +58,8 @@ class BaasCsr(C.Structure):
 class BaasOptions(C.Structure):
     _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("parts", C.c_int),
                 ("partition", C.c_int), ("smem_budget", C.c_int), ("mapping", C.c_int), ("walk", C.c_int),
-                ("analysis", C.c_int), ("ablation", C.c_int)]
+                ("analysis", C.c_int), ("ablation", C.c_int),
+                ("small_cluster", C.c_int)]
 
 
 class BaasError(RuntimeError):

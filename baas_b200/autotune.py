@@ -12,6 +12,12 @@ the schedule on the fastest:
 
 Candidates are rebuilt with `Schedule.replan` (baas_replan), which keeps the analysis, so a trial
 costs one plan build and one short run.
+
+`tune_walk` searches the other execution knobs of a single-right-hand-side solve the same way:
+
+  walk           which sweep kernel runs (chunked, fetch, level or single-CTA walk)
+  small_cluster  for the single-CTA walk, the CTAs of its cluster (1, 2, 4, 8): more SMs keep more
+                 loads in flight, at the price of a cluster barrier per level
 """
 from __future__ import annotations
 
@@ -66,4 +72,42 @@ def tune(schedule, run, parts=None, budgets=None, repeats: int = 2, warmup: int 
     t0 = time.time()
     schedule.replan(parts=best["parts"], smem_budget=best["smem_budget"])
     best["replan_s"] = round(time.time() - t0, 3)
+    return {"best": best, "table": table}
+
+
+DEFAULT_WALKS = ((1, 0), (2, 0), (3, 0), (4, 1), (4, 2), (4, 4), (4, 8))  # (walk, small_cluster)
+
+
+def tune_walk(schedule, run, candidates=None, repeats: int = 2, warmup: int = 1) -> dict:
+    """Time `run()` for each (walk, small_cluster) candidate (walks a schedule cannot take are
+    recorded with the reason) and leave `schedule` replanned with the fastest. Returns
+    {"best": {...}, "table": [...]}."""
+    import torch
+
+    table = []
+    best = None
+    for walk, cs in tuple(candidates or DEFAULT_WALKS):
+        try:
+            schedule.replan(walk=walk, small_cluster=cs)
+            for _ in range(warmup):
+                run()
+            ts = []
+            for _ in range(repeats):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                run()
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ms = min(ts)
+        except BaasError as e:
+            table.append({"walk": walk, "small_cluster": cs, "ms": None, "why": str(e)[:80]})
+            continue
+        table.append({"walk": walk, "small_cluster": cs, "ms": round(ms, 4)})
+        if best is None or ms < best["ms"]:
+            best = {"walk": walk, "small_cluster": cs, "ms": round(ms, 4)}
+    if best is None:
+        raise RuntimeError("no candidate walk runs this schedule")
+    schedule.replan(walk=best["walk"], small_cluster=best["small_cluster"])
     return {"best": best, "table": table}

@@ -1235,10 +1235,58 @@ baas::SmallArgs small_args(const baas_schedule *s, bool full) {
     return a;
 }
 
-// One launch of a single-CTA kernel with `dyn` bytes of dynamic shared memory.
-baas_status launch_small(const void *kern, size_t dyn, void **args, cudaStream_t stream) {
-    BAAS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    BAAS_CUDA(cudaLaunchKernel(kern, dim3(1), dim3(baas::kSmallBlock), args, dyn, stream));
+// The single-CTA walk runs as a cluster of kSmallCluster CTAs (each holding a full copy of the
+// solution) from this many rows up; below it, as one CTA.
+constexpr int kSmallCluster = 8;
+constexpr int kSmallClusterMinRows = 2048;
+
+int small_cs(const baas_schedule *s) {
+    if (s->opt.small_cluster > 0) return s->opt.small_cluster;
+    return s->hs.n >= kSmallClusterMinRows ? kSmallCluster : 1;
+}
+static_assert(baas::kIcScratch <= kSmallMaxDyn, "the IC0 scratch must fit the walk's dynamic shared memory");
+
+// The single-CTA walk's kernels for a cluster size (1, 2, 4 or 8).
+template <int CS>
+const void *small_kernel_cs(int which, bool flag) {
+    switch (which) {
+        case 0: return flag ? (const void *)baas::k_sweep_small<true, CS> : (const void *)baas::k_sweep_small<false, CS>;
+        case 1: return flag ? (const void *)baas::k_iccg_small<float, CS> : (const void *)baas::k_iccg_small<double, CS>;
+        default: return (const void *)baas::k_ic0_small<CS>;
+    }
+}
+// which: 0 sweep (flag = upper), 1 ICCG (flag = FP32 factors), 2 IC0
+const void *small_kernel(int cs, int which, bool flag) {
+    switch (cs) {
+        case 1: return small_kernel_cs<1>(which, flag);
+        case 2: return small_kernel_cs<2>(which, flag);
+        case 4: return small_kernel_cs<4>(which, flag);
+        default: return small_kernel_cs<8>(which, flag);
+    }
+}
+
+// One launch of a single-CTA walk kernel with `dyn` bytes of dynamic shared memory: one CTA
+// (cs = 1), or one cluster of cs CTAs (refused if this device cannot hold such a cluster).
+baas_status launch_small(const void *kern, size_t dyn, void **args, cudaStream_t stream, int cs) {
+    if (dyn > 0) BAAS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(baas::kSmallBlock);
+    cfg.dynamicSmemBytes = dyn;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = cs > 1 ? 1 : 0;
+    if (cs > 1) {
+        int nclusters = 0;
+        BAAS_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg));
+        if (nclusters < 1) return fail(BAAS_ERR_CUDA, "this device cannot hold a cluster of " + std::to_string(cs) + " CTAs");
+    }
+    BAAS_CUDA(cudaLaunchKernelExC(&cfg, kern, args));
     return BAAS_OK;
 }
 
@@ -1483,6 +1531,7 @@ void baas_options_default(baas_options *opt) {
     opt->walk = BAAS_WALK_AUTO;
     opt->analysis = BAAS_ANALYSIS_HOST;
     opt->ablation = BAAS_ABLATION_NONE;
+    opt->small_cluster = 0;
 }
 
 const char *baas_last_error_string(void) { return g_err.c_str(); }
@@ -1514,6 +1563,9 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
         return fail(BAAS_ERR_BAD_ARG, "unknown mapping");
     if (o.analysis != BAAS_ANALYSIS_HOST && o.analysis != BAAS_ANALYSIS_DEVICE)
         return fail(BAAS_ERR_BAD_ARG, "unknown analysis placement");
+    if (o.small_cluster != 0 && o.small_cluster != 1 && o.small_cluster != 2 && o.small_cluster != 4 &&
+        o.small_cluster != 8)
+        return fail(BAAS_ERR_BAD_ARG, "small_cluster must be 0, 1, 2, 4 or 8");
     if (o.ablation < BAAS_ABLATION_NONE || o.ablation > BAAS_ABLATION_WOAS)
         return fail(BAAS_ERR_BAD_ARG, "unknown ablation");
     if (o.ablation != BAAS_ABLATION_NONE && (kind != BAAS_KERNEL_SPTRSV || o.mapping != BAAS_MAPPING_FOUR_RULE))
@@ -2008,6 +2060,9 @@ baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
     if (opt->mapping != s->opt.mapping) return fail(BAAS_ERR_BAD_ARG, "mapping is fixed by the analysis");
     if (opt->parts < 0 || opt->smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "parts and smem_budget must be >= 0");
     if (opt->walk < BAAS_WALK_AUTO || opt->walk > BAAS_WALK_SMALL) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
+    if (opt->small_cluster != 0 && opt->small_cluster != 1 && opt->small_cluster != 2 && opt->small_cluster != 4 &&
+        opt->small_cluster != 8)
+        return fail(BAAS_ERR_BAD_ARG, "small_cluster must be 0, 1, 2, 4 or 8");
     if (opt->partition == BAAS_PARTITION_CUSTOM) {
         if (s->custom_part.empty()) return fail(BAAS_ERR_BAD_ARG, "no custom partition: use baas_replan_custom");
         if (opt->parts != s->opt.parts) return fail(BAAS_ERR_BAD_ARG, "a custom partition fixes parts");
@@ -2060,8 +2115,8 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
         void *args[] = {(void *)&a, (void *)&tcol, (void *)&tval};
         s->last_walk = BAAS_WALK_SMALL;
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-        BAAS_TRY(launch_small(upper ? (const void *)baas::k_sweep_small<true> : (const void *)baas::k_sweep_small<false>,
-                              sizeof(double) * (size_t)n, args, stream));
+        const int cs = small_cs(s);
+        BAAS_TRY(launch_small(small_kernel(cs, 0, upper != 0), sizeof(double) * (size_t)n, args, stream, cs));
         return read_status(s, stream);
     }
     if (walk == BAAS_WALK_LEVELS) {
@@ -2140,7 +2195,7 @@ static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void 
     cudaStream_t stream = (cudaStream_t)stream_;
     int walk = BAAS_WALK_CHUNKED;
     if (!ilu && (s->opt.walk == BAAS_WALK_AUTO || s->opt.walk == BAAS_WALK_SMALL)) BAAS_TRY(pick_walk(s, 8, true, walk));
-    if (walk == BAAS_WALK_SMALL) {  // IC0 by one CTA over the row levels (its shared memory holds no rows)
+    if (walk == BAAS_WALK_SMALL) {  // IC0 by the cluster walk over the row levels (shared memory: the row scratch only)
         BAAS_TRY(upload_small(s, true));
         baas::SmallArgs a = small_args(s, true);
         a.a_rowptr = A->rowptr;
@@ -2148,7 +2203,8 @@ static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void 
         a.lu = lu;
         void *args[] = {(void *)&a};
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-        BAAS_CUDA(cudaLaunchKernel((const void *)baas::k_ic0_small, dim3(1), dim3(baas::kSmallBlock), args, 0, stream));
+        const int cs = small_cs(s);
+        BAAS_TRY(launch_small(small_kernel(cs, 2, false), baas::kIcScratch, args, stream, cs));
         return read_status(s, stream);
     }
     BAAS_TRY(next_epoch(s, stream));
@@ -2452,8 +2508,9 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
         void *args[] = {(void *)&a};
         s->last_walk = BAAS_WALK_SMALL;
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-        BAAS_TRY(launch_small(mixed ? (const void *)baas::k_iccg_small<float> : (const void *)baas::k_iccg_small<double>,
-                              (size_t)n * (8 + (mixed ? 4 : 8)), args, stream));
+        const int cs = small_cs(s);
+        BAAS_TRY(launch_small(small_kernel(cs, 1, mixed), std::max((size_t)n * (8 + (mixed ? 4 : 8)), baas::kIcScratch),
+                              args, stream, cs));
         int it = 0;
         double rr = 0.0;
         BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));

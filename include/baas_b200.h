@@ -120,6 +120,8 @@ typedef struct baas_options {
                          data-parallel stages run; the schedule is identical either way */
     int ablation;     /* BAAS_ABLATION_NONE (default) or, for BAAS_KERNEL_SPTRSV with the four-rule
                          mapping, one of the SpTRSV runtime's ablation schedules */
+    int small_cluster; /* CTAs of BAAS_WALK_SMALL's thread-block cluster: 0 = automatic (8 from
+                         2,048 rows up, else 1), or 1, 2, 4 or 8 */
 } baas_options;
 
 /* The SpTRSV runtime's ablation classes (test/SpTRSV_level_merge.cpp:156-299), kind
@@ -147,10 +149,11 @@ enum { BAAS_ANALYSIS_HOST = 0, BAAS_ANALYSIS_DEVICE = 1 };
  * memory while the CTA's last warp brings other CTAs' results in. LEVELS: one right-hand side;
  * every thread of the launch takes groups of a level and a grid barrier ends the level -- for
  * shallow group DAGs (unstructured or permuted patterns: a few dozen wide levels). SMALL: one
- * right-hand side, one CTA: the whole solution in shared memory (8 bytes a row; ICCG adds p, and
- * z is 8 or 4 bytes), rows by row level with a block barrier per level, the next level's entries
- * loaded while the current one computes -- for systems of up to about 26,000 rows (sweeps) or
- * 13,000 (FP64 ICCG) / 17,000 (FP32 factors); baas_ic0 takes it at any size. AUTO: FETCH wherever
+ * right-hand side, one thread-block cluster of 8 CTAs (one CTA below 2,048 rows), each holding the
+ * whole solution in shared memory (8 bytes a row; ICCG adds p, and z is 8 or 4 bytes); rows by row
+ * level, a row's result stored into every CTA's copy, a cluster barrier per level, the next
+ * level's entries loaded while the current one computes -- for systems of up to about 26,000 rows
+ * (sweeps) or 13,000 (FP64 ICCG) / 17,000 (FP32 factors); baas_ic0 takes it at any size. AUTO: FETCH wherever
  * the plan qualifies and fits shared memory, else SMALL when the system fits it and its row DAG
  * has at most 64 levels each way, else LEVELS when the group DAG has at most 64 levels, else
  * CHUNKED. Sweeps and factors are bit-identical between the walks. */

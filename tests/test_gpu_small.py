@@ -1,5 +1,6 @@
-"""The single-CTA walk (BAAS_WALK_SMALL, baas_b200/csrc/small.cuh) on the GPU: one CTA holds the
-sweep's solution in shared memory and walks the row levels with block barriers.
+"""The single-CTA walk (BAAS_WALK_SMALL, baas_b200/csrc/small.cuh) on the GPU: one CTA, or one
+thread-block cluster whose CTAs each hold the sweep's full solution in shared memory, walks the row
+levels with a barrier per level.
 
   * forward and backward sweeps bit for bit against the oracle (merge/SpTRSV.cpp:24-39, 642-652),
     on a stencil's lower triangle, its transpose, and a k-NN stiffness matrix's IC0 factor;
@@ -7,7 +8,9 @@ sweep's solution in shared memory and walks the row levels with block barriers.
   * ICCG against the oracle's PCG: iterations within one, the solution within 1e-12 relative
     (FP64) / 1e-9 (FP32 factors); the walk is the one the library picks for the k-NN system;
   * the adjoint solve and its gradient against the chunked walk's;
-  * a system too large for one CTA's shared memory is refused when the walk is forced.
+  * a system too large for one CTA's shared memory is refused when the walk is forced;
+  * every cluster size (1, 2, 4, 8) gives the same factor and sweeps; the walk autotuner
+    (autotune.tune_walk) leaves the schedule on its fastest candidate.
 """
 import numpy as np
 import pytest
@@ -110,3 +113,45 @@ def test_forced_small_walk_refuses_a_large_system():
     x = _t(np.zeros(A.n))
     with pytest.raises(BaasError, match="single-CTA"):
         s.iccg(DeviceCSR.from_host(A), _t(gen.uniform_rhs(A.n, 1)), x)
+
+
+@pytest.mark.parametrize("cs", [1, 2, 4, 8])
+def test_every_cluster_size_gives_the_same_factor_and_sweeps(cs):
+    A = gen.knn_stiffness(nodes=1500, k=12, seed=6)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8, walk=WALK_SMALL, small_cluster=cs)
+    dA = DeviceCSR.from_host(A)
+    lu = dA.values.clone()
+    s.ic0(dA, lu)
+    want, _ = Port.ic0(A)
+    assert np.array_equal(lu.cpu().numpy(), want)
+    Lo = gen.CSR(A.n, A.rowptr, A.colidx, want).lower()
+    r = gen.uniform_rhs(A.n, 8)
+    y = _t(np.zeros(A.n))
+    s.forward(DeviceCSR.from_host(Lo), _t(r), y)
+    assert np.array_equal(y.cpu().numpy(), Port.lower_solve(Lo, r))
+    b = gen.uniform_rhs(A.n, 9)
+    xo, ito, _ = Port.pcg(A, b, tol=1e-10)
+    x = _t(np.zeros(A.n))
+    it, rel = s.iccg(dA, _t(b), x, tol=1e-10)
+    assert abs(it - ito) <= 1 and np.linalg.norm(x.cpu().numpy() - xo) / np.linalg.norm(xo) <= 1e-12
+
+
+def test_walk_autotuner_leaves_the_fastest_walk():
+    from baas_b200 import autotune
+
+    A = gen.knn_stiffness(nodes=1000, k=12, seed=3)
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    dA = DeviceCSR.from_host(A)
+    b = _t(gen.uniform_rhs(A.n, 1))
+    x = _t(np.zeros(A.n))
+
+    def run():
+        x.zero_()
+        s.iccg(dA, b, x, tol=1e-10)
+
+    out = autotune.tune_walk(s, run)
+    ran = [r for r in out["table"] if r["ms"] is not None]
+    assert min(r["ms"] for r in ran) == out["best"]["ms"]
+    assert any(r["ms"] is None for r in out["table"])  # the fetch walk refuses the k-NN rows
+    run()
+    assert s.last_walk == out["best"]["walk"]
