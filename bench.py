@@ -510,7 +510,29 @@ def c2_variants(flush):
     out["c2_permuted"] = _iccg_case("iccg_laplace3d_64_shift1e-3_permuted", P, gen.uniform_rhs(P.n, 1), flush)
     K = gen.knn_stiffness(nodes=4000, k=12, seed=3)
     out["c2_knn"] = _iccg_case("iccg_knn_stiffness_4000_nodes_k12", K, gen.uniform_rhs(K.n, 1), flush)
+    out["c2_knn"]["walk_table"] = _walk_table(K, gen.uniform_rhs(K.n, 1))
     return out
+
+
+def _walk_table(A, b_h):
+    """The same FP64 ICCG under every sweep walk and cluster size (autotune.tune_walk): best of
+    three CUDA-event timings after a warm-up, per candidate."""
+    import torch
+
+    from baas_b200 import KERNEL_ICCG, DeviceCSR, Schedule, autotune
+
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=8)
+    dA = DeviceCSR.from_host(A)
+    b = torch.from_numpy(b_h).cuda()
+    x = torch.zeros_like(b)
+
+    def run():
+        x.zero_()
+        s.iccg(dA, b, x, tol=TOL, maxiter=MAXITER)
+
+    names = {1: "chunked", 2: "fetch", 3: "levels", 4: "cluster"}
+    table = autotune.tune_walk(s, run, repeats=3)["table"]
+    return [{"walk": names[r["walk"]], "ctas": r["small_cluster"] or None, "ms": r["ms"]} for r in table]
 
 
 def c5_adjoint():
@@ -864,6 +886,14 @@ def profile_case(args):
         Xb = torch.zeros_like(Bb)
         run = lambda: (Xb.zero_(), sb.iccg_batched(dB, Bb, Xb, tol=TOL, maxiter=20000,  # noqa: E731
                                                     precision=PREC_FP32_FACTORS))
+    elif case == "knn_iccg":
+        # the k-NN stiffness matrix (n = 12,000): the cluster walk the library picks for it
+        K = gen.knn_stiffness(nodes=4000)
+        sk = Schedule(K, kind=KERNEL_ICCG, nthread=8)
+        dK = DeviceCSR.from_host(K)
+        bk = torch.from_numpy(gen.uniform_rhs(K.n, gen.C2_RHS_SEED)).cuda()
+        xk = torch.zeros_like(bk)
+        run = lambda: (xk.zero_(), sk.iccg(dK, bk, xk, tol=TOL, maxiter=MAXITER, precision=PREC_FP64))  # noqa: E731
     elif case == "ic0":
         lu = dA.values.clone()
         run = lambda: (lu.copy_(dA.values), s.ic0(dA, lu))  # noqa: E731
@@ -893,7 +923,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true", help="skip the other configurations")
     ap.add_argument("--profile-case", default=None,
-                    choices=["iccg", "iccg_fp32", "ic0", "sweep_lower", "sweep_upper", "batched_small"],
+                    choices=["iccg", "iccg_fp32", "ic0", "sweep_lower", "sweep_upper", "batched_small", "knn_iccg"],
                     help="run one kernel of the workload only (for ncu captures)")
     args = ap.parse_args()
     global CPU_BASELINES
