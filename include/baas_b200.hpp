@@ -214,6 +214,7 @@ class RuntimeBase {
         baas_options o;
         baas_options_default(&o);
         o.nthread = num_thread_;
+        o.ablation = ablation_;
         baas_destroy(s_);
         s_ = nullptr;
         detail::check(baas_analyze(&pattern, kind, &o, &s_), alg_name_.c_str());
@@ -235,6 +236,7 @@ class RuntimeBase {
     }
     baas_schedule *s_ = nullptr;
     int num_test_ = 10, num_thread_ = 8;
+    int ablation_ = BAAS_ABLATION_NONE;
     double analysis_time_ = 0.0, elapsed_time_ = 0.0, max_error_ = 0.0;
     std::string alg_name_;
 };
@@ -244,12 +246,15 @@ class RuntimeBase {
 template <typename CSR>
 class SpTRSVRuntime : public RuntimeBase {
    public:
+    // ablation: BAAS_ABLATION_NONE for SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule, or one of the
+    // ablation classes' schedules (the aliases below)
     SpTRSVRuntime(const CSR *csrL, const double *correct_x, int n, int nnz, double alpha, std::string algName,
-                  int num_thread)
+                  int num_thread, int ablation = BAAS_ABLATION_NONE)
         : L_(csrL), correct_x_(correct_x), n_(n), alpha_(alpha), x_(n, 0.0), b_(n, 0.0) {
         (void)nnz;
         alg_name_ = std::move(algName);
         num_thread_ = num_thread;
+        ablation_ = ablation;
     }
     const double *getSolution() const { return x_.data(); }
 
@@ -287,6 +292,32 @@ class SpTRSVRuntime : public RuntimeBase {
     baas_csr t_{};
     detail::DevCsr dL_;
     detail::DevBuf<double> db_, dx_;
+};
+
+// The SpTRSV runtime's ablation classes (test/SpTRSV_level_merge.cpp:156-299), same constructor
+// as the reference's: BAASWOS (test/SpTRSVRuntime.hpp:389-615), BAASWOAS (:855-1054), BAASWOA
+// (:1056-1262). Their schedules are the reference classes' array for array; the sweep is the GPU's.
+template <typename CSR>
+class SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P : public SpTRSVRuntime<CSR> {
+   public:
+    SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P(const CSR *csrL, const double *correct_x, int n, int nnz, double alpha,
+                                      std::string algName, int num_thread)
+        : SpTRSVRuntime<CSR>(csrL, correct_x, n, nnz, alpha, std::move(algName), num_thread, BAAS_ABLATION_WOS) {}
+};
+template <typename CSR>
+class SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRuleAblationBase : public SpTRSVRuntime<CSR> {
+   public:
+    SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRuleAblationBase(const CSR *csrL, const double *correct_x, int n, int nnz,
+                                                              double alpha, std::string algName, int num_thread)
+        : SpTRSVRuntime<CSR>(csrL, correct_x, n, nnz, alpha, std::move(algName), num_thread, BAAS_ABLATION_WOAS) {}
+};
+template <typename CSR>
+class SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRuleAblationWOAggregation : public SpTRSVRuntime<CSR> {
+   public:
+    SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRuleAblationWOAggregation(const CSR *csrL, const double *correct_x, int n,
+                                                                       int nnz, double alpha, std::string algName,
+                                                                       int num_thread)
+        : SpTRSVRuntime<CSR>(csrL, correct_x, n, nnz, alpha, std::move(algName), num_thread, BAAS_ABLATION_WOA) {}
 };
 
 // IC_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRule (test/ICRuntime.hpp:353-583) and

@@ -158,6 +158,20 @@ int main(int argc, char **argv) {
     sp.set_num_test(3);
     sp.evaluate();
     if (!(sp.getMaxError() < 1e-10)) return fail("SpTRSVRuntime");
+    // the reference's ablation classes: their schedules, the same sweep result
+    baas_b200::SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P<CSR> wos(&L, xtrue.data(), n, L.rp[n], 1.0, "BAASWOS", 8);
+    baas_b200::SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRuleAblationWOAggregation<CSR> woa(&L, xtrue.data(), n, L.rp[n],
+                                                                                          1.0, "BAASWOA", 8);
+    baas_b200::SpTRSV_DUAL_TREE_BFS_WF_Merge_P2P_MapFourRuleAblationBase<CSR> woas(&L, xtrue.data(), n, L.rp[n], 1.0,
+                                                                                  "BAASWOAS", 8);
+    baas_b200::SpTRSVRuntime<CSR> *abl[3] = {&wos, &woa, &woas};
+    for (auto *r : abl) {
+        r->set_num_test(2);
+        r->evaluate();
+        if (!(r->getMaxError() < 1e-10)) return fail(r->getAlgName().c_str());
+        for (int i = 0; i < n; i++)
+            if (r->getSolution()[i] != sp.getSolution()[i]) return fail("ablation sweep differs from BAAS's");
+    }
     baas_b200::ICRuntime<CSR> ic(&A, want.data(), n, nnz, "BAAS-B200-IC0", 8);
     ic.set_num_test(3);
     ic.evaluate();
