@@ -7,6 +7,7 @@
 // each CTA walks its rows in the global order (part_kernels.cuh). The backward sweep uses the
 // exact reverse order. The plan is uploaded on the first GPU call, to the current device.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <climits>
@@ -1541,11 +1542,21 @@ const char *baas_last_error_string(void) { return g_err.c_str(); }
 // error reporting for the library's other host sources (mtx.cpp)
 baas_status baas::set_error(baas_status code, const std::string &msg) { return fail(code, msg); }
 
+// NVTX ranges named after the reference's phase timers (pcg_opt, test/iccg_level_merge.cpp:384-521:
+// pre, ic, trsv, ... ) around each entry point, for a profiler's timeline; free without one.
+struct PhaseRange {
+    explicit PhaseRange(const char *name) { nvtxRangePushA(name); }
+    ~PhaseRange() { nvtxRangePop(); }
+    PhaseRange(const PhaseRange &) = delete;
+    PhaseRange &operator=(const PhaseRange &) = delete;
+};
+
 extern "C" {
 
 const char *baas_version(void) { return "baas_b200 0.2.0 (sm_100a)"; }
 
 baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options *opt, baas_schedule **out) {
+    PhaseRange range("pre");
     if (!A || !out) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     *out = nullptr;
     if (kind < BAAS_KERNEL_SPTRSV || kind > BAAS_KERNEL_ILU0) return fail(BAAS_ERR_BAD_ARG, "unknown kernel kind");
@@ -2095,6 +2106,7 @@ baas_status baas_replan_custom(baas_schedule *s, const int *row_part, int parts,
 
 baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const double *b, double *x, int nrhs, int ldb,
                         void *stream_) {
+    PhaseRange range("trsv");
     if (!s || !b || !x) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     const int n = s->hs.n;
     if (!csr_ok(T, n, s->nnz_l)) return fail(BAAS_ERR_BAD_ARG, "triangular factor does not match the analysed pattern");
@@ -2187,6 +2199,7 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
 }
 
 static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void *stream_, bool ilu) {
+    PhaseRange range(ilu ? "ilu" : "ic");
     if (!s || !lu) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     if (s->hs.kind == baas::SchedKind::SpTRSV) return fail(BAAS_ERR_STATE, "a SpTRSV schedule cannot drive a factorisation");
     if (!A || A->n != s->hs.n || A->nnz != s->nnz_a || !A->rowptr || !A->colidx)
@@ -2374,6 +2387,7 @@ static baas_status batch_setup(baas_schedule *s, int R) {
 
 baas_status baas_iccg_batched(baas_schedule *s, const baas_csr *A, const double *B, double *X, int nrhs, int ldb,
                               double tol, int maxiter, int precision, int *iters, double *relres, void *stream_) {
+    PhaseRange range("pcg_batched");
     if (!s || !B || !X || !iters || !relres) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     if (s->nsys < 1) return fail(BAAS_ERR_STATE, "the schedule was not made by baas_analyze_batch");
     if (!csr_ok(A, s->hs.n, s->nnz_a)) return fail(BAAS_ERR_BAD_ARG, "matrix does not match the analysed pattern");
@@ -2633,6 +2647,7 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
 
 baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, double *x, double tol, int maxiter,
                       int precision, int *iters, double *relres, void *stream) {
+    PhaseRange range("pcg");
     return iccg_launch(s, A, b, x, tol, maxiter, precision, iters, relres, stream, false, nullptr, nullptr);
 }
 
@@ -2642,6 +2657,7 @@ baas_status baas_iccg(baas_schedule *s, const baas_csr *A, const double *b, doub
 baas_status baas_iccg_adjoint(baas_schedule *s, const baas_csr *A, const double *g, double *lambda, const double *x,
                               double *grad_a, double tol, int maxiter, int precision, int *iters, double *relres,
                               void *stream_) {
+    PhaseRange range("pcg_adjoint");
     if (!s || !g || !lambda) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     if ((x == nullptr) != (grad_a == nullptr)) return fail(BAAS_ERR_BAD_ARG, "x and grad_a go together");
     if (s->factor_prec != precision)
