@@ -1555,7 +1555,18 @@ extern "C" {
 
 const char *baas_version(void) { return "baas_b200 0.2.0 (sm_100a)"; }
 
+static baas_status analyze_common(const baas_csr *A, baas_kernel kind, const baas_options *opt, baas_schedule **out,
+                                  const std::vector<int> *sys_off);
+
 baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options *opt, baas_schedule **out) {
+    return analyze_common(A, kind, opt, out, nullptr);
+}
+
+}  // extern "C"
+
+// sys_off: row offsets of a block-diagonal batch (baas_analyze_batch), or nullptr
+static baas_status analyze_common(const baas_csr *A, baas_kernel kind, const baas_options *opt, baas_schedule **out,
+                                  const std::vector<int> *sys_off) {
     PhaseRange range("pre");
     if (!A || !out) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
     *out = nullptr;
@@ -1604,7 +1615,7 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     }
     std::string reason;
     if (!baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping,
-                              (baas::Ablation)o.ablation, dev, reason)) {
+                              (baas::Ablation)o.ablation, dev, reason, sys_off)) {
         delete s;
         return fail(dev && reason.rfind("device analysis", 0) == 0 ? BAAS_ERR_CUDA : BAAS_ERR_BAD_ARG, reason);
     }
@@ -1617,6 +1628,8 @@ baas_status baas_analyze(const baas_csr *A, baas_kernel kind, const baas_options
     *out = s;
     return BAAS_OK;
 }
+
+extern "C" {
 
 int baas_schedule_export(const baas_schedule *s, int field, int *out) {
     if (!s) return -1;
@@ -2320,8 +2333,9 @@ baas_status baas_analyze_batch(const baas_csr *A, const int *sys_off, int nsys, 
                 if (A->colidx[e] < sys_off[k] || A->colidx[e] >= sys_off[k + 1])
                     return fail(BAAS_ERR_BAD_ARG, "an entry couples two systems (the pattern must be block diagonal)");
     }
-    BAAS_TRY(baas_analyze(A, BAAS_KERNEL_ICCG, opt, out));
-    (*out)->sys_off.assign(sys_off, sys_off + nsys + 1);
+    const std::vector<int> offsets(sys_off, sys_off + nsys + 1);
+    BAAS_TRY(analyze_common(A, BAAS_KERNEL_ICCG, opt, out, &offsets));
+    (*out)->sys_off = offsets;
     (*out)->nsys = nsys;
     return BAAS_OK;
 }

@@ -7,6 +7,7 @@
 #include "schedule.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -15,6 +16,7 @@
 #include <limits>
 #include <memory>
 #include <numeric>
+#include <thread>
 #include <unordered_set>
 
 namespace baas {
@@ -224,6 +226,96 @@ void level_sets(const Csx &dag, HostSchedule &s) {
     s.perm_to_orig.assign(q.begin(), q.begin() + n);
     s.perm.assign(n, 0);
     for (int i = 0; i < n; i++) s.perm[s.perm_to_orig[i]] = i;
+}
+
+// Stages 2-7 of a block-diagonal pattern (systems at rows off[q] .. off[q + 1]), system by system on
+// host threads, concatenated into s (groups, their rows, the final group DAG, the level set) and
+// fdag. No DAG edge joins two systems, so every stage restricted to one system is that system's own:
+// a tree grows from a root of its system, and each system's roots are visited in the same relative
+// order as in the whole pattern's BFS (initial roots ascending, then appended roots in discovery
+// order); relabel_groups orders groups by a representative row, which keeps the systems in row
+// order; the Kahn levels of independent DAGs are the unions of their levels, nodes ascending. The
+// concatenation is therefore identical to the whole pattern's stages 2-7.
+void split_stages(HostSchedule &s, const std::vector<int> &off, Csx &fdag) {
+    const int ns = (int)off.size() - 1;
+    struct Part {
+        std::vector<int> gptr, gset;
+        Csx fdag;
+        HostSchedule lv;
+    };
+    std::vector<Part> parts(ns);
+    auto work = [&](int q) {
+        const int r0 = off[q], m = off[q + 1] - off[q];
+        const int e0 = s.l_rowptr[r0];
+        Csx lower;
+        lower.ptr.resize(m + 1);
+        for (int i = 0; i <= m; i++) lower.ptr[i] = s.l_rowptr[r0 + i] - e0;
+        lower.idx.resize(lower.ptr[m]);
+        for (int e = 0; e < lower.ptr[m]; e++) lower.idx[e] = s.l_colidx[e0 + e] - r0;
+        const Csx dag = two_hop_reduce(transpose(lower));
+        const Grouping rev = tree_coarsen(dag, true);
+        const Csx gdag = group_dag(m, rev, dag);
+        const Grouping fwd = tree_coarsen(gdag, false);
+        Part &P = parts[q];
+        P.gptr.assign(1, 0);
+        for (int f = 0; f < fwd.ngroups; f++) {
+            for (int t = fwd.ptr[f]; t < fwd.ptr[f + 1]; t++) {
+                const int g = fwd.set[t];
+                for (int e = rev.ptr[g]; e < rev.ptr[g + 1]; e++) P.gset.push_back(rev.set[e] + r0);
+            }
+            P.gptr.push_back((int)P.gset.size());
+        }
+        P.fdag = group_dag(rev.ngroups, fwd, gdag);
+        level_sets(P.fdag, P.lv);
+    };
+    const int nt = std::max(1, std::min<int>(ns, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next(0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; t++)
+        pool.emplace_back([&] {
+            for (int q = next++; q < ns; q = next++) work(q);
+        });
+    for (auto &t : pool) t.join();
+
+    std::vector<int> goff(ns + 1, 0);
+    int nlev = 0;
+    for (int q = 0; q < ns; q++) {
+        goff[q + 1] = goff[q] + (int)parts[q].gptr.size() - 1;
+        nlev = std::max(nlev, parts[q].lv.nlevels);
+    }
+    const int ng = goff[ns];
+    s.ngroups = ng;
+    s.group_ptr.assign(1, 0);
+    s.group_set.clear();
+    fdag.ptr.assign(1, 0);
+    fdag.idx.clear();
+    s.node_to_level.clear();
+    for (int q = 0; q < ns; q++) {
+        const Part &P = parts[q];
+        const int base = (int)s.group_set.size();
+        for (size_t g = 1; g < P.gptr.size(); g++) s.group_ptr.push_back(base + P.gptr[g]);
+        s.group_set.insert(s.group_set.end(), P.gset.begin(), P.gset.end());
+        for (int g = 0; g + 1 < (int)P.fdag.ptr.size(); g++) {
+            for (int e = P.fdag.ptr[g]; e < P.fdag.ptr[g + 1]; e++) fdag.idx.push_back(P.fdag.idx[e] + goff[q]);
+            fdag.ptr.push_back((int)fdag.idx.size());
+        }
+        s.node_to_level.insert(s.node_to_level.end(), P.lv.node_to_level.begin(), P.lv.node_to_level.end());
+    }
+    s.nlevels = nlev;
+    s.level_ptr.assign(nlev + 1, 0);
+    s.perm_to_orig.clear();
+    s.perm_to_orig.reserve(ng);
+    for (int l = 0; l < nlev; l++) {
+        for (int q = 0; q < ns; q++) {
+            const HostSchedule &L = parts[q].lv;
+            if (l >= L.nlevels) continue;
+            for (int p = L.level_ptr[l]; p < L.level_ptr[l + 1]; p++) s.perm_to_orig.push_back(L.perm_to_orig[p] + goff[q]);
+        }
+        s.level_ptr[l + 1] = (int)s.perm_to_orig.size();
+    }
+    s.exec_level_ptr = s.level_ptr;
+    s.perm.assign(ng, 0);
+    for (int i = 0; i < ng; i++) s.perm[s.perm_to_orig[i]] = i;
 }
 
 // Stage 8: merge/LevelMerge.cpp:118-262.
@@ -518,6 +610,12 @@ void four_rule_map(HostSchedule &s, const Csx &dag_csr) {
     std::vector<int> aff_thr;
     std::vector<double> aff_val, aff_total;
     const double pen0 = kLoadBeta * std::log(1.0 + (1.0 - 0.0));
+    // the vote's two logarithms, computed once per group and per level distance (the same calls
+    // on the same arguments give the same values)
+    std::vector<double> log_size(nodes);
+    for (int g = 0; g < nodes; g++) log_size[g] = std::log2(1.0 * (s.group_ptr[g + 1] - s.group_ptr[g] + 1));
+    double log_diff[kLevelWindow + 1];
+    for (int d = 0; d <= kLevelWindow; d++) log_diff[d] = std::log2(d + 1);
 
     for (int lvl = 1; lvl < nl; lvl++) {
         const int lb = lp[lvl], le = lp[lvl + 1];
@@ -553,8 +651,7 @@ void four_rule_map(HostSchedule &s, const Csx &dag_csr) {
                     const int rt = node_thread[par];
                     const int diff = nlev - s.node_to_level[par];
                     if (diff > kLevelWindow) continue;
-                    const double vote = kAmplify * std::log2(1.0 * (s.group_ptr[par + 1] - s.group_ptr[par] + 1)) /
-                                        std::log2(diff + 1);
+                    const double vote = kAmplify * log_size[par] / log_diff[diff];
                     if (!in_touched[rt]) {
                         in_touched[rt] = 1;
                         part[rt] = 0.0;
@@ -963,9 +1060,11 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
 }
 
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
-                    Mapping mapping, Ablation ablation, bool device, std::string &why) {
+                    Mapping mapping, Ablation ablation, bool device, std::string &why, const std::vector<int> *sys_off) {
     // BAASWOA and BAASWOAS leave the rows ungrouped: one group per row on the two-hop DAG
     const bool aggregate = ablation == Ablation::None || ablation == Ablation::WOS;
+    // a block-diagonal batch: stages 2-7 system by system on host threads
+    const bool split = sys_off && sys_off->size() > 2 && !device && aggregate;
     auto t0 = std::chrono::steady_clock::now();
     // BAAS_ANALYSIS_TRACE=1: stage times of the analysis on stderr
     const bool trace = getenv("BAAS_ANALYSIS_TRACE") && atoi(getenv("BAAS_ANALYSIS_TRACE")) > 0;
@@ -1050,6 +1149,9 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         D->download(df, fdag.ptr, fdag.idx);
         if (!D->ok()) return dev_failed();
         stage("group DAG of the forward groups (device)");
+    } else if (split) {
+        split_stages(s, *sys_off, fdag);
+        stage("stages 2-7 per system (host threads)");
     } else {
         Csx lower{s.l_rowptr, s.l_colidx};
         Csx dag0 = transpose(lower);  // column j: j itself, then the rows that depend on j
@@ -1065,7 +1167,9 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
             fdag = dag;
         }
     }
-    if (aggregate) {
+    if (split) {
+        // groups, group DAG and level set already concatenated
+    } else if (aggregate) {
         // remap forward groups (of reverse groups) onto rows (merge/Coarsen.cpp:896-928)
         s.ngroups = fwd.ngroups;
         s.group_ptr.assign(1, 0);
@@ -1114,7 +1218,7 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
         for (int i = 0; i < s.ngroups; i++) s.perm[s.perm_to_orig[i]] = i;
         D.reset();
         stage("level sets + inverse DAG (device)");
-    } else {
+    } else if (!split) {
         level_sets(fdag, s);  // stage 7
         stage("level sets");
     }

@@ -114,10 +114,13 @@ private:
 };
 
 // Runs stages 1-10. `rowptr`/`colidx` are host arrays of the analysed matrix. With `device`, the
-// stages DeviceStages covers run on the current CUDA device; the schedule is the same. False with
-// `why` set when the affinity mapping would leave a group unmapped (the reference's P2P_MAPPING
-// scan can) or a device stage failed.
+// stages DeviceStages covers run on the current CUDA device; the schedule is the same. With
+// `sys_off` (the row offsets of a block-diagonal batch, no entry coupling two systems), stages 2-7
+// run system by system on host threads; the schedule is again the same. False with `why` set when
+// the affinity mapping would leave a group unmapped (the reference's P2P_MAPPING scan can) or a
+// device stage failed.
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
-                    Mapping mapping, Ablation ablation, bool device, std::string &why);
+                    Mapping mapping, Ablation ablation, bool device, std::string &why,
+                    const std::vector<int> *sys_off = nullptr);
 
 }  // namespace baas
