@@ -85,7 +85,7 @@ class Schedule:
     def __init__(self, A: CSR, kind: int = KERNEL_ICCG, nthread: int = 8, spin_limit: int = 0,
                  parts: int = 0, partition: int = PARTITION_AUTO, smem_budget: int = 0, mapping: int = 0,
                  walk: int = 0, analysis: int = ANALYSIS_HOST, ablation: int = ABLATION_NONE,
-                 small_cluster: int = 0):
+                 small_cluster: int = 0, scoring: dict | None = None):
         L = _native.lib()
         self._rowptr = np.ascontiguousarray(A.rowptr, dtype=np.int32)
         self._colidx = np.ascontiguousarray(A.colidx, dtype=np.int32)
@@ -102,6 +102,12 @@ class Schedule:
         opt.analysis = analysis
         opt.ablation = ablation
         opt.small_cluster = small_cluster
+        # the four-rule mapping's scoring constants (level_window, amplify, over_gamma,
+        # award_alpha, load_beta); unnamed ones keep the reference's values
+        for key, val in (scoring or {}).items():
+            if key not in ("level_window", "amplify", "over_gamma", "award_alpha", "load_beta"):
+                raise KeyError(key)
+            setattr(opt, key, val)
         h = C.c_void_p()
         _native.check(L.baas_analyze(C.byref(c), kind, C.byref(opt), C.byref(h)), "baas_analyze")
         self._h = h

@@ -59,7 +59,8 @@ class BaasOptions(C.Structure):
     _fields_ = [("nthread", C.c_int), ("spin_limit", C.c_int), ("parts", C.c_int),
                 ("partition", C.c_int), ("smem_budget", C.c_int), ("mapping", C.c_int), ("walk", C.c_int),
                 ("analysis", C.c_int), ("ablation", C.c_int),
-                ("small_cluster", C.c_int)]
+                ("small_cluster", C.c_int), ("level_window", C.c_int), ("amplify", C.c_double),
+                ("over_gamma", C.c_double), ("award_alpha", C.c_double), ("load_beta", C.c_double)]
 
 
 class BaasError(RuntimeError):

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <map>
 #include <mutex>
 #include <cstdio>
@@ -1533,6 +1534,12 @@ void baas_options_default(baas_options *opt) {
     opt->analysis = BAAS_ANALYSIS_HOST;
     opt->ablation = BAAS_ABLATION_NONE;
     opt->small_cluster = 0;
+    const baas::ScoreParams sp;
+    opt->level_window = sp.level_window;
+    opt->amplify = sp.amplify;
+    opt->over_gamma = sp.over_gamma;
+    opt->award_alpha = sp.award_alpha;
+    opt->load_beta = sp.load_beta;
 }
 
 const char *baas_last_error_string(void) { return g_err.c_str(); }
@@ -1588,6 +1595,9 @@ static baas_status analyze_common(const baas_csr *A, baas_kernel kind, const baa
     if (o.small_cluster != 0 && o.small_cluster != 1 && o.small_cluster != 2 && o.small_cluster != 4 &&
         o.small_cluster != 8)
         return fail(BAAS_ERR_BAD_ARG, "small_cluster must be 0, 1, 2, 4 or 8");
+    if (o.level_window < 0 || o.level_window > 1024 || !std::isfinite(o.amplify) || !std::isfinite(o.over_gamma) ||
+        !std::isfinite(o.award_alpha) || !std::isfinite(o.load_beta))
+        return fail(BAAS_ERR_BAD_ARG, "scoring constants: level_window in [0, 1024] and finite weights");
     if (o.ablation < BAAS_ABLATION_NONE || o.ablation > BAAS_ABLATION_WOAS)
         return fail(BAAS_ERR_BAD_ARG, "unknown ablation");
     if (o.ablation != BAAS_ABLATION_NONE && (kind != BAAS_KERNEL_SPTRSV || o.mapping != BAAS_MAPPING_FOUR_RULE))
@@ -1614,8 +1624,14 @@ static baas_status analyze_common(const baas_csr *A, baas_kernel kind, const baa
         }
     }
     std::string reason;
+    baas::ScoreParams score;
+    score.level_window = o.level_window;
+    score.amplify = o.amplify;
+    score.over_gamma = o.over_gamma;
+    score.award_alpha = o.award_alpha;
+    score.load_beta = o.load_beta;
     if (!baas::build_schedule(s->hs, A->n, A->rowptr, A->colidx, sk, o.nthread, (baas::Mapping)o.mapping,
-                              (baas::Ablation)o.ablation, dev, reason, sys_off)) {
+                              (baas::Ablation)o.ablation, dev, reason, sys_off, score)) {
         delete s;
         return fail(dev && reason.rfind("device analysis", 0) == 0 ? BAAS_ERR_CUDA : BAAS_ERR_BAD_ARG, reason);
     }

@@ -22,12 +22,6 @@
 namespace baas {
 namespace {
 
-// Tuning constants of the four-rule mapper, merge/include/MergeMarco.hpp:5-23.
-constexpr int kLevelWindow = 6;
-constexpr double kAmplify = 2.0;
-constexpr double kOverGamma = 6.0;
-constexpr double kAwardAlpha = 1.0;
-constexpr double kLoadBeta = 0.1;
 
 struct Csx {  // compressed sparse rows or columns
     std::vector<int> ptr, idx;
@@ -609,13 +603,14 @@ void four_rule_map(HostSchedule &s, const Csx &dag_csr) {
     std::vector<int> aff_ptr;
     std::vector<int> aff_thr;
     std::vector<double> aff_val, aff_total;
-    const double pen0 = kLoadBeta * std::log(1.0 + (1.0 - 0.0));
+    const ScoreParams &sp = s.score;
+    const double pen0 = sp.load_beta * std::log(1.0 + (1.0 - 0.0));
     // the vote's two logarithms, computed once per group and per level distance (the same calls
     // on the same arguments give the same values)
     std::vector<double> log_size(nodes);
     for (int g = 0; g < nodes; g++) log_size[g] = std::log2(1.0 * (s.group_ptr[g + 1] - s.group_ptr[g] + 1));
-    double log_diff[kLevelWindow + 1];
-    for (int d = 0; d <= kLevelWindow; d++) log_diff[d] = std::log2(d + 1);
+    std::vector<double> log_diff(std::max(sp.level_window, 0) + 1);
+    for (int d = 0; d <= std::max(sp.level_window, 0); d++) log_diff[d] = std::log2(d + 1);
 
     for (int lvl = 1; lvl < nl; lvl++) {
         const int lb = lp[lvl], le = lp[lvl + 1];
@@ -650,8 +645,8 @@ void four_rule_map(HostSchedule &s, const Csx &dag_csr) {
                     const int par = dag_csr.idx[q];
                     const int rt = node_thread[par];
                     const int diff = nlev - s.node_to_level[par];
-                    if (diff > kLevelWindow) continue;
-                    const double vote = kAmplify * log_size[par] / log_diff[diff];
+                    if (diff > sp.level_window) continue;
+                    const double vote = sp.amplify * log_size[par] / log_diff[diff];
                     if (!in_touched[rt]) {
                         in_touched[rt] = 1;
                         part[rt] = 0.0;
@@ -697,7 +692,7 @@ void four_rule_map(HostSchedule &s, const Csx &dag_csr) {
                         a = aff_val[q];
                         break;
                     }
-                score[t] = kAwardAlpha * (a / total) + penalty[t];
+                score[t] = sp.award_alpha * (a / total) + penalty[t];
                 if (score[t] > best) {
                     best = score[t];
                     target = t;
@@ -708,11 +703,11 @@ void four_rule_map(HostSchedule &s, const Csx &dag_csr) {
             const double util = local_load[target] / avg;
             double pen;
             if (util < 1.0)
-                pen = kLoadBeta * std::log(1.0 + (1.0 - util));
+                pen = sp.load_beta * std::log(1.0 + (1.0 - util));
             else if (util > 1.05)
                 pen = std::numeric_limits<double>::lowest();
             else
-                pen = -kOverGamma * (std::exp(10 * (util - 1)) - 1);
+                pen = -sp.over_gamma * (std::exp(10 * (util - 1)) - 1);
             penalty[target] = pen;
         }
 
@@ -905,9 +900,9 @@ bool affinity_map(HostSchedule &s, const Csx &dag_csr) {
             for (int q = dag_csr.ptr[node]; q < dag_csr.ptr[node + 1] - 1; q++) {
                 const int par = dag_csr.idx[q];
                 const int diff = nlev - n2l[par];
-                if (diff < kLevelWindow)
+                if (diff < s.score.level_window)
                     node_score[node_thread[par]] +=
-                        kAmplify * std::log2(1.0 * (s.group_ptr[par + 1] - s.group_ptr[par] + 1)) / std::log2(1.0 * (diff + 1));
+                        s.score.amplify * std::log2(1.0 * (s.group_ptr[par + 1] - s.group_ptr[par] + 1)) / std::log2(1.0 * (diff + 1));
             }
             std::iota(tidx.begin(), tidx.end(), 0);
             std::partial_sort(tidx.begin(), tidx.begin() + sw, tidx.end(), [&](int a, int b) { return node_score[a] > node_score[b]; });
@@ -1060,7 +1055,8 @@ const char *validate_pattern(int n, const int *rowptr, const int *colidx, SchedK
 }
 
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
-                    Mapping mapping, Ablation ablation, bool device, std::string &why, const std::vector<int> *sys_off) {
+                    Mapping mapping, Ablation ablation, bool device, std::string &why, const std::vector<int> *sys_off,
+                    const ScoreParams &score) {
     // BAASWOA and BAASWOAS leave the rows ungrouped: one group per row on the two-hop DAG
     const bool aggregate = ablation == Ablation::None || ablation == Ablation::WOS;
     // a block-diagonal batch: stages 2-7 system by system on host threads
@@ -1077,6 +1073,7 @@ bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx
     };
     s = HostSchedule();
     s.kind = kind;
+    s.score = score;
     s.n = n;
     s.nthread = nthread;
     const int nnz = rowptr[n];

@@ -23,8 +23,21 @@ namespace baas {
 
 enum class SchedKind { SpTRSV = 0, ICCG = 1, IC0 = 2, ILU0 = 3 };
 
+// The four-rule mapper's scoring constants, the reference's compile-time macros
+// (merge/include/MergeMarco.hpp:5-23: LEVEL_WINDOW_SIZE, AMPLIFY_FACTOR, OVER_REGULARIZATION_GMMA,
+// AWARD_ALPHA, LOAD_REGULARIZATION_BETA); the defaults are the reference's values. The affinity
+// mapping (P2P_MAPPING) reads the window and the amplification too.
+struct ScoreParams {
+    int level_window = 6;
+    double amplify = 2.0;
+    double over_gamma = 6.0;
+    double award_alpha = 1.0;
+    double load_beta = 0.1;
+};
+
 struct HostSchedule {
     SchedKind kind = SchedKind::ICCG;
+    ScoreParams score;
     int n = 0;
     int nthread = 1;
 
@@ -121,6 +134,6 @@ private:
 // device stage failed.
 bool build_schedule(HostSchedule &s, int n, const int *rowptr, const int *colidx, SchedKind kind, int nthread,
                     Mapping mapping, Ablation ablation, bool device, std::string &why,
-                    const std::vector<int> *sys_off = nullptr);
+                    const std::vector<int> *sys_off = nullptr, const ScoreParams &score = ScoreParams());
 
 }  // namespace baas

@@ -122,6 +122,14 @@ typedef struct baas_options {
                          mapping, one of the SpTRSV runtime's ablation schedules */
     int small_cluster; /* CTAs of BAAS_WALK_SMALL's thread-block cluster: 0 = automatic (8 from
                          2,048 rows up, else 1), or 1, 2, 4 or 8 */
+    /* The four-rule mapping's scoring constants, the reference's compile-time macros
+     * (merge/include/MergeMarco.hpp:5-23); baas_options_default sets the reference's values.
+     * The affinity mapping (BAAS_MAPPING_AFFINITY) reads level_window and amplify. */
+    int level_window;   /* LEVEL_WINDOW_SIZE: parents more levels up than this do not vote (6) */
+    double amplify;     /* AMPLIFY_FACTOR: weight of a parent group's size in its vote (2.0) */
+    double over_gamma;  /* OVER_REGULARIZATION_GMMA: penalty slope past the load average (6.0) */
+    double award_alpha; /* AWARD_ALPHA: weight of the affinity award (1.0) */
+    double load_beta;   /* LOAD_REGULARIZATION_BETA: weight of the under-load bonus (0.1) */
 } baas_options;
 
 /* The SpTRSV runtime's ablation classes (test/SpTRSV_level_merge.cpp:156-299), kind

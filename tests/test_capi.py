@@ -89,3 +89,20 @@ def test_analysis_placement_option():
     with pytest.raises(BaasError) as e:
         Schedule(gen.laplace2d(4), kind=KERNEL_ICCG, nthread=2, analysis=ANALYSIS_DEVICE)
     assert e.value.status_name == "BAAS_ERR_NO_DEVICE"
+
+
+def test_scoring_constants():
+    """The four-rule mapping's scoring constants (the reference's MergeMarco.hpp macros): the
+    defaults are the reference's values, so naming them changes nothing; other values change the
+    mapping but not the level sets; out-of-range values are refused."""
+    A = gen.knn_stiffness(nodes=600, k=12, seed=3)
+    base = Schedule(A, kind=KERNEL_ICCG, nthread=8).arrays()
+    same = Schedule(A, kind=KERNEL_ICCG, nthread=8,
+                    scoring={"level_window": 6, "amplify": 2.0, "over_gamma": 6.0, "award_alpha": 1.0,
+                             "load_beta": 0.1}).arrays()
+    assert all(np.array_equal(base[f], same[f]) for f in base)
+    other = Schedule(A, kind=KERNEL_ICCG, nthread=8, scoring={"award_alpha": 0.0, "level_window": 2}).arrays()
+    assert np.array_equal(base["level_ptr"], other["level_ptr"])
+    assert not np.array_equal(base["thread_cont_to_orig"], other["thread_cont_to_orig"])
+    _bad(A, scoring={"level_window": -1})
+    _bad(A, scoring={"amplify": float("nan")})
