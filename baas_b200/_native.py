@@ -6,9 +6,12 @@ this module never falls back to anything else: if the library is missing, :func:
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libbaas_b200.so"
+# BAAS_LIB=bounds selects the bounds-checked build (python -m baas_b200.build --debug-bounds)
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / (
+    "libbaas_b200_bounds.so" if os.environ.get("BAAS_LIB") == "bounds" else "libbaas_b200.so")
 _lib = None
 
 BAAS_OK = 0

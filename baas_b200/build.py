@@ -17,6 +17,9 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libbaas_b200.so"
+# the bounds-checked variant (-DBAAS_DEBUG_BOUNDS): kernels record an out-of-range index in the
+# status word instead of touching memory outside an array; loaded when BAAS_LIB=bounds
+LIB_BOUNDS = LIB_DIR / "libbaas_b200_bounds.so"
 SOURCES = ["capi.cu", "analysis.cu", "schedule.cpp", "mtx.cpp"]
 HEADERS = ["kernels.cuh", "part_kernels.cuh", "staged.cuh", "fetch.cuh", "batched.cuh", "small.cuh", "device_common.cuh",
            "schedule.hpp"]
@@ -42,19 +45,22 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build_lib(force: bool = False, verbose: bool = False) -> Path:
+def build_lib(force: bool = False, verbose: bool = False, bounds: bool = False) -> Path:
+    target = LIB_BOUNDS if bounds else LIB
     deps = [CSRC / s for s in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "baas_b200.h"]
-    if not force and not _stale(LIB, deps):
-        return LIB
+    if not force and not _stale(target, deps):
+        return target
     LIB_DIR.mkdir(exist_ok=True)
     cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-ffp-contract=off", *_host_cxx(), "-o", str(LIB)]
+           "-Xcompiler", "-ffp-contract=off", *_host_cxx(), "-o", str(target)]
+    if bounds:
+        cmd.append("-DBAAS_DEBUG_BOUNDS")
     cmd += [str(CSRC / s) for s in SOURCES]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    return LIB
+    return target
 
 
 def reference_tree():
@@ -73,6 +79,9 @@ def build_oracle(verbose: bool = False) -> None:
 
 
 if __name__ == "__main__":
-    build_lib(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    build_oracle()
-    print(LIB)
+    if "--debug-bounds" in sys.argv:
+        print(build_lib(force="--force" in sys.argv, verbose="-v" in sys.argv, bounds=True))
+    else:
+        build_lib(force="--force" in sys.argv, verbose="-v" in sys.argv)
+        build_oracle()
+        print(LIB)

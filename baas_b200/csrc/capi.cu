@@ -1219,6 +1219,9 @@ baas_status upload_small(baas_schedule *s, bool full) {
 baas::SmallArgs small_args(const baas_schedule *s, bool full) {
     baas::SmallArgs a{};
     a.n = s->hs.n;
+    a.nnz_a = s->nnz_a;
+    a.nnz_t = s->nnz_l;
+    a.npair = (int)s->sm.ic_pair.size();
     for (int d = 0; d < 2; d++)
         a.dir[d] = baas::SmallDir{s->sm.nlev[d], s->d_sm_lev[d], full ? s->d_sm_rec_a[d] : s->d_sm_rec_t[d]};
     a.st = s->d_status;
@@ -1462,6 +1465,8 @@ baas_status read_status(baas_schedule *s, cudaStream_t stream) {
     const DevStatus &ds = *s->h_status;
     if (ds.code == baas::kTimeout)
         return fail(BAAS_ERR_TIMEOUT, "a device wait ran out (at " + std::to_string(ds.where) + ")");
+    if (ds.code == baas::kBounds)
+        return fail(BAAS_ERR_CUDA, "a device bounds check failed (site " + std::to_string(ds.where) + ")");
     if (ds.code != 0) return fail(BAAS_ERR_CUDA, "device status " + std::to_string(ds.code));
     if (ds.zero_pivots > 0)
         return fail(BAAS_ERR_ZERO_PIVOT, std::to_string(ds.zero_pivots) + " non-positive / zero pivot(s)");

@@ -9,7 +9,7 @@
 namespace baas {
 
 // Status words written by kernels (mirrors baas_status).
-enum : int { kOk = 0, kTimeout = 3, kZeroPivot = 4 };
+enum : int { kOk = 0, kTimeout = 3, kZeroPivot = 4, kBounds = 5 };
 
 struct DevStatus {
     int code;        // first error (kOk if none)
@@ -101,6 +101,24 @@ struct Waiter {
         return true;
     }
 };
+
+// Bounds-checked builds (-DBAAS_DEBUG_BOUNDS: python -m baas_b200.build --debug-bounds): an index
+// outside [0, n) is recorded (status kBounds, `where` = the check's site) and replaced by 0, so the
+// kernel goes on without touching memory outside the array and the host reports the first site.
+// In the ordinary build the check compiles to nothing.
+__device__ __forceinline__ int bounded(int i, int n, DevStatus *st, int site) {
+#ifdef BAAS_DEBUG_BOUNDS
+    if ((unsigned int)i >= (unsigned int)n) {
+        if (atomicCAS(&st->code, kOk, kBounds) == kOk) st->where = site;
+        return 0;
+    }
+#else
+    (void)n;
+    (void)st;
+    (void)site;
+#endif
+    return i;
+}
 
 // Shared-memory value-as-flag (producer and consumer in the same CTA).
 template <typename T> struct SSent;

@@ -33,6 +33,7 @@ struct SmallDir {
 
 struct SmallArgs {
     int n;
+    int nnz_a, nnz_t, npair;                // sizes for the bounds-checked build: A, the caller's T, IC0 pairs
     SmallDir dir[2];                        // 0: forward (L), 1: backward (U = L^T)
     const int *a_rowptr, *a_colidx, *a_diag;
     const double *a_val;
@@ -74,6 +75,8 @@ struct SmallSrc {
     const V *diag;       // indexed by the diagonal position (by_row = 0) or by the row (1)
     int by_row;
     const double *rhs;   // global right-hand side, or nullptr: the row's own slot of xs
+    int n, nval, ndiag;  // rows, entries of col / val, entries of diag (bounds-checked build)
+    DevStatus *st;
 };
 
 template <bool DESC>
@@ -83,17 +86,17 @@ __device__ __forceinline__ int small_pos(int e, int cnt, int q) {
 
 template <typename V, bool DESC>
 __device__ __forceinline__ void small_load(const int4 *rec, int q, const SmallSrc<V> &S, SmallRow<V> &r) {
-    const int4 c = __ldg(rec + q);
-    r.i = c.x;
+    const int4 c = __ldg(rec + bounded(q, S.n, S.st, 101));
+    r.i = bounded(c.x, S.n, S.st, 102);
     r.e = c.y;
     r.cnt = c.z;
-    r.dv = S.diag[S.by_row ? c.x : c.w];
-    if (S.rhs) r.rhs = (V)S.rhs[c.x];
+    r.dv = S.diag[S.by_row ? r.i : bounded(c.w, S.ndiag, S.st, 103)];
+    if (S.rhs) r.rhs = (V)S.rhs[r.i];
 #pragma unroll
     for (int k = 0; k < kSmallPF; k++)
         if (k < r.cnt) {
-            const int p = small_pos<DESC>(r.e, r.cnt, k);
-            r.col[k] = __ldg(S.col + p);
+            const int p = bounded(small_pos<DESC>(r.e, r.cnt, k), S.nval, S.st, 104);
+            r.col[k] = bounded(__ldg(S.col + p), S.n, S.st, 105);
             r.val[k] = S.val[p];
         }
 }
@@ -108,8 +111,8 @@ __device__ __forceinline__ void small_tail(int e, int cnt, int k0, const V *xs, 
         V v[4];
 #pragma unroll
         for (int t = 0; t < 4; t++) {
-            const int p = small_pos<DESC>(e, cnt, k + t);
-            c[t] = __ldg(S.col + p);
+            const int p = bounded(small_pos<DESC>(e, cnt, k + t), S.nval, S.st, 106);
+            c[t] = bounded(__ldg(S.col + p), S.n, S.st, 107);
             v[t] = S.val[p];
         }
 #pragma unroll
@@ -121,12 +124,13 @@ __device__ __forceinline__ void small_tail(int e, int cnt, int k0, const V *xs, 
         }
     }
     for (; k < cnt; k++) {
-        const int p = small_pos<DESC>(e, cnt, k);
+        const int p = bounded(small_pos<DESC>(e, cnt, k), S.nval, S.st, 108);
         const V v = S.val[p];
+        const int c = bounded(__ldg(S.col + p), S.n, S.st, 109);
         if constexpr (sizeof(V) == 8)
-            sum = __dadd_rn(sum, __dmul_rn(v, xs[__ldg(S.col + p)]));
+            sum = __dadd_rn(sum, __dmul_rn(v, xs[c]));
         else
-            sum = fmaf(xs[__ldg(S.col + p)], v, sum);
+            sum = fmaf(xs[c], v, sum);
     }
 }
 
@@ -184,8 +188,9 @@ struct SmallGrp {
 // A row of a level with more rows than threads: the same arithmetic, entries loaded as it goes.
 template <typename V, bool DESC, int CS>
 __device__ __forceinline__ void small_direct(const int4 *rec, int q, V *xs, const SmallSrc<V> &S) {
-    const int4 c = __ldg(rec + q);
-    const V dv = S.diag[S.by_row ? c.x : c.w];
+    int4 c = __ldg(rec + bounded(q, S.n, S.st, 110));
+    c.x = bounded(c.x, S.n, S.st, 111);
+    const V dv = S.diag[S.by_row ? c.x : bounded(c.w, S.ndiag, S.st, 112)];
     const V rhs = S.rhs ? (V)S.rhs[c.x] : xs[c.x];
     V sum = (V)0;
     small_tail<V, DESC>(c.y, c.z, 0, xs, S, sum);
@@ -294,23 +299,27 @@ __device__ __forceinline__ void small_ic0(const SmallArgs &A, const int *lev, un
     int bad = 0;
     for (int l = 0; l < D.nlev; l++) {
         for (int q = lev[l] + gt; q < lev[l + 1]; q += G) {
-            const int4 c = __ldg(D.rec + q);  // {row, first entry, lower entries, diagonal}
+            int4 c = __ldg(D.rec + bounded(q, A.n, A.st, 120));  // {row, first entry, lower entries, diagonal}
+            c.w = bounded(c.w, A.nnz_a, A.st, 121);
             const int rb = c.y, m = c.z;
+            bounded(rb + m, A.nnz_a + 1, A.st, 122);
             const int pb0 = __ldg(A.ic_ptr + rb);
             const int np = __ldg(A.ic_ptr + rb + m) - pb0;
+            bounded(pb0 + np, A.npair + 1, A.st, 123);
             if (scratch && m <= kIcRow && np <= kIcPairs) {
 #pragma unroll 4
                 for (int k = 0; k < m; k++) {
                     IC_D(k) = A.lu[rb + k];
-                    IC_D(kIcRow + k) = A.lu[__ldg(A.a_diag + __ldg(A.a_colidx + rb + k))];
+                    IC_D(kIcRow + k) = A.lu[bounded(__ldg(A.a_diag + bounded(__ldg(A.a_colidx + rb + k), A.n, A.st, 126)),
+                                                    A.nnz_a, A.st, 127)];
                 }
 #pragma unroll 4
                 for (int k = 0; k <= m; k++) IC_B(kIcPairs + k) = (unsigned char)(__ldg(A.ic_ptr + rb + k) - pb0);
 #pragma unroll 4
                 for (int p = 0; p < np; p++) {
                     const int2 pr = __ldg(A.ic_pair + pb0 + p);
-                    IC_B(p) = (unsigned char)(pr.x - rb);
-                    IC_D(2 * kIcRow + p) = A.lu[pr.y];
+                    IC_B(p) = (unsigned char)bounded(pr.x - rb, m, A.st, 124);
+                    IC_D(2 * kIcRow + p) = A.lu[bounded(pr.y, A.nnz_a, A.st, 125)];
                 }
                 for (int k = 0; k < m; k++) {
                     double dp = 0.0;
@@ -404,7 +413,7 @@ __global__ void __launch_bounds__(kSmallBlock, 1) k_sweep_small(SmallArgs A, con
     const int *lev[2];
     small_stage_levels<CS>(A, sl, lev);
     double *xs = reinterpret_cast<double *>(smem_small);
-    const SmallSrc<double> S{tcol, tval, tval, 0, A.b};
+    const SmallSrc<double> S{tcol, tval, tval, 0, A.b, A.n, A.nnz_t, A.nnz_t, A.st};
     small_sweep<double, UPPER, CS>(A.dir[UPPER ? 1 : 0], lev[UPPER ? 1 : 0], xs, S);
     const int gt = (int)threadIdx.x * CS + SmallGrp<CS>::rank();
     for (int i = gt; i < A.n; i += CS * kSmallBlock) A.x[i] = xs[i];
@@ -457,8 +466,9 @@ __global__ void __launch_bounds__(kSmallBlock, 1) k_iccg_small(SmallArgs A) {
     const T *lval = sizeof(T) == 8 ? (const T *)A.lu : (const T *)A.lf32;
     const T *uval = sizeof(T) == 8 ? (const T *)A.ut : (const T *)A.ut32;
     const T *dg = sizeof(T) == 8 ? (const T *)A.lu : (const T *)A.rcp32;
-    const SmallSrc<T> SL{A.a_colidx, lval, dg, sizeof(T) == 4, A.r};
-    const SmallSrc<T> SU{A.ub_col, uval, dg, sizeof(T) == 4, nullptr};
+    const int nd = sizeof(T) == 4 ? n : A.nnz_a;
+    const SmallSrc<T> SL{A.a_colidx, lval, dg, sizeof(T) == 4, A.r, n, A.nnz_a, nd, A.st};
+    const SmallSrc<T> SU{A.ub_col, uval, dg, sizeof(T) == 4, nullptr, n, A.nub, nd, A.st};
     // z = U^-1 L^-1 r, in place in zs (every CTA's copy); returns r.z
     auto precond = [&]() -> double {
         small_sweep<T, false, CS>(A.dir[0], lev[0], zs, SL);

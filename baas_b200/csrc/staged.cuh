@@ -852,7 +852,7 @@ __device__ __forceinline__ bool level_walk(const LevelDir &D, const T *v, const 
                 wv[k] = T(0);
             }
             for (int p = __ldg(D.item + it), pe = __ldg(D.item + it + 1); p < pe; p++) {
-                const int row = __ldg(D.row + p);
+                const int row = bounded(__ldg(D.row + bounded(p, D.npos, st, 130)), D.npos, st, 131);
                 T sum = T(0);
                 // eight entries' loads in flight at once (dependency rows, then their values),
                 // then their products summed in entry order
@@ -862,8 +862,9 @@ __device__ __forceinline__ bool level_walk(const LevelDir &D, const T *v, const 
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
                         const bool in = e0 + u < ee;
-                        dr[u] = in ? __ldg(D.dep + e0 + u) : row;
-                        vv[u] = in ? __ldg(v + e0 + u) : T(0);
+                        const int e = in ? bounded(e0 + u, D.nent, st, 132) : 0;
+                        dr[u] = in ? bounded(__ldg(D.dep + e), D.npos, st, 133) : row;
+                        vv[u] = in ? __ldg(v + e) : T(0);
                     }
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
