@@ -117,6 +117,23 @@ class Schedule:
         self.nthread = nthread
         self.mapping = mapping
 
+    def save(self, path) -> None:
+        """Write the analysed schedule to `path` (baas_schedule_save): a later `Schedule.load`
+        skips the analysis."""
+        _native.check(_native.lib().baas_schedule_save(self._h, str(path).encode()), "baas_schedule_save")
+
+    @classmethod
+    def load(cls, path) -> "Schedule":
+        """A schedule read from a file written by `save` (baas_schedule_load), ready for GPU calls."""
+        h = C.c_void_p()
+        _native.check(_native.lib().baas_schedule_load(str(path).encode(), C.byref(h)), "baas_schedule_load")
+        s = cls.__new__(cls)
+        s._h = h
+        info = np.zeros(6, dtype=np.int32)
+        _native.lib().baas_schedule_info(h, info.ctypes.data)
+        s.n, s.nnz, s.kind, s.nthread, s.mapping = (int(v) for v in info[:5])
+        return s
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

@@ -49,7 +49,8 @@ EXPORTS = [
     "baas_options_default", "baas_analyze", "baas_schedule_export", "baas_schedule_analysis_ms",
     "baas_destroy", "baas_sptrsv", "baas_ic0", "baas_ilu0", "baas_iccg", "baas_last_error_string",
     "baas_version", "baas_test_inject_unsatisfiable_wait", "baas_ic0_noalloc", "baas_test_emulate_sweep", "baas_iccg_adjoint", "baas_batch_concat", "baas_analyze_batch", "baas_iccg_batched", "baas_replan", "baas_test_divide", "baas_replan_custom", "baas_csr_read_mtx", "baas_csr_free",
-    "baas_schedule_last_walk", "baas_test_emulate_fetch", "baas_plan_parts",
+    "baas_schedule_last_walk", "baas_test_emulate_fetch", "baas_plan_parts", "baas_schedule_save",
+    "baas_schedule_load", "baas_schedule_info",
 ]
 
 
@@ -98,6 +99,12 @@ def lib():
     L.baas_schedule_last_walk.restype = i
     L.baas_plan_parts.argtypes = [vp, vp]
     L.baas_plan_parts.restype = i
+    L.baas_schedule_save.argtypes = [vp, C.c_char_p]
+    L.baas_schedule_save.restype = i
+    L.baas_schedule_load.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.baas_schedule_load.restype = i
+    L.baas_schedule_info.argtypes = [vp, vp]
+    L.baas_schedule_info.restype = i
     L.baas_destroy.argtypes = [vp]
     L.baas_destroy.restype = None
     L.baas_sptrsv.argtypes = [vp, C.POINTER(BaasCsr), i, vp, vp, i, i, vp]

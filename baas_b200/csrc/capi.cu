@@ -2342,6 +2342,136 @@ int baas_batch_concat(int nsys, const baas_csr *const *sys, int *rowptr, int *co
     return (int)nnz;
 }
 
+}  // extern "C"
+
+// Schedule file: "BAASSCH" + format version, the options, the sizes, then every array of the
+// analysis (each as a count and its elements), so that loading rebuilds the schedule without
+// repeating the analysis. Host byte order; the file is for the machine or cluster that wrote it.
+namespace {
+constexpr char kSchedMagic[8] = {'B', 'A', 'A', 'S', 'S', 'C', 'H', '1'};
+
+struct SchedWriter {
+    FILE *f;
+    bool ok = true;
+    void raw(const void *p, size_t n) { ok = ok && std::fwrite(p, 1, n, f) == n; }
+    template <typename T>
+    void val(T v) { raw(&v, sizeof(T)); }
+    template <typename T>
+    void vec(const std::vector<T> &v) {
+        val<long long>((long long)v.size());
+        if (!v.empty()) raw(v.data(), sizeof(T) * v.size());
+    }
+};
+struct SchedReader {
+    FILE *f;
+    bool ok = true;
+    void raw(void *p, size_t n) { ok = ok && std::fread(p, 1, n, f) == n; }
+    template <typename T>
+    T val() {
+        T v{};
+        raw(&v, sizeof(T));
+        return v;
+    }
+    template <typename T>
+    void vec(std::vector<T> &v, long long max_count) {
+        const long long n = val<long long>();
+        if (!ok || n < 0 || n > max_count) {
+            ok = false;
+            return;
+        }
+        v.resize((size_t)n);
+        if (n) raw(v.data(), sizeof(T) * (size_t)n);
+    }
+};
+
+template <class IO, class H, class V>
+void sched_arrays(IO &io, H &h, V vec) {
+    vec(h.a_rowptr), vec(h.a_colidx), vec(h.a_diagptr), vec(h.l_rowptr), vec(h.l_colidx), vec(h.l_src);
+    vec(h.group_ptr), vec(h.group_set), vec(h.level_ptr), vec(h.perm_to_orig), vec(h.node_to_level), vec(h.perm);
+    vec(h.exec_level_ptr), vec(h.nthread_per_level), vec(h.thread_boundaries), vec(h.task_boundaries);
+    vec(h.thread_cont_to_orig), vec(h.orig_to_thread_cont), vec(h.task_ptr), vec(h.task_set), vec(h.btask_ptr);
+    vec(h.btask_set), vec(h.fdag_ptr), vec(h.fdag_set);
+    (void)io;
+}
+}  // namespace
+
+extern "C" {
+
+baas_status baas_schedule_save(const baas_schedule *s, const char *path) {
+    if (!s || !path) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(BAAS_ERR_BAD_ARG, std::string("cannot open ") + path + " for writing");
+    SchedWriter w{f};
+    const baas::HostSchedule &h = s->hs;
+    w.raw(kSchedMagic, sizeof(kSchedMagic));
+    w.val<int>((int)sizeof(baas_options));
+    w.raw(&s->opt, sizeof(baas_options));
+    w.val<int>((int)h.kind), w.val<int>(h.n), w.val<int>(h.nthread), w.val<int>(h.ngroups), w.val<int>(h.nlevels);
+    w.val<int>(h.ntasks), w.val<int>(s->nnz_a), w.val<int>(s->nnz_l), w.val<int>(s->nsys);
+    w.val<double>(h.analysis_ms);
+    w.val<int>(h.score.level_window), w.val<double>(h.score.amplify), w.val<double>(h.score.over_gamma);
+    w.val<double>(h.score.award_alpha), w.val<double>(h.score.load_beta);
+    w.vec(h.cost);
+    w.vec(s->sys_off);
+    sched_arrays(w, h, [&](const std::vector<int> &v) { w.vec(v); });
+    const bool ok = w.ok && std::fclose(f) == 0;
+    if (!ok) return fail(BAAS_ERR_BAD_ARG, std::string("writing ") + path + " failed");
+    return BAAS_OK;
+}
+
+int baas_schedule_info(const baas_schedule *s, int *info) {
+    if (!s || !info) return -1;
+    info[0] = s->hs.n;
+    info[1] = s->nnz_a;
+    info[2] = (int)s->hs.kind;
+    info[3] = s->hs.nthread;
+    info[4] = s->opt.mapping;
+    info[5] = s->nsys;
+    return 6;
+}
+
+baas_status baas_schedule_load(const char *path, baas_schedule **out) {
+    if (!path || !out) return fail(BAAS_ERR_BAD_ARG, "NULL argument");
+    *out = nullptr;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(BAAS_ERR_BAD_ARG, std::string("cannot open ") + path);
+    SchedReader r{f};
+    char magic[8];
+    r.raw(magic, sizeof(magic));
+    if (!r.ok || std::memcmp(magic, kSchedMagic, sizeof(magic)) != 0 || r.val<int>() != (int)sizeof(baas_options)) {
+        std::fclose(f);
+        return fail(BAAS_ERR_BAD_ARG, std::string(path) + " is not a schedule file of this library version");
+    }
+    baas_schedule *s = new baas_schedule();
+    baas::HostSchedule &h = s->hs;
+    r.raw(&s->opt, sizeof(baas_options));
+    h.kind = (baas::SchedKind)r.val<int>();
+    h.n = r.val<int>(), h.nthread = r.val<int>(), h.ngroups = r.val<int>(), h.nlevels = r.val<int>();
+    h.ntasks = r.val<int>(), s->nnz_a = r.val<int>(), s->nnz_l = r.val<int>(), s->nsys = r.val<int>();
+    h.analysis_ms = r.val<double>();
+    h.score.level_window = r.val<int>(), h.score.amplify = r.val<double>(), h.score.over_gamma = r.val<double>();
+    h.score.award_alpha = r.val<double>(), h.score.load_beta = r.val<double>();
+    const long long cap = (long long)std::max(s->nnz_a, 0) + 2LL * std::max(h.n, 0) + 16;  // no array is longer
+    r.vec(h.cost, cap);
+    r.vec(s->sys_off, cap);
+    sched_arrays(r, h, [&](std::vector<int> &v) { r.vec(v, cap); });
+    std::fclose(f);
+    const int n = h.n;
+    const bool sane = r.ok && n > 0 && (int)h.a_rowptr.size() == n + 1 && (int)h.a_colidx.size() == s->nnz_a &&
+                      (int)h.l_rowptr.size() == n + 1 && (int)h.l_colidx.size() == s->nnz_l &&
+                      (int)h.group_ptr.size() == h.ngroups + 1 && (int)h.group_set.size() == n &&
+                      (int)h.perm_to_orig.size() == h.ngroups && (int)h.level_ptr.size() == h.nlevels + 1 &&
+                      (h.kind >= baas::SchedKind::SpTRSV && h.kind <= baas::SchedKind::ILU0) &&
+                      (s->nsys == 0 || (int)s->sys_off.size() == s->nsys + 1);
+    if (!sane) {
+        delete s;
+        return fail(BAAS_ERR_BAD_ARG, std::string(path) + " is truncated or inconsistent");
+    }
+    build_order(s);
+    *out = s;
+    return BAAS_OK;
+}
+
 baas_status baas_analyze_batch(const baas_csr *A, const int *sys_off, int nsys, const baas_options *opt,
                                baas_schedule **out) {
     if (!A || !sys_off || !out || nsys < 1) return fail(BAAS_ERR_BAD_ARG, "NULL argument or no systems");

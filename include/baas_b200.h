@@ -239,6 +239,19 @@ int baas_plan_parts(const baas_schedule *s, int *box);
 /* Frees the schedule and its device memory. */
 void baas_destroy(baas_schedule *s);
 
+/* Writes the analysed schedule (its options, the pattern it was built for and every array of the
+ * analysis) to a file, and reads one back, so that a later process skips the analysis; the loaded
+ * schedule behaves as the one saved (its device plan is built at its first GPU call). No
+ * counterpart in the reference, which re-analyses on every run. The file is in this host's byte
+ * order and this library version's layout; a file of another version, or a truncated or
+ * inconsistent one, is refused with BAAS_ERR_BAD_ARG. */
+baas_status baas_schedule_save(const baas_schedule *s, const char *path);
+baas_status baas_schedule_load(const char *path, baas_schedule **out);
+
+/* What a schedule was analysed for, into info[0..5]: rows, nnz of the analysed matrix, kind
+ * (baas_kernel), nthread, mapping, systems of a batch (0 otherwise). Returns 6 (-1 on NULL). */
+int baas_schedule_info(const baas_schedule *s, int *info);
+
 /* MatrixMarket ingestion. Replaces SPM::CSR(const char *fileName) (spm/CSR.cpp:90-112), which
  * reads through loadMatrixMarket_mmio_highlevel_coo (spm/COO.cpp:322-338), mmio_allinone_coo
  * (spm/mmio_highlevel.cpp:748-921) and dcoo2csr (spm/COO.cpp:222-317). Reads a coordinate
