@@ -1552,3 +1552,162 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_levels(LevelDir D, con
 }
 
 }  // namespace baas
+
+namespace baas {
+
+// ILU0 by the level walk's plan: every thread of the launch takes groups of the current level
+// (grid stride), factors their rows in order, and a grid barrier ends the level, so no row waits
+// on a flag. Row i (merge/ILU.cpp:638-720): for each lower entry j in ascending column order,
+// lu_ij /= lu_jj, then every later entry of row i whose column row j's upper part also holds loses
+// lu_ij * lu_j,col -- the same operations on the same values as k_factor_part<true>, so the factor
+// is bit-identical. Rows of at most kFacRegs entries whose lower entries (at most kIluLow) each
+// name a row with at most kIluUp upper entries run from registers: the row, its pivots and its
+// partners' upper entries are loaded first, all at once; each entry of row i matches at most one
+// upper entry of a given row j, so applying row j's matches in any order gives the merge's result.
+// Other rows take ilu0_row_merge, the reference's merge loop.
+constexpr int kIluLow = 4, kIluUp = 4;
+
+__device__ __forceinline__ void ilu0_row_merge(int i, const int *__restrict__ rowptr, const int *__restrict__ colidx,
+                                               const int *__restrict__ diagptr, double *lu, DevStatus *st) {
+    const int rb = __ldg(rowptr + i), di = __ldg(diagptr + i), re = __ldg(rowptr + i + 1);
+    for (int j = rb; j < di; j++) {
+        const int c = __ldg(colidx + j);
+        const int dc = __ldg(diagptr + c), ec = __ldg(rowptr + c + 1);
+        const double pivot = ld_l2(lu + dc);
+        if (pivot == 0.0) atomicAdd(&st->zero_pivots, 1);
+        const double tmp = __ddiv_rn(lu[j], pivot);
+        lu[j] = tmp;
+        int k1 = j + 1, k2 = dc + 1;
+        while (k1 < re && k2 < ec) {
+            const int c1 = __ldg(colidx + k1), c2 = __ldg(colidx + k2);
+            if (c1 < c2) {
+                k1++;
+            } else if (c1 > c2) {
+                k2++;
+            } else {
+                lu[k1] = __dsub_rn(lu[k1], __dmul_rn(tmp, ld_l2(lu + k2)));
+                k1++;
+                k2++;
+            }
+        }
+    }
+}
+
+// A row of the level ILU0 in registers: its record (host-built per plan position: row, first
+// entry, entries, lower entries -- entries < 0 sends the row down the merge path), its columns and
+// values, and per lower entry the partner row's diagonal position and upper-entry count. All of it
+// is static or not yet written when a level starts, so the next level's first row is loaded before
+// the barrier; only the pivots and the partners' upper values wait for it.
+struct IluRow {
+    int i, rb, n, nlow;
+    int c[kFacRegs];
+    double v[kFacRegs];
+    int dc[kIluLow], nu[kIluLow];
+};
+
+__device__ __forceinline__ void ilu_load(int p, const int4 *__restrict__ irec, const int2 *__restrict__ idep,
+                                         const int *__restrict__ colidx, const double *lu, IluRow &R) {
+    const int4 r = __ldg(irec + p);
+    R.i = r.x;
+    R.rb = r.y;
+    R.n = r.z;
+    R.nlow = r.w;
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++)
+        if (t < R.n) {
+            R.c[t] = __ldg(colidx + R.rb + t);
+            R.v[t] = lu[R.rb + t];
+        }
+#pragma unroll
+    for (int t = 0; t < kIluLow; t++)
+        if (t < R.nlow) {
+            const int2 d = __ldg(idep + (size_t)p * kIluLow + t);
+            R.dc[t] = d.x;
+            R.nu[t] = d.y;
+        }
+}
+
+__device__ __forceinline__ void ilu_finish(IluRow &R, const int *__restrict__ rowptr, const int *__restrict__ colidx,
+                                           const int *__restrict__ diagptr, double *lu, DevStatus *st) {
+    if (R.n < 0) {
+        ilu0_row_merge(R.i, rowptr, colidx, diagptr, lu, st);
+        return;
+    }
+    double piv[kIluLow], uv[kIluLow][kIluUp];
+    int uc[kIluLow][kIluUp];
+#pragma unroll
+    for (int t = 0; t < kIluLow; t++)
+        if (t < R.nlow) {
+            piv[t] = ld_l2(lu + R.dc[t]);
+#pragma unroll
+            for (int q = 0; q < kIluUp; q++)
+                if (q < R.nu[t]) {
+                    uc[t][q] = __ldg(colidx + R.dc[t] + 1 + q);
+                    uv[t][q] = ld_l2(lu + R.dc[t] + 1 + q);
+                }
+        }
+#pragma unroll
+    for (int t = 0; t < kIluLow; t++)
+        if (t < R.nlow) {
+            if (piv[t] == 0.0) atomicAdd(&st->zero_pivots, 1);
+            const double tmp = __ddiv_rn(R.v[t], piv[t]);
+            R.v[t] = tmp;
+#pragma unroll
+            for (int q = 0; q < kIluUp; q++)
+                if (q < R.nu[t]) {
+#pragma unroll
+                    for (int u = 0; u < kFacRegs; u++)
+                        if (u > t && u < R.n && R.c[u] == uc[t][q]) R.v[u] = __dsub_rn(R.v[u], __dmul_rn(tmp, uv[t][q]));
+                }
+        }
+#pragma unroll
+    for (int t = 0; t < kFacRegs; t++)
+        if (t < R.n) lu[R.rb + t] = R.v[t];
+}
+
+__global__ void __launch_bounds__(kStageBlock, 1) k_ilu0_levels(LevelDir D, const int4 *__restrict__ irec,
+                                                                const int2 *__restrict__ idep,
+                                                                const int *__restrict__ rowptr,
+                                                                const int *__restrict__ colidx,
+                                                                const int *__restrict__ diagptr, double *lu,
+                                                                unsigned int *bar, DevStatus *st, unsigned int limit) {
+    const int W = gridDim.x * blockDim.x;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned int nb = 0;
+    IluRow cur, nxt;
+    cur.i = -1;
+    // this thread's first item of level l: its first position is prefetched one level ahead
+    auto first = [&](int l) -> int {
+        const int it = __ldg(D.lev + l) + gt;
+        return it < __ldg(D.lev + l + 1) ? bounded(__ldg(D.item + it), D.npos, st, 141) : -1;
+    };
+    if (D.nlev > 0) {
+        const int p0 = first(0);
+        if (p0 >= 0) ilu_load(p0, irec, idep, colidx, lu, cur);
+    }
+    for (int l = 0; l < D.nlev; l++) {
+        const int ib = __ldg(D.lev + l), ie = __ldg(D.lev + l + 1);
+        nxt.i = -1;
+        if (l + 1 < D.nlev) {
+            const int pn = first(l + 1);
+            if (pn >= 0) ilu_load(pn, irec, idep, colidx, lu, nxt);
+        }
+        for (int it = ib + gt; it < ie; it += W) {
+            int p = __ldg(D.item + it);
+            const int pe = __ldg(D.item + it + 1);
+            if (it == ib + gt && cur.i >= 0) {
+                ilu_finish(cur, rowptr, colidx, diagptr, lu, st);
+                p++;
+            }
+            for (; p < pe; p++) {  // the group's later rows, and the thread's further groups
+                IluRow r;
+                ilu_load(bounded(p, D.npos, st, 142), irec, idep, colidx, lu, r);
+                ilu_finish(r, rowptr, colidx, diagptr, lu, st);
+            }
+        }
+        if (!grid_barrier(bar, nb, st, limit)) return;
+        cur = nxt;
+    }
+}
+
+}  // namespace baas

@@ -63,3 +63,19 @@ def test_level_walk_iccg(name, precision):
     assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) <= tol
     # the walks agree to the last bits of the dot products' summation order
     assert np.linalg.norm(xg - got[WALK_CHUNKED][1]) / np.linalg.norm(xo) <= tol
+
+
+@pytest.mark.parametrize("k", [14, 40])
+def test_level_walk_ilu0_bitexact(k):
+    """ILU0 by the level walk's plan (k_ilu0_levels: grid barrier per group level, no flags) gives
+    the oracle's factor bit for bit (merge/ILU.cpp:350-386)."""
+    from baas_b200 import KERNEL_ILU0
+
+    A = gen.convdiff3d(k)
+    s = Schedule(A, kind=KERNEL_ILU0, nthread=8, walk=WALK_LEVELS)
+    dA = DeviceCSR.from_host(A)
+    lu = dA.values.clone()
+    s.ilu0(dA, lu)
+    want, bad = Port.ilu0(A)
+    assert bad == 0
+    assert np.array_equal(lu.cpu().numpy(), want)
