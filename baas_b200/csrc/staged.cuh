@@ -862,9 +862,8 @@ __device__ __forceinline__ bool level_walk(const LevelDir &D, const T *v, const 
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
                         const bool in = e0 + u < ee;
-                        const int e = in ? bounded(e0 + u, D.nent, st, 132) : 0;
-                        dr[u] = in ? bounded(__ldg(D.dep + e), D.npos, st, 133) : row;
-                        vv[u] = in ? __ldg(v + e) : T(0);
+                        dr[u] = in ? bounded(__ldg(D.dep + bounded(e0 + u, D.nent, st, 132)), D.npos, st, 133) : row;
+                        vv[u] = in ? __ldg(v + bounded(e0 + u, D.nent, st, 134)) : T(0);
                     }
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
