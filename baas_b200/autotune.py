@@ -16,7 +16,7 @@ costs one plan build and one short run.
 `tune_walk` searches the other execution knobs of a single-right-hand-side solve the same way:
 
   walk           which sweep kernel runs (chunked, fetch, level or single-CTA walk)
-  small_cluster  for the single-CTA walk, the CTAs of its cluster (1, 2, 4, 8): more SMs keep more
+  small_cluster  for the single-CTA walk, the CTAs of its cluster (1, 2, 4, 8, 16): more SMs keep more
                  loads in flight, at the price of a cluster barrier per level
 """
 from __future__ import annotations
@@ -75,7 +75,7 @@ def tune(schedule, run, parts=None, budgets=None, repeats: int = 2, warmup: int 
     return {"best": best, "table": table}
 
 
-DEFAULT_WALKS = ((1, 0), (2, 0), (3, 0), (4, 1), (4, 2), (4, 4), (4, 8))  # (walk, small_cluster)
+DEFAULT_WALKS = ((1, 0), (2, 0), (3, 0), (4, 1), (4, 2), (4, 4), (4, 8), (4, 16))  # (walk, small_cluster)
 
 
 def tune_walk(schedule, run, candidates=None, repeats: int = 2, warmup: int = 1) -> dict:

@@ -1243,12 +1243,17 @@ baas::SmallArgs small_args(const baas_schedule *s, bool full) {
 }
 
 // The single-CTA walk runs as a cluster of kSmallCluster CTAs (each holding a full copy of the
-// solution) from this many rows up; below it, as one CTA.
+// solution) from kSmallClusterMinRows rows up, of 16 CTAs from kSmallCluster16MinRows rows up (k-NN
+// n = 12,000 ICCG: 8 CTAs 2.58 ms, 16 CTAs 2.23 ms); below it, as one CTA.
 constexpr int kSmallCluster = 8;
 constexpr int kSmallClusterMinRows = 2048;
 
+// 16-CTA clusters (non-portable) from this many rows up, where the device can hold one
+constexpr int kSmallCluster16MinRows = 8192;
+
 int small_cs(const baas_schedule *s) {
     if (s->opt.small_cluster > 0) return s->opt.small_cluster;
+    if (s->hs.n >= kSmallCluster16MinRows) return 16;
     return s->hs.n >= kSmallClusterMinRows ? kSmallCluster : 1;
 }
 static_assert(baas::kIcScratch <= kSmallMaxDyn, "the IC0 scratch must fit the walk's dynamic shared memory");
@@ -1268,34 +1273,48 @@ const void *small_kernel(int cs, int which, bool flag) {
         case 1: return small_kernel_cs<1>(which, flag);
         case 2: return small_kernel_cs<2>(which, flag);
         case 4: return small_kernel_cs<4>(which, flag);
+        case 16: return small_kernel_cs<16>(which, flag);
         default: return small_kernel_cs<8>(which, flag);
     }
 }
 
-// One launch of a single-CTA walk kernel with `dyn` bytes of dynamic shared memory: one CTA
-// (cs = 1), or one cluster of cs CTAs (refused if this device cannot hold such a cluster).
-baas_status launch_small(const void *kern, size_t dyn, void **args, cudaStream_t stream, int cs) {
-    if (dyn > 0) BAAS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(cs);
-    cfg.blockDim = dim3(baas::kSmallBlock);
-    cfg.dynamicSmemBytes = dyn;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cs;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = cs > 1 ? 1 : 0;
-    if (cs > 1) {
-        int nclusters = 0;
-        BAAS_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg));
-        if (nclusters < 1) return fail(BAAS_ERR_CUDA, "this device cannot hold a cluster of " + std::to_string(cs) + " CTAs");
+// One launch of a single-CTA walk kernel (small_kernel's `which` / `flag`) with `dyn` bytes of
+// dynamic shared memory: one CTA (cs = 1), or one cluster of cs CTAs. A cluster size the device
+// cannot hold is refused when the caller asked for it, and halved when it was the automatic choice.
+baas_status launch_small(const baas_schedule *s, int which, bool flag, size_t dyn, void **args, cudaStream_t stream) {
+    int cs = small_cs(s);
+    const bool forced = s->opt.small_cluster > 0;
+    for (;;) {
+        const void *kern = small_kernel(cs, which, flag);
+        if (dyn > 0) BAAS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        if (cs > 8) BAAS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(baas::kSmallBlock);
+        cfg.dynamicSmemBytes = dyn;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cs;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = cs > 1 ? 1 : 0;
+        if (cs > 1) {
+            int nclusters = 0;
+            const cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg);
+            if (e != cudaSuccess || nclusters < 1) {
+                cudaGetLastError();
+                if (forced) return fail(BAAS_ERR_CUDA, "this device cannot hold a cluster of " + std::to_string(cs) + " CTAs");
+                cs /= 2;
+                continue;
+            }
+        }
+        BAAS_CUDA(cudaLaunchKernelExC(&cfg, kern, args));
+        return BAAS_OK;
     }
-    BAAS_CUDA(cudaLaunchKernelExC(&cfg, kern, args));
-    return BAAS_OK;
 }
+
 
 baas_status pick_walk(baas_schedule *s, int vbytes, bool iccg, int &walk) {
     const bool fits = s->fch.ok && fetch_smem(s->fch, vbytes, iccg) <= (size_t)kMaxDynSmem;
@@ -1600,8 +1619,8 @@ static baas_status analyze_common(const baas_csr *A, baas_kernel kind, const baa
     if (o.analysis != BAAS_ANALYSIS_HOST && o.analysis != BAAS_ANALYSIS_DEVICE)
         return fail(BAAS_ERR_BAD_ARG, "unknown analysis placement");
     if (o.small_cluster != 0 && o.small_cluster != 1 && o.small_cluster != 2 && o.small_cluster != 4 &&
-        o.small_cluster != 8)
-        return fail(BAAS_ERR_BAD_ARG, "small_cluster must be 0, 1, 2, 4 or 8");
+        o.small_cluster != 8 && o.small_cluster != 16)
+        return fail(BAAS_ERR_BAD_ARG, "small_cluster must be 0, 1, 2, 4, 8 or 16");
     if (o.level_window < 0 || o.level_window > 1024 || !std::isfinite(o.amplify) || !std::isfinite(o.over_gamma) ||
         !std::isfinite(o.award_alpha) || !std::isfinite(o.load_beta))
         return fail(BAAS_ERR_BAD_ARG, "scoring constants: level_window in [0, 1024] and finite weights");
@@ -2108,8 +2127,8 @@ baas_status baas_replan(baas_schedule *s, const baas_options *opt) {
     if (opt->parts < 0 || opt->smem_budget < 0) return fail(BAAS_ERR_BAD_ARG, "parts and smem_budget must be >= 0");
     if (opt->walk < BAAS_WALK_AUTO || opt->walk > BAAS_WALK_SMALL) return fail(BAAS_ERR_BAD_ARG, "unknown walk");
     if (opt->small_cluster != 0 && opt->small_cluster != 1 && opt->small_cluster != 2 && opt->small_cluster != 4 &&
-        opt->small_cluster != 8)
-        return fail(BAAS_ERR_BAD_ARG, "small_cluster must be 0, 1, 2, 4 or 8");
+        opt->small_cluster != 8 && opt->small_cluster != 16)
+        return fail(BAAS_ERR_BAD_ARG, "small_cluster must be 0, 1, 2, 4, 8 or 16");
     if (opt->partition == BAAS_PARTITION_CUSTOM) {
         if (s->custom_part.empty()) return fail(BAAS_ERR_BAD_ARG, "no custom partition: use baas_replan_custom");
         if (opt->parts != s->opt.parts) return fail(BAAS_ERR_BAD_ARG, "a custom partition fixes parts");
@@ -2163,8 +2182,7 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
         void *args[] = {(void *)&a, (void *)&tcol, (void *)&tval};
         s->last_walk = BAAS_WALK_SMALL;
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-        const int cs = small_cs(s);
-        BAAS_TRY(launch_small(small_kernel(cs, 0, upper != 0), sizeof(double) * (size_t)n, args, stream, cs));
+        BAAS_TRY(launch_small(s, 0, upper != 0, sizeof(double) * (size_t)n, args, stream));
         return read_status(s, stream);
     }
     if (walk == BAAS_WALK_LEVELS) {
@@ -2293,8 +2311,7 @@ static baas_status factor(baas_schedule *s, const baas_csr *A, double *lu, void 
         a.lu = lu;
         void *args[] = {(void *)&a};
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-        const int cs = small_cs(s);
-        BAAS_TRY(launch_small(small_kernel(cs, 2, false), baas::kIcScratch, args, stream, cs));
+        BAAS_TRY(launch_small(s, 2, false, baas::kIcScratch, args, stream));
         return read_status(s, stream);
     }
     BAAS_TRY(next_epoch(s, stream));
@@ -2730,9 +2747,7 @@ static baas_status iccg_launch(baas_schedule *s, const baas_csr *A, const double
         void *args[] = {(void *)&a};
         s->last_walk = BAAS_WALK_SMALL;
         BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-        const int cs = small_cs(s);
-        BAAS_TRY(launch_small(small_kernel(cs, 1, mixed), std::max((size_t)n * (8 + (mixed ? 4 : 8)), baas::kIcScratch),
-                              args, stream, cs));
+        BAAS_TRY(launch_small(s, 1, mixed, std::max((size_t)n * (8 + (mixed ? 4 : 8)), baas::kIcScratch), args, stream));
         int it = 0;
         double rr = 0.0;
         BAAS_CUDA(cudaMemcpyAsync(&it, s->d_iters, sizeof(int), cudaMemcpyDeviceToHost, stream));

@@ -120,8 +120,10 @@ typedef struct baas_options {
                          data-parallel stages run; the schedule is identical either way */
     int ablation;     /* BAAS_ABLATION_NONE (default) or, for BAAS_KERNEL_SPTRSV with the four-rule
                          mapping, one of the SpTRSV runtime's ablation schedules */
-    int small_cluster; /* CTAs of BAAS_WALK_SMALL's thread-block cluster: 0 = automatic (8 from
-                         2,048 rows up, else 1), or 1, 2, 4 or 8 */
+    int small_cluster; /* CTAs of BAAS_WALK_SMALL's thread-block cluster: 0 = automatic (16 from
+                         8,192 rows up where the device holds such a cluster, else 8; 8 from 2,048
+                         rows up; else 1), or 1, 2, 4, 8 or 16 (16: a non-portable cluster size,
+                         refused where the device cannot hold one) */
     /* The four-rule mapping's scoring constants, the reference's compile-time macros
      * (merge/include/MergeMarco.hpp:5-23); baas_options_default sets the reference's values.
      * The affinity mapping (BAAS_MAPPING_AFFINITY) reads level_window and amplify. */
@@ -157,7 +159,7 @@ enum { BAAS_ANALYSIS_HOST = 0, BAAS_ANALYSIS_DEVICE = 1 };
  * memory while the CTA's last warp brings other CTAs' results in. LEVELS: one right-hand side;
  * every thread of the launch takes groups of a level and a grid barrier ends the level -- for
  * shallow group DAGs (unstructured or permuted patterns: a few dozen wide levels). SMALL: one
- * right-hand side, one thread-block cluster of 8 CTAs (one CTA below 2,048 rows), each holding the
+ * right-hand side, one thread-block cluster of 8 or 16 CTAs (one CTA below 2,048 rows), each holding the
  * whole solution in shared memory (8 bytes a row; ICCG adds p, and z is 8 or 4 bytes); rows by row
  * level, a row's result stored into every CTA's copy, a cluster barrier per level, the next
  * level's entries loaded while the current one computes -- for systems of up to about 26,000 rows

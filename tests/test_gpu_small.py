@@ -9,7 +9,7 @@ levels with a barrier per level.
     (FP64) / 1e-9 (FP32 factors); the walk is the one the library picks for the k-NN system;
   * the adjoint solve and its gradient against the chunked walk's;
   * a system too large for one CTA's shared memory is refused when the walk is forced;
-  * every cluster size (1, 2, 4, 8) gives the same factor and sweeps; the walk autotuner
+  * every cluster size (1, 2, 4, 8, 16) gives the same factor and sweeps; the walk autotuner
     (autotune.tune_walk) leaves the schedule on its fastest candidate.
 """
 import numpy as np
@@ -115,7 +115,7 @@ def test_forced_small_walk_refuses_a_large_system():
         s.iccg(DeviceCSR.from_host(A), _t(gen.uniform_rhs(A.n, 1)), x)
 
 
-@pytest.mark.parametrize("cs", [1, 2, 4, 8])
+@pytest.mark.parametrize("cs", [1, 2, 4, 8, 16])
 def test_every_cluster_size_gives_the_same_factor_and_sweeps(cs):
     A = gen.knn_stiffness(nodes=1500, k=12, seed=6)
     s = Schedule(A, kind=KERNEL_ICCG, nthread=8, walk=WALK_SMALL, small_cluster=cs)
