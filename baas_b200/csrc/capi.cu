@@ -301,6 +301,9 @@ struct baas_schedule {
     double *d_lv64[2] = {nullptr, nullptr}, *d_ld64[2] = {nullptr, nullptr};  // its values (ICCG, FP64)
     float *d_lv32[2] = {nullptr, nullptr}, *d_ld32[2] = {nullptr, nullptr};   // (ICCG, FP32 factors)
     double *d_lvT[2] = {nullptr, nullptr}, *d_ldT[2] = {nullptr, nullptr};    // (caller's factor, sweeps)
+    double *d_fbuf[2] = {nullptr, nullptr};  // standalone fetch sweeps: publication buffers, used in turn
+    int fbuf_cur = 0;                        // the buffer the next sweep publishes into
+    bool fbuf_ready = false;                 // both hold the sentinel wherever the next sweep will look
     int4 *d_ilu_rec = nullptr;               // level ILU0: per plan position {row, first entry, entries, lower}
     int2 *d_ilu_dep = nullptr;               // ... and per lower entry {partner diagonal, partner upper entries}
     SmallHost sm;                            // single-CTA walk plan (host), built on first use
@@ -2081,7 +2084,7 @@ static void release_device(baas_schedule *s) {
                 if (p) cudaFree(p);
         }
         void *smp[] = {s->d_sm_ic_ptr, s->d_sm_ub_col, s->d_sm_ub_pos, s->d_sm_ic_pair, s->d_sm_ut, s->d_sm_lf32,
-                       s->d_sm_ut32, s->d_sm_rcp32, s->d_ilu_rec, s->d_ilu_dep};
+                       s->d_sm_ut32, s->d_sm_rcp32, s->d_ilu_rec, s->d_ilu_dep, s->d_fbuf[0], s->d_fbuf[1]};
         for (void *p : smp)
             if (p) cudaFree(p);
         void *ptrs[] = {s->d_a_diag, s->d_status, s->d_flags, s->d_bar, s->d_lu, s->d_r, s->d_y, s->d_z, s->d_p,
@@ -2209,17 +2212,30 @@ baas_status baas_sptrsv(baas_schedule *s, const baas_csr *T, int upper, const do
         const size_t smem = fetch_smem(s->fch, 8, false);
         unsigned int spin = s->spin();
         double *gv = s->d_gfT[d];
-        void *args[] = {(void *)&fp, (void *)&d, (void *)&T->values, (void *)&gv, (void *)&b, (void *)&x,
-                        (void *)&s->d_status, (void *)&spin, (void *)&s->d_trace};
+        // the rows' results are published into one of two schedule buffers, which the kernel
+        // leaves reset for the next call; after a failed call both are reset here again
+        if (!s->d_fbuf[0]) {
+            BAAS_TRY(dalloc(s->d_fbuf[0], (size_t)n));
+            BAAS_TRY(dalloc(s->d_fbuf[1], (size_t)n));
+        }
+        if (!s->fbuf_ready) {
+            const int fill_blocks = (int)std::min<long long>(4LL * s->num_sms, ((long long)n + 255) / 256);
+            for (int k = 0; k < 2; k++)
+                baas::k_fill_sentinel<double><<<std::max(fill_blocks, 1), 256, 0, stream>>>(s->d_fbuf[k], n, 1, n);
+            BAAS_CUDA(cudaGetLastError());
+            s->fbuf_ready = true;
+        }
         s->last_walk = BAAS_WALK_FETCH;
         for (int ieee = 0; ieee < 2; ieee++) {
+            double *xg = s->d_fbuf[s->fbuf_cur], *xnext = s->d_fbuf[s->fbuf_cur ^ 1];
+            void *args[] = {(void *)&fp, (void *)&d, (void *)&T->values, (void *)&gv, (void *)&b, (void *)&x,
+                            (void *)&xg, (void *)&xnext, (void *)&s->d_status, (void *)&spin, (void *)&s->d_trace};
             BAAS_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(DevStatus), stream));
-            const int fill_blocks = (int)std::min<long long>(4LL * s->num_sms, ((long long)n + 255) / 256);
-            baas::k_fill_sentinel<double><<<std::max(fill_blocks, 1), 256, 0, stream>>>(x, n, 1, ldb);
-            BAAS_CUDA(cudaGetLastError());
             BAAS_CUDA(cudaLaunchCooperativeKernel(sweep_fetch_kernel(ieee != 0), s->P, baas::kStageBlock, args, smem, stream));
+            s->fbuf_cur ^= 1;
             dump_trace(s, upper ? "sptrsv-upper" : "sptrsv-lower", stream);
             const baas_status st = read_status(s, stream);
+            if (st != BAAS_OK) s->fbuf_ready = false;
             if (!needs_ieee_repeat(s)) return st;
         }
         return fail(BAAS_ERR_CUDA, "IEEE sweep reported a fast-path division");

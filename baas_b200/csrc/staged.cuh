@@ -1487,12 +1487,17 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
 
 // Standalone sweep of the caller's triangular CSR by the fetch walk (fetch.cuh): one right-hand
 // side, direction d (0: L, 1: U = L^T). gv: this direction's record values, gathered from tval
-// here; x must hold the sentinel on entry (its entries are the rows' ready flags). IEEE: divide
-// with __ddiv_rn (the repeat of a launch whose div_fast divisions left their range).
+// here. xg: the schedule's publication buffer for this call (every entry holds the sentinel on
+// entry; the rows' results are published there for the other CTAs' fetchers, the values being
+// their own ready flags); xnext: the other buffer, which each CTA resets to the sentinel for its
+// rows once its walk is done, so that the next call finds it ready without a separate fill
+// launch; x: the caller's solution, written from the CTA's slots. IEEE: divide with __ddiv_rn
+// (the repeat of a launch whose div_fast divisions left their range).
 template <bool IEEE>
 __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_fetch(FetchPlan fp, int d, const double *__restrict__ tval,
                                                                double *gv, const double *__restrict__ b, double *x,
-                                                               DevStatus *st, unsigned int spin, unsigned long long *trace) {
+                                                               double *xg, double *xnext, DevStatus *st,
+                                                               unsigned int spin, unsigned long long *trace) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr unsigned int S = sizeof(double);
     const int tid = (int)threadIdx.x;
@@ -1528,13 +1533,20 @@ __global__ void __launch_bounds__(kStageBlock, 1) k_sweep_fetch(FetchPlan fp, in
     trace_mark(trace, 1);
     bool slow = false;
     if (tid >= kFetchWarp * 32) {
-        fetch_run<double>(F.FL[d], d ? F.nf1 : F.nf0, x, F.SL + S * (unsigned int)(F.nrows + 1 + (d ? F.nf0 : 0)), spin, st,
-                          F.ctl);
+        fetch_run<double>(F.FL[d], d ? F.nf1 : F.nf0, xg, F.SL + S * (unsigned int)(F.nrows + 1 + (d ? F.nf0 : 0)), spin,
+                          st, F.ctl);
     } else if (tid < fp.ncomp) {
-        walk_fetch<double, IEEE ? 2 : 1>(F.I[0], F.V[d], F.SL, F.RW, F.ns[d], fp.ncomp, x, spin, st, F.ctl, slow);
+        walk_fetch<double, IEEE ? 2 : 1>(F.I[0], F.V[d], F.SL, F.RW, F.ns[d], fp.ncomp, xg, spin, st, F.ctl, slow);
     }
     if (!IEEE && slow) st->slow_div = 1;
-    __syncthreads();
+    // every slot holds its row's result (or, after a failed wait, whatever it held): the caller's
+    // solution, and the next call's publication buffer reset for this CTA's rows
+    if (__syncthreads_or(F.ctl->err)) return;
+    for (int k = tid; k < F.nrows; k += blockDim.x) {
+        const int row = __ldg(fp.srow + F.s0 + k);
+        x[row] = Sh<double>::ldu(F.SL + S * (unsigned int)k);
+        xnext[row] = Sent<double>::value();
+    }
     trace_mark(trace, 2);
 }
 
