@@ -1201,7 +1201,7 @@ template <typename T, bool STG, bool IEEE, int WK>
 __global__ void __launch_bounds__(kStageBlock, 1) k_iccg_chunked(IccgArgs A) {
     constexpr bool FW = WK == kWalkFetch, LW = WK == kWalkLevels;
     constexpr bool kMixed = sizeof(T) == 4;
-    constexpr int kLanes = 4;  // rows whose SpMV loads a thread keeps in flight together
+    constexpr int kLanes = 4;  // rows whose SpMV loads a thread keeps in flight together (8: slower)
     extern __shared__ __align__(128) unsigned char smem[];
     const int n = A.n;
     const int W = gridDim.x * blockDim.x;
