@@ -106,3 +106,17 @@ def test_scoring_constants():
     assert not np.array_equal(base["thread_cont_to_orig"], other["thread_cont_to_orig"])
     _bad(A, scoring={"level_window": -1})
     _bad(A, scoring={"amplify": float("nan")})
+
+
+def test_execution_option_checks():
+    """walk, small_cluster and ablation values outside their sets are refused at analysis time."""
+    A = gen.laplace2d(6)
+    _bad(A, walk=9)
+    _bad(A, small_cluster=3)
+    _bad(A, small_cluster=32)
+    _bad(gen.laplace2d(6).lower(), kind=KERNEL_SPTRSV, ablation=4)
+    from baas_b200 import WALK_SMALL
+
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=2, walk=WALK_SMALL, small_cluster=16)
+    with pytest.raises(BaasError):
+        s.replan(walk=WALK_SMALL, small_cluster=5)
