@@ -459,7 +459,7 @@ bool choose_boxes(const int dims[3], int max_boxes, int vmax, int box[3], int nb
 // natural-order stencil whose rows (of L and of U = L^T) hold at most 3 off-diagonal entries and
 // the fetch walk is allowed (those are the plans the fetch walk runs fastest on), else RANGES.
 // BLOCKS: grid boxes whenever the pattern is a grid, else RANGES. RANGES: `parts`, or about one
-// CTA per 2,048 rows (at most 128, at most one per SM).
+// CTA per 2,048 rows (at most one per SM).
 int choose_partition(baas_schedule *s, int num_sms) {
     const baas::HostSchedule &h = s->hs;
     const int n = h.n;
@@ -480,7 +480,7 @@ int choose_partition(baas_schedule *s, int num_sms) {
         }
     }
     if (s->opt.parts > 0) return std::min(s->opt.parts, n);
-    return std::max(1, std::min({(n + 2047) / 2048, 128, num_sms}));
+    return std::max(1, std::min((n + 2047) / 2048, num_sms));
 }
 
 // Groups -> CTAs. RANGES: the CTA whose row range holds the group's first row (P contiguous,
@@ -1098,7 +1098,7 @@ void build_plans(baas_schedule *s, int P, int num_sms) {
         const bool fits = s->fch.ok && fetch_smem(s->fch, 8, s->hs.kind != baas::SchedKind::SpTRSV) <= (size_t)kMaxDynSmem;
         if (!s->use_boxes || s->opt.partition != BAAS_PARTITION_AUTO || fits) return;
         s->use_boxes = false;
-        P = s->opt.parts > 0 ? std::min(s->opt.parts, s->hs.n) : std::max(1, std::min({(s->hs.n + 2047) / 2048, 128, num_sms}));
+        P = s->opt.parts > 0 ? std::min(s->opt.parts, s->hs.n) : std::max(1, std::min((s->hs.n + 2047) / 2048, num_sms));
     }
 }
 
@@ -1423,7 +1423,7 @@ baas_status ensure_device(baas_schedule *s) {
     s->smem_budget = s->opt.smem_budget > 0 ? std::min(s->opt.smem_budget, kMaxSmemBudget) : (int)kSmemBudget;
 
     // partition size: BAAS_THREADS: the schedule's threads; else `parts`, or about one CTA per
-    // 2,048 rows (at most 128, at most one per SM)
+    // 2,048 rows (at most one per SM)
     const int n = s->hs.n;
     if (s->opt.partition == BAAS_PARTITION_BAAS_THREADS && s->opt.parts > 0 && s->opt.parts != s->hs.nthread)
         return fail(BAAS_ERR_BAD_ARG, "BAAS_THREADS partition needs parts == nthread");

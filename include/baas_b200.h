@@ -105,7 +105,7 @@ typedef struct baas_options {
     int nthread;      /* the reference's num_thread: virtual threads of the schedule (>= 1) */
     int spin_limit;   /* polls before a device wait gives up (0 = library default) */
     int parts;        /* CTAs that own rows in the partitioned kernels (0 = automatic: about one
-                         per 2,048 rows, at most 128 and at most one per SM) */
+                         per 2,048 rows, at most one per SM) */
     int partition;    /* BAAS_PARTITION_AUTO (default), BAAS_PARTITION_RANGES, BAAS_PARTITION_BLOCKS,
                          BAAS_PARTITION_BAAS_THREADS, or BAAS_PARTITION_CUSTOM (set by
                          baas_replan_custom only) */
