@@ -78,3 +78,30 @@ def test_scheduler_mapping_on_gpu(mapping):
     y = torch.zeros(A.n, dtype=torch.float64, device="cuda")
     s.forward(DeviceCSR.from_host(Lo), _t(b), y)
     assert np.array_equal(y.cpu().numpy(), Port.lower_solve(Lo, b))
+
+
+@pytest.mark.parametrize("k", [32, 72])
+def test_default_range_count(k):
+    """Automatic row ranges: one CTA per 2,048 rows, rounded up, and never more CTAs than SMs
+    (32^3: 16 CTAs; 72^3 = 373,248 rows: capped at the SM count). The sweep on that plan solves
+    L y = b, with L = I + tril(C, -1) diag(C)^-1 (columns scaled as in an ILU0 factor, so that
+    forward substitution stays bounded)."""
+    import scipy.sparse as sp
+    import torch
+
+    from baas_b200 import KERNEL_ILU0, PARTITION_RANGES
+
+    C = gen.convdiff3d(k)
+    Cs = C.to_scipy()
+    Lo = gen.from_scipy(sp.tril(Cs, k=-1) @ sp.diags(1.0 / Cs.diagonal()) + sp.identity(C.n))
+    s = Schedule(C, kind=KERNEL_ILU0, nthread=8, partition=PARTITION_RANGES)
+    b = gen.normal_rhs(C.n, 5)
+    y = _t(np.zeros(C.n))
+    s.forward(DeviceCSR.from_host(Lo), _t(b), y)
+    torch.cuda.synchronize()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    P, box, _ = s.plan_parts()
+    assert box is None
+    assert P == min((C.n + 2047) // 2048, sms)
+    r = Lo.to_scipy() @ y.cpu().numpy() - b
+    assert np.linalg.norm(r) <= 1e-12 * np.linalg.norm(b)
