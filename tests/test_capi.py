@@ -73,6 +73,20 @@ def test_bad_arg_on_null_and_size_mismatch():
     assert L.baas_schedule_export(s._h, 99, None) == -1
 
 
+def test_ic0_noalloc_refuses_patterns_above_its_scratch_size():
+    # the allocation-free IC0's static scratch holds one ready flag per row, at most 2,097,152;
+    # a larger pattern is refused on the host, before any device call (a diagonal keeps the
+    # analysis cheap)
+    n = (1 << 21) + 1
+    A = gen.CSR(n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), np.ones(n))
+    s = Schedule(A, kind=KERNEL_ICCG, nthread=2)
+    L = _native.lib()
+    c = _native.BaasCsr(n, n, A.rowptr.ctypes.data, A.colidx.ctypes.data, A.values.ctypes.data)
+    lu = np.ones(n)
+    assert L.baas_ic0_noalloc(s._h, C.byref(c), lu.ctypes.data, None) == 1  # BAAS_ERR_BAD_ARG
+    assert "at most 2097152 rows" in L.baas_last_error_string().decode()
+
+
 def test_analysis_time_reported():
     s = Schedule(gen.laplace3d(8, 1e-3), kind=KERNEL_ICCG, nthread=4)
     assert s.analysis_ms > 0.0
